@@ -1,0 +1,95 @@
+"""ctypes binding of the C ABI declared in include/ctsim_b200.h.
+
+The library is the in-tree build ``ctsim_b200/_lib/libctsim_b200.so``.  There is
+no fallback: if it is missing and cannot be built, importing the projector API
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+_f, _i, _p, _d = C.c_float, C.c_int, C.c_void_p, C.c_double
+GEOM_ARGS = [_i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i, _f, _f, _f, _f, _f, _f, _f, _i, _p, _p, _i]
+
+CTSIM_OK = 0
+STATUS = {0: "OK", 1: "ERR_ARGUMENT", 2: "ERR_CUDA", 3: "ERR_ALLOC", 4: "ERR_UNSUPPORTED", 5: "ERR_NO_DEVICE"}
+METHODS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3, "back,pd": 4, "back,hpd": 5}
+
+# symbols declared in include/ctsim_b200.h
+EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd", "ctsim_proj_tf", "ctsim_back_tf",
+            "ctsim_back_pd", "ctsim_cbct_geom", "ctsim_plan_create", "ctsim_plan_destroy", "ctsim_plan_device_bytes",
+            "ctsim_plan_project", "ctsim_plan_backproject", "ctsim_plan_check"]
+
+
+class CtsimGeom(C.Structure):
+    _fields_ = [("nx", _i), ("ny", _i), ("nz", _i), ("dx", _f), ("dy", _f), ("dz", _f),
+                ("offset_x", _f), ("offset_y", _f), ("offset_z", _f), ("nu", _i), ("nv", _i),
+                ("du", _f), ("dv", _f), ("offset_u", _f), ("offset_v", _f),
+                ("sad", _f), ("add", _f), ("sdd", _f), ("noviews", _i), ("detector_type", _i)]
+
+
+class CtsimError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load():
+    """Load (building first if needed) the projector library."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if not os.path.exists(path) or _build.needs_rebuild():
+        try:
+            _build.build()
+        except Exception as exc:  # no nvcc on this machine and no prebuilt library
+            if not os.path.exists(path):
+                raise ImportError(f"libctsim_b200.so is missing and could not be built: {exc}") from exc
+    L = C.CDLL(path)
+    L.ctsim_last_error.restype = C.c_char_p
+    L.ctsim_version.restype = C.c_char_p
+    for name in ("ctsim_proj_dd", "ctsim_proj_tf"):
+        fn = getattr(L, name)
+        fn.argtypes = GEOM_ARGS + [_p, _p, _p]
+        fn.restype = C.c_bool
+    for name in ("ctsim_back_dd", "ctsim_back_tf"):
+        fn = getattr(L, name)
+        fn.argtypes = GEOM_ARGS + [_p, _p, _p]
+        fn.restype = C.c_bool
+    L.ctsim_back_pd.argtypes = GEOM_ARGS + [_p, _p, _p, C.c_bool]
+    L.ctsim_back_pd.restype = C.c_bool
+    L.ctsim_cbct_geom.argtypes = [C.c_char_p] + GEOM_ARGS + [_p, _p, _p]
+    L.ctsim_cbct_geom.restype = C.c_bool
+    L.ctsim_plan_create.argtypes = [C.POINTER(CtsimGeom), _p, _p, _p, C.POINTER(_p)]
+    L.ctsim_plan_create.restype = _i
+    L.ctsim_plan_destroy.argtypes = [_p]
+    L.ctsim_plan_destroy.restype = _i
+    L.ctsim_plan_device_bytes.argtypes = [_p]
+    L.ctsim_plan_device_bytes.restype = C.c_size_t
+    L.ctsim_plan_project.argtypes = [_p, _i, _p, _p, _i, _i, _i, _p]
+    L.ctsim_plan_project.restype = _i
+    L.ctsim_plan_backproject.argtypes = [_p, _i, _p, _p, _i, _i, _i, _f, _p]
+    L.ctsim_plan_backproject.restype = _i
+    L.ctsim_plan_check.argtypes = [_p]
+    L.ctsim_plan_check.restype = _i
+    _lib = L
+    return L
+
+
+def check(status: int, what: str = "ctsim"):
+    if status != CTSIM_OK:
+        msg = load().ctsim_last_error().decode(errors="replace")
+        raise CtsimError(f"{what}: {STATUS.get(status, status)}: {msg}")
+
+
+def last_error() -> str:
+    return load().ctsim_last_error().decode(errors="replace")

@@ -1,0 +1,403 @@
+// C ABI: plans (device-resident geometry tables + scratch) and the drop-in
+// host-pointer entry points that replace the reference's cbct_*_gpu functions.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ctsim_b200.h"
+#include "kernels.cuh"
+
+using namespace ctsim;
+
+namespace {
+
+thread_local std::string g_last_error = "";
+
+ctsim_status fail(ctsim_status s, const std::string &msg) {
+    g_last_error = msg;
+    return s;
+}
+
+ctsim_status cuda_fail(cudaError_t e, const char *what) {
+    return fail(CTSIM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Centre offset "- ( n - 1.0 ) / 2.0 + offset" in double, stored as float
+// (geom/cbct/cbct_proj.c:244-247).
+float centre(int n, float off) { return (float)(-((double)n - 1.0) / 2.0 + (double)off); }
+
+// Smallest float f with (double)f >= x.
+float float_at_or_above(double x) {
+    float f = (float)x;
+    if ((double)f < x) f = std::nextafter(f, INFINITY);
+    return f;
+}
+// Largest float f with (double)f <= x.
+float float_at_or_below(double x) {
+    float f = (float)x;
+    if ((double)f > x) f = std::nextafter(f, -INFINITY);
+    return f;
+}
+
+int pow2_at_least(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+}  // namespace
+
+struct ctsim_plan {
+    ctsim_geom geom{};
+    Geom g{};
+    int device = 0;
+    View *d_views = nullptr;
+    float *d_ampv = nullptr;
+    uint8_t *d_map = nullptr;
+    float *d_xc = nullptr;  // axial prefix sums [nx*ny][nz+1] (forward projector scratch)
+    int *d_err = nullptr;
+    size_t bytes = 0;
+    float margin = 0.f;      // candidate window margin of the forward projector (pixels)
+    float zinc_max = 0.f;    // upper bound of a voxel's height in detector rows
+    int back_mz = 1, back_qcap = 0, pd_mz = 1;
+    bool fwd_ok = true;
+    std::string fwd_reason;
+};
+
+extern "C" const char *ctsim_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *ctsim_version(void) { return "ctsim_b200 0.1 (sm_100a)"; }
+
+static void free_plan(ctsim_plan *p) {
+    if (!p) return;
+    cudaFree(p->d_views);
+    cudaFree(p->d_ampv);
+    cudaFree(p->d_map);
+    cudaFree(p->d_xc);
+    cudaFree(p->d_err);
+    delete p;
+}
+
+extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *betas, const float *couchz,
+                                          const bool *map, ctsim_plan **out) {
+    if (!geom || !betas || !couchz || !out) return fail(CTSIM_ERR_ARGUMENT, "null argument");
+    *out = nullptr;
+    const ctsim_geom G = *geom;
+    if (G.nx < 1 || G.ny < 1 || G.nz < 1 || G.nu < 2 || G.nv < 2 || G.noviews < 1)
+        return fail(CTSIM_ERR_ARGUMENT, "sizes must be positive (nu, nv >= 2)");
+    if (!(G.dx > 0 && G.dy > 0 && G.dz > 0 && G.du > 0 && G.dv > 0 && G.sad > 0 && G.sdd > 0))
+        return fail(CTSIM_ERR_ARGUMENT, "spacings and distances must be positive");
+    if (G.detector_type != 0 && G.detector_type != 1)
+        return fail(CTSIM_ERR_ARGUMENT, "detector_type must be 1 (flat) or 0 (curved)");
+    const long long nxy = (long long)G.nx * G.ny;
+    if (nxy * G.nz > (1LL << 31) - 1 || (long long)G.nu * G.nv * G.noviews > (1LL << 40))
+        return fail(CTSIM_ERR_ARGUMENT, "volume too large");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(CTSIM_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+    if (prop.major != 10) return fail(CTSIM_ERR_NO_DEVICE, "ctsim_b200 is built for sm_100a (B200) only");
+
+    ctsim_plan *p = new ctsim_plan();
+    p->geom = G;
+    p->device = dev;
+    Geom &g = p->g;
+    g.nx = G.nx; g.ny = G.ny; g.nz = G.nz; g.nu = G.nu; g.nv = G.nv; g.det = G.detector_type;
+    g.dx = G.dx; g.dy = G.dy; g.dz = G.dz; g.sad = G.sad; g.sdd = G.sdd; g.du = G.du; g.dv = G.dv;
+    g.wx = centre(G.nx, G.offset_x);
+    g.wy = centre(G.ny, G.offset_y);
+    g.wu = centre(G.nu, G.offset_u);
+    g.wv = centre(G.nv, G.offset_v);
+    g.sdd_du = G.sdd / G.du;
+    g.dz_dv = G.dz / G.dv;
+    g.wz_pd = centre(G.nz, G.offset_z);
+    g.roff = G.offset_u * G.du * G.sad / G.sdd;
+    g.u_lo = float_at_or_above(1e-6);
+    g.u_hi = float_at_or_below((double)G.nu - 1.0 - 1e-6);
+    g.v_lo = float_at_or_above(1e-6);
+    g.v_hi = float_at_or_below((double)G.nv - 1.0 - 1e-6);
+    g.v_clamp_lo = 0.5f;
+    g.v_clamp_hi = (float)((double)G.nv - 1.5);
+
+    // per-view table, geom/cbct/cbct_proj.c:256-265, cbct_back.c:47-52
+    std::vector<View> views(G.noviews);
+    for (int ib = 0; ib < G.noviews; ib++) {
+        View &v = views[ib];
+        v.sin_a = (float)std::sin(betas[ib]);
+        v.cos_a = (float)std::cos(betas[ib]);
+        const float cz = couchz[ib] / G.dz;
+        v.wz = (float)((-((double)G.nz - 1.0) / 2.0 + (double)G.offset_z) + (double)cz);
+        v.dx_sin_2 = (float)((double)(G.dx * v.sin_a) / 2.0);
+        v.dx_cos_2 = (float)((double)(G.dx * v.cos_a) / 2.0);
+        v.dy_sin_2 = (float)((double)(G.dy * v.sin_a) / 2.0);
+        v.n_dy_cos_2 = (float)((double)(-G.dy * v.cos_a) / 2.0);
+        v.couch_pd = (float)(int)couchz[ib];
+    }
+    // axial amplitude per detector pixel, geom/cbct/cbct_proj.c:432-450
+    std::vector<float> ampv((size_t)G.nu * G.nv);
+    for (int iu = 0; iu < G.nu; iu++) {
+        const float u = ((float)iu + g.wu) * G.du;
+        const float uu = G.sdd * G.sdd + u * u;
+        for (int iv = 0; iv < G.nv; iv++) {
+            const float v = ((float)iv + g.wv) * G.dv;
+            float a;
+            if (G.detector_type == 1) a = (float)std::sqrt((double)((uu + v * v) / uu));
+            else a = (float)(std::sqrt((double)(G.sdd * G.sdd + v * v)) / (double)G.sdd);
+            ampv[(size_t)iu * G.nv + iv] = a;
+        }
+    }
+    std::vector<uint8_t> mp((size_t)nxy, 1);
+    if (map)
+        for (long long i = 0; i < nxy; i++) mp[i] = map[i] ? 1 : 0;
+
+    // Bounds used to size the kernels: the largest distance of a voxel column
+    // centre from the rotation axis, hence the smallest source distance.
+    double rmax = 0.0;
+    for (int cx = 0; cx < 2; cx++)
+        for (int cy = 0; cy < 2; cy++) {
+            const double xc = ((cx ? G.nx - 1 : 0) + (double)g.wx) * G.dx;
+            const double yc = ((cy ? G.ny - 1 : 0) + (double)g.wy) * G.dy;
+            rmax = std::max(rmax, std::sqrt(xc * xc + yc * yc));
+        }
+    const double diag = std::sqrt((double)G.dx * G.dx + (double)G.dy * G.dy);
+    const double dmin = (double)G.sad - rmax - diag;
+    if (!(dmin > 0.0)) {
+        free_plan(p);
+        return fail(CTSIM_ERR_UNSUPPORTED, "the source orbit must lie outside the volume (SAD > volume radius)");
+    }
+    p->zinc_max = (float)((double)G.dz / G.dv * G.sdd / ((double)G.sad - rmax) * 1.0001 + 1e-6);
+    const double umm = std::max(std::fabs((double)g.wu * G.du), std::fabs(((double)G.nu - 1 + g.wu) * G.du)) + G.du;
+    const double stretch = G.detector_type == 1 ? 1.0 + (umm / G.sdd) * (umm / G.sdd) : 1.0;
+    p->margin = (float)std::ceil(0.5 * diag * G.sdd / dmin / G.du * stretch) + 2.0f;
+    if (p->zinc_max > 9.0f) {
+        p->fwd_ok = false;
+        p->fwd_reason = "forward projection needs every voxel's axial footprint within 10 detector rows (dz/dv*SDD/dist <= 9)";
+    }
+    if (G.nx > proj_max_lines() || G.ny > proj_max_lines()) {
+        p->fwd_ok = false;
+        p->fwd_reason = "forward projection supports nx, ny <= 2048";
+    }
+    if (proj_smem_bytes(G.nv) > 190 * 1024) {
+        p->fwd_ok = false;
+        p->fwd_reason = "forward projection supports nv <= 6080";
+    }
+    // A^T: z pass of 32*MZ voxels and the per-warp row buffer that covers its shadow
+    {
+        int mz = std::min(8, pow2_at_least((G.nz + 31) / 32));
+        int qcap = 0;
+        for (;; mz >>= 1) {
+            qcap = std::min(G.nv, (int)std::ceil(32.0 * mz * p->zinc_max) + 3);
+            if ((size_t)8 * qcap * sizeof(float) <= 200 * 1024 || mz == 1) break;
+        }
+        p->back_mz = mz;
+        p->back_qcap = qcap;
+        p->pd_mz = std::min(8, pow2_at_least((G.nz + 31) / 32));
+    }
+
+    // device allocations
+    size_t bytes = 0;
+#define CTSIM_ALLOC(ptr, n)                                                          \
+    do {                                                                             \
+        e = cudaMalloc((void **)&(ptr), (n));                                        \
+        if (e != cudaSuccess) {                                                      \
+            free_plan(p);                                                            \
+            return fail(CTSIM_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)); \
+        }                                                                            \
+        bytes += (n);                                                                \
+    } while (0)
+    CTSIM_ALLOC(p->d_views, sizeof(View) * G.noviews);
+    CTSIM_ALLOC(p->d_ampv, sizeof(float) * ampv.size());
+    CTSIM_ALLOC(p->d_map, mp.size());
+    CTSIM_ALLOC(p->d_err, sizeof(int));
+    if (p->fwd_ok) CTSIM_ALLOC(p->d_xc, sizeof(float) * (size_t)nxy * (G.nz + 1));
+#undef CTSIM_ALLOC
+    p->bytes = bytes;
+    if ((e = cudaMemcpy(p->d_views, views.data(), sizeof(View) * G.noviews, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(p->d_ampv, ampv.data(), sizeof(float) * ampv.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(p->d_map, mp.data(), mp.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemset(p->d_err, 0, sizeof(int))) != cudaSuccess) {
+        free_plan(p);
+        return cuda_fail(e, "plan upload");
+    }
+    *out = p;
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_plan_destroy(ctsim_plan *plan) {
+    free_plan(plan);
+    return CTSIM_OK;
+}
+
+extern "C" size_t ctsim_plan_device_bytes(const ctsim_plan *plan) { return plan ? plan->bytes : 0; }
+
+static ctsim_status check_views(const ctsim_plan *p, int vb, int vs, int vc) {
+    if (vc < 1 || vs < 1 || vb < 0 || (long long)vb + (long long)(vc - 1) * vs >= p->geom.noviews)
+        return fail(CTSIM_ERR_ARGUMENT, "view selection outside the plan's views");
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_plan_project(ctsim_plan *p, int method, const float *d_image, float *d_proj,
+                                           int view_begin, int view_stride, int view_count, void *stream) {
+    if (!p || !d_image || !d_proj) return fail(CTSIM_ERR_ARGUMENT, "null argument");
+    if (method != CTSIM_PROJ_DD && method != CTSIM_PROJ_TF) return fail(CTSIM_ERR_ARGUMENT, "unknown forward method");
+    ctsim_status s = check_views(p, view_begin, view_stride, view_count);
+    if (s != CTSIM_OK) return s;
+    if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nxy = p->g.nx * p->g.ny;
+    cudaError_t e = launch_prefix(d_image, p->d_xc, nxy, p->g.nz, st);
+    if (e != cudaSuccess) return cuda_fail(e, "prefix kernel");
+    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->g, p->d_views, p->d_xc, p->d_ampv, p->d_map, d_proj,
+                    view_begin, view_stride, view_count, p->margin, st);
+    if (e != cudaSuccess) return cuda_fail(e, "forward projection kernel");
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_plan_backproject(ctsim_plan *p, int method, const float *d_proj, float *d_image,
+                                               int view_begin, int view_stride, int view_count, float scale,
+                                               void *stream) {
+    if (!p || !d_image || !d_proj) return fail(CTSIM_ERR_ARGUMENT, "null argument");
+    ctsim_status s = check_views(p, view_begin, view_stride, view_count);
+    if (s != CTSIM_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    switch (method) {
+    case CTSIM_BACK_DD:
+    case CTSIM_BACK_TF:
+        e = launch_back(method == CTSIM_BACK_DD ? kDD : kTF, p->back_mz, p->g, p->d_views, d_proj, p->d_ampv,
+                        p->d_map, d_image, view_begin, view_stride, view_count, scale, p->back_qcap, p->d_err, st);
+        break;
+    case CTSIM_BACK_PD:
+    case CTSIM_BACK_HPD:
+        e = launch_pd(method == CTSIM_BACK_PD, p->pd_mz, p->g, p->d_views, d_proj, p->d_map, d_image, view_begin,
+                      view_stride, view_count, scale, st);
+        break;
+    default:
+        return fail(CTSIM_ERR_ARGUMENT, "unknown backprojection method");
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "backprojection kernel");
+    return CTSIM_OK;
+}
+
+// Synchronous check of the plan's device error flag (set if a kernel met a
+// footprint larger than its buffers; never expected for a valid plan).
+extern "C" ctsim_status ctsim_plan_check(ctsim_plan *p) {
+    if (!p) return fail(CTSIM_ERR_ARGUMENT, "null plan");
+    int h = 0;
+    cudaError_t e = cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "error flag read");
+    if (h) return fail(CTSIM_ERR_UNSUPPORTED, "a footprint exceeded the kernel's row buffer");
+    return CTSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Drop-in host-pointer entry points.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct DeviceBuf {
+    void *p = nullptr;
+    ~DeviceBuf() { cudaFree(p); }
+};
+
+bool run_host(int method, const ctsim_geom &G, const double *betas, const float *couchz, const bool *map,
+              const float *in, float *out) {
+    if (!betas || !couchz || !in || !out) {
+        fail(CTSIM_ERR_ARGUMENT, "null argument");
+        return false;
+    }
+    ctsim_plan *p = nullptr;
+    if (ctsim_plan_create(&G, betas, couchz, map, &p) != CTSIM_OK) return false;
+    const bool fwd = method == CTSIM_PROJ_DD || method == CTSIM_PROJ_TF;
+    const size_t nimg = (size_t)G.nx * G.ny * G.nz, nsino = (size_t)G.nu * G.nv * G.noviews;
+    const size_t nin = fwd ? nimg : nsino, nout = fwd ? nsino : nimg;
+    DeviceBuf din, dout;
+    cudaStream_t st = nullptr;
+    bool ok = false;
+    cudaError_t e;
+    do {
+        if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) { cuda_fail(e, "stream"); break; }
+        if ((e = cudaMalloc(&din.p, nin * sizeof(float))) != cudaSuccess ||
+            (e = cudaMalloc(&dout.p, nout * sizeof(float))) != cudaSuccess) {
+            fail(CTSIM_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+            break;
+        }
+        if ((e = cudaMemcpyAsync(din.p, in, nin * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess) {
+            cuda_fail(e, "host to device copy");
+            break;
+        }
+        ctsim_status s = fwd ? ctsim_plan_project(p, method, (const float *)din.p, (float *)dout.p, 0, 1, G.noviews, st)
+                             : ctsim_plan_backproject(p, method, (const float *)din.p, (float *)dout.p, 0, 1,
+                                                      G.noviews, 1.0f, st);
+        if (s != CTSIM_OK) break;
+        if ((e = cudaMemcpyAsync(out, dout.p, nout * sizeof(float), cudaMemcpyDeviceToHost, st)) != cudaSuccess) {
+            cuda_fail(e, "device to host copy");
+            break;
+        }
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) { cuda_fail(e, "kernel execution"); break; }
+        if (ctsim_plan_check(p) != CTSIM_OK) break;
+        ok = true;
+    } while (0);
+    if (st) cudaStreamDestroy(st);
+    ctsim_plan_destroy(p);
+    return ok;
+}
+
+ctsim_geom make_geom(int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy, float oz, int nu,
+                     int nv, float du, float dv, float ou, float ov, float sad, float add, float sdd, int noviews,
+                     int detector_type) {
+    ctsim_geom G;
+    G.nx = nx; G.ny = ny; G.nz = nz; G.dx = dx; G.dy = dy; G.dz = dz;
+    G.offset_x = ox; G.offset_y = oy; G.offset_z = oz;
+    G.nu = nu; G.nv = nv; G.du = du; G.dv = dv; G.offset_u = ou; G.offset_v = ov;
+    G.sad = sad; G.add = add; G.sdd = sdd; G.noviews = noviews; G.detector_type = detector_type;
+    return G;
+}
+
+}  // namespace
+
+#define CTSIM_GEOM_PARAMS                                                                                        \
+    int nx, int ny, int nz, float dx, float dy, float dz, float offset_x, float offset_y, float offset_z, int nu, \
+        int nv, float du, float dv, float offset_u, float offset_v, float sad, float add, float sdd, int noviews, \
+        const double *betas, const float *couchz, int detector_type
+#define CTSIM_GEOM_VALUES \
+    make_geom(nx, ny, nz, dx, dy, dz, offset_x, offset_y, offset_z, nu, nv, du, dv, offset_u, offset_v, sad, add, sdd, noviews, detector_type)
+
+extern "C" bool ctsim_proj_dd(CTSIM_GEOM_PARAMS, const float *image, float *proj, const bool *map) {
+    return run_host(CTSIM_PROJ_DD, CTSIM_GEOM_VALUES, betas, couchz, map, image, proj);
+}
+extern "C" bool ctsim_proj_tf(CTSIM_GEOM_PARAMS, const float *image, float *proj, const bool *map) {
+    return run_host(CTSIM_PROJ_TF, CTSIM_GEOM_VALUES, betas, couchz, map, image, proj);
+}
+extern "C" bool ctsim_back_dd(CTSIM_GEOM_PARAMS, float *image, const float *proj, const bool *map) {
+    return run_host(CTSIM_BACK_DD, CTSIM_GEOM_VALUES, betas, couchz, map, proj, image);
+}
+extern "C" bool ctsim_back_tf(CTSIM_GEOM_PARAMS, float *image, const float *proj, const bool *map) {
+    return run_host(CTSIM_BACK_TF, CTSIM_GEOM_VALUES, betas, couchz, map, proj, image);
+}
+extern "C" bool ctsim_back_pd(CTSIM_GEOM_PARAMS, float *image, const float *proj, const bool *map, bool offBoundary) {
+    return run_host(offBoundary ? CTSIM_BACK_PD : CTSIM_BACK_HPD, CTSIM_GEOM_VALUES, betas, couchz, map, proj, image);
+}
+
+extern "C" bool ctsim_cbct_geom(const char *type, CTSIM_GEOM_PARAMS, const float *data, float *out, const bool *map) {
+    if (!type) {
+        fail(CTSIM_ERR_ARGUMENT, "The 1st argument is invalid!");
+        return false;
+    }
+    // string dispatch of geom/cbct/cbct_geom_mex.c:267-306 ("proj,rd" and "back,var" are not provided)
+    int method = -1;
+    if (!std::strcmp(type, "proj,dd")) method = CTSIM_PROJ_DD;
+    else if (!std::strcmp(type, "proj,tf")) method = CTSIM_PROJ_TF;
+    else if (!std::strcmp(type, "back,dd")) method = CTSIM_BACK_DD;
+    else if (!std::strcmp(type, "back,tf")) method = CTSIM_BACK_TF;
+    else if (!std::strcmp(type, "back,pd")) method = CTSIM_BACK_PD;
+    else if (!std::strcmp(type, "back,hpd")) method = CTSIM_BACK_HPD;
+    if (method < 0) {
+        fail(CTSIM_ERR_ARGUMENT, "Error: unknown geom type.");
+        return false;
+    }
+    return run_host(method, CTSIM_GEOM_VALUES, betas, couchz, map, data, out);
+}

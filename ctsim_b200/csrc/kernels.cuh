@@ -1,0 +1,33 @@
+// Launcher declarations for the projector kernels (kernels.cu).
+#pragma once
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace ctsim {
+
+cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *proj, const float *ampv,
+                        const uint8_t *map, float *image, int view_begin, int view_stride, int view_count,
+                        float scale, int qcap, int *err, cudaStream_t st);
+
+cudaError_t launch_prefix(const float *image, float *xc, int nxy, int nz, cudaStream_t st);
+
+cudaError_t launch_proj(int method, const Geom &g, const View *views, const float *xc, const float *ampv,
+                        const uint8_t *map, float *proj, int view_begin, int view_stride, int view_count,
+                        float margin, cudaStream_t st);
+
+cudaError_t launch_pd(bool off_boundary, int mz, const Geom &g, const View *views, const float *proj,
+                      const uint8_t *map, float *image, int view_begin, int view_stride, int view_count, float scale,
+                      cudaStream_t st);
+
+cudaError_t launch_scale(float *y, size_t n, float s, cudaStream_t st);
+
+size_t proj_smem_bytes(int nv);
+int proj_group_width();
+int proj_max_lines();
+
+}  // namespace ctsim

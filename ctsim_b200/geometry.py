@@ -1,0 +1,107 @@
+"""Cone-beam geometry, mirroring the reference's MATLAB ``geom`` struct.
+
+The reference builds this struct in ``parameters/loadProjectionGeometryCT.m``
+and passes its fields to the MEX projectors in a fixed order
+(``geom/shell/forwardProjectMex.m:82-85``)::
+
+    <mex>(type, int32(reconSize), single(reconSpacing), single(reconOffset),
+          int32(detSize), single(detSpacing), single(detOffset),
+          single(SAD), single(ADD), single(SDD), int32(noViews),
+          double(betas), single(couchZ), int32(flatPanel), single(data),
+          logical(map))
+
+Array conventions used throughout this package (C order, numpy/torch):
+
+* image  ``float32[nz, ny, nx]``  == MATLAB ``single[nx ny nz]`` (x fastest)
+* sino   ``float32[noViews, nu, nv]`` == MATLAB ``single[nv nu noViews]`` (v fastest)
+* map    ``bool[ny, nx]``          == MATLAB ``logical[nx ny]``
+
+Units follow the reference: lengths in mm, attenuation in 1/cm inside the
+projectors (they divide the in-plane path length by 10,
+``geom/cbct/cbct_proj.c:300``).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field, replace
+from typing import Optional
+
+import numpy as np
+
+
+@dataclass
+class CTGeometry:
+    reconSize: tuple            # (nx, ny, nz)
+    reconSpacing: tuple         # (dx, dy, dz) mm
+    reconOffset: tuple          # (ox, oy, oz) in voxels
+    detSize: tuple              # (nu, nv)
+    detSpacing: tuple           # (du, dv) mm
+    detOffset: tuple            # (ou, ov) in pixels
+    SAD: float
+    ADD: float
+    SDD: float
+    betas: np.ndarray           # float64[noViews], radians
+    couchZ: Optional[np.ndarray] = None   # float32[noViews], mm
+    flatPanel: int = 1          # 1 flat, 0 curved (equiangular)
+    map: Optional[np.ndarray] = None      # bool[ny, nx]
+    shortScan: bool = False
+
+    def __post_init__(self):
+        self.reconSize = tuple(int(v) for v in self.reconSize)
+        self.reconSpacing = tuple(float(np.float32(v)) for v in self.reconSpacing)
+        self.reconOffset = tuple(float(np.float32(v)) for v in self.reconOffset)
+        self.detSize = tuple(int(v) for v in self.detSize)
+        self.detSpacing = tuple(float(np.float32(v)) for v in self.detSpacing)
+        self.detOffset = tuple(float(np.float32(v)) for v in self.detOffset)
+        self.betas = np.ascontiguousarray(np.asarray(self.betas, dtype=np.float64).reshape(-1))
+        if self.couchZ is None:
+            self.couchZ = np.zeros(self.betas.size, dtype=np.float32)
+        self.couchZ = np.ascontiguousarray(np.asarray(self.couchZ, dtype=np.float32).reshape(-1))
+        if self.map is None:
+            self.map = np.ones((self.ny, self.nx), dtype=bool)
+        self.map = np.ascontiguousarray(np.asarray(self.map, dtype=bool))
+        if self.map.shape != (self.ny, self.nx):
+            raise ValueError("map must have shape (ny, nx)")
+        if self.couchZ.size != self.betas.size:
+            raise ValueError("couchZ must have one entry per view")
+
+    # convenience accessors -------------------------------------------------
+    nx = property(lambda s: s.reconSize[0])
+    ny = property(lambda s: s.reconSize[1])
+    nz = property(lambda s: s.reconSize[2])
+    nu = property(lambda s: s.detSize[0])
+    nv = property(lambda s: s.detSize[1])
+    noViews = property(lambda s: int(s.betas.size))
+
+    @property
+    def image_shape(self):
+        return (self.nz, self.ny, self.nx)
+
+    @property
+    def sino_shape(self):
+        return (self.noViews, self.nu, self.nv)
+
+    @property
+    def voxel_views(self) -> int:
+        return self.nx * self.ny * self.nz * self.noViews
+
+    def subset(self, M: int, isub: int) -> "CTGeometry":
+        """Views ``1+mod(isub,M):M:end`` (geom/shell/forwardProjectMex.m:36-38)."""
+        if M == 1:
+            return self
+        sel = slice(isub % M, None, M)
+        return replace(self, betas=self.betas[sel].copy(), couchZ=self.couchZ[sel].copy())
+
+    def scalars(self):
+        """The scalar MEX arguments in reference order (after ``type``)."""
+        return (self.nx, self.ny, self.nz,
+                self.reconSpacing[0], self.reconSpacing[1], self.reconSpacing[2],
+                self.reconOffset[0], self.reconOffset[1], self.reconOffset[2],
+                self.nu, self.nv, self.detSpacing[0], self.detSpacing[1],
+                self.detOffset[0], self.detOffset[1],
+                float(np.float32(self.SAD)), float(np.float32(self.ADD)), float(np.float32(self.SDD)),
+                self.noViews)
+
+
+def circular_betas(n_views: int, arc: float = 2 * np.pi) -> np.ndarray:
+    """Evenly spaced view angles ``(0:N-1) * arc / N`` (geom/test_projectors_3d.m:59)."""
+    return np.arange(n_views, dtype=np.float64) * (arc / n_views)

@@ -1,0 +1,163 @@
+/*
+ * ctsim_b200 -- C ABI of the B200 (sm_100a) cone-beam projector library.
+ *
+ * Two families of entry points:
+ *
+ * 1. Drop-in replacements for the reference's CUDA MEX back ends.  Same argument
+ *    order, types and array layouts; host pointers in, host pointers out;
+ *    synchronous; return true on success (the reference returns bool, and its MEX
+ *    gateway turns false into mexErrMsgTxt("Error: cbct_geom_mex() failed.")).
+ *    Unlike the reference, errors never exit() the host process and inputs are
+ *    never modified (the reference's CPU back-projectors scale the sinogram
+ *    argument in place).
+ *
+ *      image   float[nz][ny][nx]        (MATLAB single [nx ny nz], x fastest)
+ *      proj    float[noviews][nu][nv]   (MATLAB single [nv nu noviews], v fastest)
+ *      map     bool[ny][nx]             (MATLAB logical [nx ny])
+ *      betas   double[noviews] (radians), couchz float[noviews] (mm)
+ *      detector_type: 1 flat panel, 0 curved (equiangular)
+ *
+ *    Outputs are overwritten (the reference MEX allocates them zero-filled and
+ *    accumulates; the result is the same).
+ *
+ * 2. Device-resident plans for callers that keep volumes and sinograms in GPU
+ *    memory (FDK, OS-PWLS loops, batching).  A plan holds the per-view geometry
+ *    tables and scratch buffers; its projector calls take device pointers and a
+ *    CUDA stream (as void*), allocate nothing, and are asynchronous.
+ *
+ * Status codes returned by the plan API: see ctsim_status.
+ */
+#ifndef CTSIM_B200_H
+#define CTSIM_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    CTSIM_OK = 0,
+    CTSIM_ERR_ARGUMENT = 1,    /* invalid sizes, null pointers, unknown method */
+    CTSIM_ERR_CUDA = 2,        /* a CUDA runtime call or kernel launch failed */
+    CTSIM_ERR_ALLOC = 3,       /* device or host allocation failed */
+    CTSIM_ERR_UNSUPPORTED = 4, /* geometry outside what the kernels implement (see the DESIGN notes) */
+    CTSIM_ERR_NO_DEVICE = 5    /* no usable sm_100 device */
+} ctsim_status;
+
+/* Projector methods (the reference's geom type strings). */
+typedef enum {
+    CTSIM_PROJ_DD = 0,  /* "proj,dd"  */
+    CTSIM_PROJ_TF = 1,  /* "proj,tf"  */
+    CTSIM_BACK_DD = 2,  /* "back,dd"  */
+    CTSIM_BACK_TF = 3,  /* "back,tf"  */
+    CTSIM_BACK_PD = 4,  /* "back,pd"  */
+    CTSIM_BACK_HPD = 5  /* "back,hpd" */
+} ctsim_method;
+
+/* Last error message of the calling thread (never NULL). */
+const char *ctsim_last_error(void);
+
+/* Library version string. */
+const char *ctsim_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Family 1: drop-in host-pointer entry points.
+ * ------------------------------------------------------------------------- */
+
+/* Replaces cbct_proj_dd_gpu (geom/dd_cuda/cbct_dd_proj.c:407-432) and the CPU
+ * cbct_proj_dd (geom/cbct/cbct_proj.c:217-242): distance-driven forward projection. */
+bool ctsim_proj_dd(int nx, int ny, int nz, float dx, float dy, float dz, float offset_x, float offset_y,
+                   float offset_z, int nu, int nv, float du, float dv, float offset_u, float offset_v, float sad,
+                   float add, float sdd, int noviews, const double *betas, const float *couchz, int detector_type,
+                   const float *image, float *proj, const bool *map);
+
+/* Replaces cbct_back_dd_gpu (geom/dd_cuda/cbct_dd_back.c:299-324) and the CPU
+ * cbct_back_dd (geom/cbct/cbct_back.c:136-161): matched distance-driven backprojection. */
+bool ctsim_back_dd(int nx, int ny, int nz, float dx, float dy, float dz, float offset_x, float offset_y,
+                   float offset_z, int nu, int nv, float du, float dv, float offset_u, float offset_v, float sad,
+                   float add, float sdd, int noviews, const double *betas, const float *couchz, int detector_type,
+                   float *image, const float *proj, const bool *map);
+
+/* Replaces cbct_proj_tf_gpu (geom/sf_cuda/cbct_sf_proj.c:443) and the CPU cbct_proj_tf
+ * (geom/cbct/cbct_proj.c:464-489): separable-footprint (trapezoid/rectangle) forward projection. */
+bool ctsim_proj_tf(int nx, int ny, int nz, float dx, float dy, float dz, float offset_x, float offset_y,
+                   float offset_z, int nu, int nv, float du, float dv, float offset_u, float offset_v, float sad,
+                   float add, float sdd, int noviews, const double *betas, const float *couchz, int detector_type,
+                   const float *image, float *proj, const bool *map);
+
+/* Replaces cbct_back_tf_gpu (geom/sf_cuda/cbct_sf_back.c:334) and the CPU cbct_back_tf
+ * (geom/cbct/cbct_back.c:375-400): matched separable-footprint backprojection. */
+bool ctsim_back_tf(int nx, int ny, int nz, float dx, float dy, float dz, float offset_x, float offset_y,
+                   float offset_z, int nu, int nv, float du, float dv, float offset_u, float offset_v, float sad,
+                   float add, float sdd, int noviews, const double *betas, const float *couchz, int detector_type,
+                   float *image, const float *proj, const bool *map);
+
+/* Replaces cbct_back_pd_gpu (geom/fdk_cuda/cbct_back_pd.c:230-256) and the CPU cbct_back_pd
+ * (geom/cbct/cbct_back.c:7-33): voxel-driven bilinear FDK backprojection.
+ * offBoundary true = "back,pd" (rows off the detector dropped),
+ * false = "back,hpd" (v clamped to [0.5, nv-1.5]). */
+bool ctsim_back_pd(int nx, int ny, int nz, float dx, float dy, float dz, float offset_x, float offset_y,
+                   float offset_z, int nu, int nv, float du, float dv, float offset_u, float offset_v, float sad,
+                   float add, float sdd, int noviews, const double *betas, const float *couchz, int detector_type,
+                   float *image, const float *proj, const bool *map, bool offBoundary);
+
+/* String dispatch of the reference gateway (geom/cbct/cbct_geom_mex.c:253-312): type is one of
+ * "proj,dd" "proj,tf" "back,dd" "back,tf" "back,pd" "back,hpd"; data is the image for "proj,*"
+ * and the sinogram for "back,*"; out is the sinogram or image. */
+bool ctsim_cbct_geom(const char *type, int nx, int ny, int nz, float dx, float dy, float dz, float offset_x,
+                     float offset_y, float offset_z, int nu, int nv, float du, float dv, float offset_u,
+                     float offset_v, float sad, float add, float sdd, int noviews, const double *betas,
+                     const float *couchz, int detector_type, const float *data, float *out, const bool *map);
+
+/* ---------------------------------------------------------------------------
+ * Family 2: device-resident plans.
+ * ------------------------------------------------------------------------- */
+
+typedef struct ctsim_plan ctsim_plan;
+
+/* Geometry scalars in the reference's MEX order. */
+typedef struct {
+    int nx, ny, nz;
+    float dx, dy, dz;
+    float offset_x, offset_y, offset_z;
+    int nu, nv;
+    float du, dv;
+    float offset_u, offset_v;
+    float sad, add, sdd;
+    int noviews;
+    int detector_type;
+} ctsim_geom;
+
+/* Create a plan on the current CUDA device.  betas/couchz/map are HOST arrays
+ * (map may be NULL = all columns on).  The plan allocates its view tables and
+ * scratch once; projector calls on it allocate nothing. */
+ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *betas, const float *couchz,
+                               const bool *map, ctsim_plan **plan);
+ctsim_status ctsim_plan_destroy(ctsim_plan *plan);
+
+/* Bytes of device memory the plan holds (tables + scratch). */
+size_t ctsim_plan_device_bytes(const ctsim_plan *plan);
+
+/* Forward projection of views [view_begin, view_begin + view_count*view_stride) with
+ * stride view_stride (ordered subsets: begin = isub % M, stride = M).  d_proj receives
+ * view_count views, contiguous [view_count][nu][nv].  method: CTSIM_PROJ_DD / CTSIM_PROJ_TF. */
+ctsim_status ctsim_plan_project(ctsim_plan *plan, int method, const float *d_image, float *d_proj,
+                                int view_begin, int view_stride, int view_count, void *stream);
+
+/* Backprojection of view_count views read contiguously from d_proj (same view selection
+ * as ctsim_plan_project).  The image is overwritten with (scale * A^T y); map-off columns are 0.
+ * method: CTSIM_BACK_DD / CTSIM_BACK_TF / CTSIM_BACK_PD / CTSIM_BACK_HPD. */
+ctsim_status ctsim_plan_backproject(ctsim_plan *plan, int method, const float *d_proj, float *d_image,
+                                    int view_begin, int view_stride, int view_count, float scale, void *stream);
+
+/* Synchronous: waits for the device and reports whether any kernel on this plan met a
+ * footprint larger than its buffers (a device-side flag; never expected for a valid plan). */
+ctsim_status ctsim_plan_check(ctsim_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CTSIM_B200_H */

@@ -1,0 +1,112 @@
+"""ctypes bindings to the oracle libraries (TEST INFRASTRUCTURE ONLY).
+
+* ``oracle_cbct``  -> this project's CPU restatement, ``_build/libcbct_oracle.so``
+* ``ref_cbct``     -> the reference's own geom/cbct C, ``_ref/libcbct_ref.so``
+                      (single-threaded, or over view chunks with ``nthreads``)
+
+Both take and return numpy arrays in the package conventions
+(image ``[nz, ny, nx]``, sino ``[noViews, nu, nv]``, float32).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libcbct_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libcbct_ref.so")
+
+KINDS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3,
+         "back,pd": 4, "back,hpd": 5, "back,var": 6}
+
+_f = C.c_float
+_i = C.c_int
+_p = C.c_void_p
+_GEOM_ARGS = [_i, _i, _i, _f, _f, _f, _f, _f, _f, _i, _i, _f, _f, _f, _f, _f, _f, _f, _i, _p, _p, _i, _p, _p, _p]
+
+_libs = {}
+
+
+def build():
+    """Build the oracle libraries (make -C oracle)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load(path):
+    if path not in _libs:
+        if not os.path.exists(path):
+            build()
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        lib = C.CDLL(path)
+        if path == ORACLE_SO:
+            lib.orc_proj.argtypes = [_i] + _GEOM_ARGS
+            lib.orc_back.argtypes = [_i] + _GEOM_ARGS
+            lib.orc_back_pd.argtypes = _GEOM_ARGS + [_i]
+            for fn in (lib.orc_proj, lib.orc_back, lib.orc_back_pd):
+                fn.restype = _i
+        else:
+            lib.ref_cbct_call.argtypes = [_i] + _GEOM_ARGS
+            lib.ref_cbct_call.restype = _i
+            lib.ref_cbct_call_mt.argtypes = [_i, _i] + _GEOM_ARGS
+            lib.ref_cbct_call_mt.restype = _i
+        _libs[path] = lib
+    return _libs[path]
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def _prep(kind, geom, data):
+    if kind not in KINDS:
+        raise ValueError(f"unknown geom type {kind!r}")
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    if kind.startswith("proj"):
+        if data.shape != geom.image_shape:
+            raise ValueError("image must have shape (nz, ny, nx)")
+        out = np.zeros(geom.sino_shape, dtype=np.float32)
+    else:
+        if data.shape != geom.sino_shape:
+            raise ValueError("sinogram must have shape (noViews, nu, nv)")
+        out = np.zeros(geom.image_shape, dtype=np.float32)
+    betas = np.ascontiguousarray(geom.betas, dtype=np.float64)
+    couch = np.ascontiguousarray(geom.couchZ, dtype=np.float32)
+    mp = np.ascontiguousarray(geom.map, dtype=np.bool_)
+    tail = (betas.ctypes.data, couch.ctypes.data, int(geom.flatPanel), data.ctypes.data, out.ctypes.data,
+            mp.ctypes.data)
+    keep = (data, betas, couch, mp)
+    return data, out, tuple(geom.scalars()) + tail, keep
+
+
+def oracle_cbct(kind: str, geom, data) -> np.ndarray:
+    """Run this project's CPU restatement of one reference projector."""
+    lib = _load(ORACLE_SO)
+    data, out, args, keep = _prep(kind, geom, data)
+    if kind.startswith("proj"):
+        ok = lib.orc_proj(KINDS[kind], *args)
+    elif kind in ("back,dd", "back,tf"):
+        ok = lib.orc_back(KINDS[kind] - 2, *args)
+    elif kind in ("back,pd", "back,hpd"):
+        ok = lib.orc_back_pd(*args, 1 if kind == "back,pd" else 0)
+    else:
+        raise NotImplementedError(kind)
+    if not ok:
+        raise RuntimeError("oracle call failed")
+    return out
+
+
+def ref_cbct(kind: str, geom, data, nthreads: int = 1) -> np.ndarray:
+    """Run the reference's own compiled geom/cbct projector (needs _ref/libcbct_ref.so)."""
+    lib = _load(REF_SO)
+    data, out, args, keep = _prep(kind, geom, data)
+    if nthreads <= 1:
+        ok = lib.ref_cbct_call(KINDS[kind], *args)
+    else:
+        ok = lib.ref_cbct_call_mt(int(nthreads), KINDS[kind], *args)
+    if not ok:
+        raise RuntimeError("reference call failed")
+    return out

@@ -1,0 +1,41 @@
+"""Generate the golden fixtures from the reference's own compiled C.
+
+Runs every case of tests/cases.py through the reference's geom/cbct projectors
+(built unmodified by oracle/Makefile into oracle/_ref/libcbct_ref.so) and saves
+inputs and outputs as tests/golden/<case>.npz.  Needs the reference checkout
+only when the library has to be built.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+from cases import KINDS, case_inputs, make_cases  # noqa: E402
+from oracle.bindings import build, ref_available, ref_cbct  # noqa: E402
+
+
+def main():
+    if not ref_available():
+        build()
+    for name, g in make_cases().items():
+        x, y = case_inputs(g)
+        out = {"image_in": x, "sino_in": y, "betas": g.betas, "couchZ": g.couchZ, "map": g.map}
+        for k in KINDS:
+            src = x if k.startswith("proj") else y
+            out[k.replace(",", "_")] = ref_cbct(k, g, src)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(path, os.path.getsize(path))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,78 @@
+"""The oracle is pinned before it is trusted.
+
+* against the golden fixtures (outputs of the reference's own compiled C,
+  tests/golden/make_golden.py): bit-identical;
+* against the reference library itself on fresh seeded inputs, where it is
+  available (oracle/_ref): bit-identical;
+* a planted mistake in the oracle's inputs is caught (the comparison is live).
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from cases import KINDS, case_inputs, make_cases
+from oracle.bindings import oracle_cbct, ref_available, ref_cbct
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+CASES = make_cases()
+
+
+def test_golden_fixtures_present():
+    names = {os.path.basename(p)[:-4] for p in GOLDEN}
+    assert names == set(CASES), "regenerate with tests/golden/make_golden.py"
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
+def test_oracle_matches_golden(path):
+    name = os.path.basename(path)[:-4]
+    g = CASES[name]
+    d = np.load(path)
+    assert np.array_equal(d["betas"], g.betas) and np.array_equal(d["map"], g.map)
+    for k in KINDS:
+        src = d["image_in"] if k.startswith("proj") else d["sino_in"]
+        got = oracle_cbct(k, g, src)
+        assert np.array_equal(got, d[k.replace(",", "_")]), f"{name} {k}: oracle differs from the reference output"
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("name", ["basic", "offsets_curved", "couch_map", "thick_slices"])
+def test_oracle_matches_reference_library(name):
+    g = CASES[name]
+    x, y = case_inputs(g, seed=7)
+    for k in KINDS:
+        src = x if k.startswith("proj") else y
+        assert np.array_equal(oracle_cbct(k, g, src), ref_cbct(k, g, src)), k
+
+
+def test_planted_mistake_is_detected():
+    g = CASES["basic"]
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "basic.npz"))
+    x = d["image_in"].copy()
+    x[3, 4, 5] += 0.25  # planted on the CPU, in the oracle's input
+    assert not np.array_equal(oracle_cbct("proj,dd", g, x), d["proj_dd"])
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference library not built")
+def test_reference_threaded_harness_matches_single_thread():
+    g = CASES["couch_map"]
+    x, y = case_inputs(g, seed=3)
+    a = ref_cbct("proj,dd", g, x)
+    b = ref_cbct("proj,dd", g, x, nthreads=4)
+    assert np.array_equal(a, b)  # disjoint view slices: identical
+    a = ref_cbct("back,tf", g, y)
+    b = ref_cbct("back,tf", g, y, nthreads=4)
+    assert np.allclose(a, b, rtol=1e-5, atol=1e-6)  # per-thread images summed: reassociated
+
+
+def test_oracle_adjointness():
+    """<A x, y> == <x, A^T y> for the oracle's DD and SF pairs (FP64 dot products)."""
+    g = CASES["basic"]
+    x, y = case_inputs(g, seed=11)
+    for f, b in (("proj,dd", "back,dd"), ("proj,tf", "back,tf")):
+        ax = oracle_cbct(f, g, x).astype(np.float64)
+        aty = oracle_cbct(b, g, y).astype(np.float64)
+        lhs = float(np.sum(ax * y))
+        rhs = float(np.sum(x.astype(np.float64) * aty))
+        assert abs(lhs - rhs) / abs(lhs) < 1e-6
