@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""Benchmark: distance-driven cone-beam A and A^T on one B200.
+
+Workload (default): the full-size plain reconstruction geometry -- volume
+512x512x256 at 0.5 mm (seeded ellipsoid phantom), 720 views over 2 pi, flat
+detector 1024x384 at 0.8 mm, SAD 1000 mm, SDD 1500 mm.  One step = one
+distance-driven forward projection A x plus one matched backprojection A^T y
+(y = log-transformed Poisson data).  Metric: GVoxel-views/s = 2 * nx*ny*nz*views
+per step / time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: the projector does not exchange data between GPUs (replicas only):
+every rank runs the same workload on its own GPU; the time is the max over
+ranks and ``value`` counts the work of all ranks.
+
+``--impl reference`` times the reference's own CPU C (geom/cbct, compiled
+unmodified into oracle/_ref) over all host cores on a bounded sample of views
+of the same workload (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GVoxel-views/s for DD A and A^T"
+UNIT = "GVoxel-views/s"
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per launch recorded from an ncu capture (profiles/*.txt line 'traffic_bytes_per_launch <k> <n>')."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith(".txt"):
+            continue
+        with open(os.path.join(pdir, fn)) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+                    return float(parts[2])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        import torch
+        uuid = None
+        try:
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(self.dev).uuid)
+        except Exception:
+            pass
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+        if uuid:
+            cmd += ["-i", uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        mhz, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [s.strip() for s in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(mhz)) if mhz else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def make_workload(views: int = 0):
+    """The benchmark workload; ``views`` > 0 keeps every (720/views)-th view (profiling captures)."""
+    from dataclasses import replace
+    from ctsim_b200.phantom import config2, to_projector_units
+    g, x_mm = config2(seed=2)
+    if views:
+        s = max(1, g.noViews // views)
+        g = replace(g, betas=g.betas[::s][:views].copy(), couchZ=g.couchZ[::s][:views].copy())
+    return g, to_projector_units(x_mm)
+
+
+def cpu_reference_sample(g, x, y, seconds_hint=True):
+    """Time the reference C (all host cores) on a bounded sample of the workload's views."""
+    from oracle.bindings import ref_available, ref_cbct, oracle_cbct
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    nxyz = g.nx * g.ny * g.nz
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 16 << 30
+    # the threaded backprojection keeps one image per thread
+    threads = max(1, min(ncores, int(avail * 0.5 // (nxyz * 4))))
+    nviews = threads
+    gs = g.subset(1, 0)
+    from dataclasses import replace
+    gs = replace(g, betas=g.betas[:: g.noViews // nviews][:nviews].copy(),
+                 couchZ=g.couchZ[:: g.noViews // nviews][:nviews].copy())
+    ys = np.ascontiguousarray(y[:: g.noViews // nviews][:nviews])
+    if ref_available():
+        kind = "reference"
+        t0 = time.perf_counter()
+        ref_cbct("proj,dd", gs, x, nthreads=threads)
+        ref_cbct("back,dd", gs, ys, nthreads=threads)
+        dt = time.perf_counter() - t0
+    else:  # the oracle port, single-threaded, one view
+        kind, threads = "port", 1
+        gs = replace(gs, betas=gs.betas[:1].copy(), couchZ=gs.couchZ[:1].copy())
+        ys = ys[:1]
+        t0 = time.perf_counter()
+        oracle_cbct("proj,dd", gs, x)
+        oracle_cbct("back,dd", gs, ys)
+        dt = time.perf_counter() - t0
+    vv = 2.0 * nxyz * gs.noViews
+    return {"value": vv / dt / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"DD A then A^T of {gs.noViews} of the {g.noViews} views on the full "
+                      f"{g.nx}x{g.ny}x{g.nz} volume ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    rank, local, world = rank_info()
+    if rank != 0:
+        return
+    g, x = make_workload()
+    rng = np.random.default_rng(3)
+    y = rng.random(g.sino_shape, dtype=np.float32)
+    for _ in range(args.warmup):
+        cpu_reference_sample(g, x, y)
+    vals, cb = [], None
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cb = cpu_reference_sample(g, x, y)
+        vals.append(cb["value"])
+    wall = time.perf_counter() - t0
+    value = float(np.mean(vals))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "DD A + A^T, 512x512x256 @0.5mm, 720 views, flat 1024x384 @0.8mm, SAD 1000, SDD 1500",
+                       "sample": cb["sample"]},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cb["cores"], "kind": cb["kind"],
+                             "sample": cb["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    from ctsim_b200 import _lib
+    from ctsim_b200.projector import Plan
+
+    rank, local, world = rank_info()
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    g, x = make_workload(args.views)
+    vv = float(g.nx * g.ny * g.nz * g.noViews)
+    plan = Plan(g)
+    xd = torch.from_numpy(x).to(dev)
+    # log-transformed Poisson data: counts ~ Poisson(I0 exp(-A x)), y = log(I0 / max(counts, 10))
+    with torch.no_grad():
+        p = plan.project(xd, "dd")
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(1234 + rank)
+        counts = torch.poisson(1e5 * torch.exp(-p), generator=gen)
+        yd = torch.log(1e5 / torch.clamp(counts, min=10.0)).contiguous()
+        del p, counts
+    sino = torch.empty(g.sino_shape, dtype=torch.float32, device=dev)
+    img = torch.empty(g.image_shape, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        plan.project(xd, "dd", out=sino)
+        plan.backproject(yd, "dd", out=img)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    plan.check()
+
+    # timed region
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    clocks = ClockSampler(dev)
+    if dist:
+        td.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for i in range(K):
+        ev[i][0].record(stream)
+        plan.project(xd, "dd", out=sino)
+        ev[i][1].record(stream)
+        plan.backproject(yd, "dd", out=img)
+        ev[i][2].record(stream)
+    end.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        td.barrier()
+    total_ms = start.elapsed_time(end)
+    t_a = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
+    t_b = float(np.mean([e[1].elapsed_time(e[2]) for e in ev]))
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / K
+    value = 2.0 * vv * K * world / (total_ms / 1e3) / 1e9
+
+    # roofline of the dominant kernel (streaming model: every view reads the volume and writes/reads its view)
+    peak, peak_src = measured_peaks()
+    alg_bytes = g.noViews * (g.nx * g.ny * g.nz * 4 + g.nu * g.nv * 4)
+    dom, t_dom = ("proj_kernel", t_a) if t_a >= t_b else ("back_kernel", t_b)
+    achieved = alg_bytes / (t_dom / 1e3) / 1e9
+    traffic = profile_traffic(dom)
+
+    # end to end through the drop-in C ABI with pinned host buffers (H2D/D2H inside the timed region)
+    L = _lib.load()
+    h_img = torch.from_numpy(x).pin_memory()
+    h_sino_in = yd.cpu().pin_memory()
+    h_sino_out = torch.empty(g.sino_shape, dtype=torch.float32).pin_memory()
+    h_img_out = torch.empty(g.image_shape, dtype=torch.float32).pin_memory()
+    betas = np.ascontiguousarray(g.betas)
+    couch = np.ascontiguousarray(g.couchZ)
+    mp = np.ascontiguousarray(g.map)
+    sc = g.scalars()
+
+    def e2e_step():
+        ok1 = L.ctsim_proj_dd(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, h_img.data_ptr(),
+                              h_sino_out.data_ptr(), mp.ctypes.data)
+        ok2 = L.ctsim_back_dd(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, h_img_out.data_ptr(),
+                              h_sino_in.data_ptr(), mp.ctypes.data)
+        if not (ok1 and ok2):
+            raise RuntimeError(_lib.last_error())
+
+    e2e_val, e2e_s = None, None
+    if not args.no_e2e:
+        e2e_val, e2e_s = run_e2e(e2e_step, K, dist, dev, vv, world)
+    nbytes_img = g.nx * g.ny * g.nz * 4
+    nbytes_sino = g.nu * g.nv * g.noViews * 4
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_reference_sample(g, x, yd.cpu().numpy())
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+                "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "DD A + A^T, 512x512x256 @0.5mm, 720 views, flat 1024x384 @0.8mm, "
+                                       "SAD 1000, SDD 1500 (seeded 20-ellipsoid phantom, log Poisson data I0=1e5)",
+                           "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2 (268 MB volume, 1.13 GB sinogram), no flush"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": dom,
+                             "peak_source": peak_src,
+                             "model": "views*(nx*ny*nz*4 + nu*nv*4) bytes per launch"},
+                "kernels_ms": {"A (prefix+proj)": t_a, "A^T (back)": t_b},
+                "A_gvv_s": vv / (t_a / 1e3) / 1e9, "AT_gvv_s": vv / (t_b / 1e3) / 1e9,
+                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes_img + nbytes_sino,
+                        "d2h_bytes_per_step": nbytes_sino + nbytes_img,
+                        "api": "ctsim_proj_dd + ctsim_back_dd (host pointers, pinned)"},
+                "gpu_launches": 4 * K,
+                "clocks": clk,
+                "cpu_baseline": cpu}
+        if args.extras:
+            line["extras"] = extras(plan, xd, yd, sino, img, vv)
+        print(json.dumps(line), flush=True)
+    if dist:
+        td.destroy_process_group()
+
+
+def run_e2e(e2e_step, K, dist, dev, vv, world):
+    import torch
+    e2e_step()
+    ke = max(2, min(K, 5))
+    if dist:
+        import torch.distributed as td
+        td.barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / ke
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    return 2.0 * vv * world / e2e_s / 1e9, e2e_s
+
+
+def extras(plan, xd, yd, sino, img, vv):
+    """Other rows of the path on the same workload: SF pair and FDK backprojection."""
+    import torch
+    out = {}
+    for name, fn in (("SF A", lambda: plan.project(xd, "tf", out=sino)),
+                     ("SF A^T", lambda: plan.backproject(yd, "tf", out=img)),
+                     ("FDK back,hpd", lambda: plan.backproject(yd, "hpd", out=img))):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(3):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / 3
+        out[name] = {"ms": ms, "gvv_s": vv / (ms / 1e3) / 1e9}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", dest="no_cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--extras", action="store_true", help="also time SF A/A^T and FDK back,hpd")
+    ap.add_argument("--views", type=int, default=0, help="keep only this many views (profiling captures)")
+    ap.add_argument("--no-e2e", dest="no_e2e", action="store_true", help="skip the end-to-end host-buffer leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -56,7 +56,8 @@ struct ctsim_plan {
     View *d_views = nullptr;
     float *d_ampv = nullptr;
     uint8_t *d_map = nullptr;
-    float *d_xc = nullptr;  // axial prefix sums [nx*ny][nz+1] (forward projector scratch)
+    float *d_xs = nullptr;   // axial prefix sums [nx*ny][nz+1] -- forward projector scratch
+    float *d_ps = nullptr;   // sinogram scaled by ampv [noviews][nu][nv] -- backprojector scratch
     int *d_err = nullptr;
     size_t bytes = 0;
     float margin = 0.f;      // candidate window margin of the forward projector (pixels)
@@ -74,7 +75,8 @@ static void free_plan(ctsim_plan *p) {
     cudaFree(p->d_views);
     cudaFree(p->d_ampv);
     cudaFree(p->d_map);
-    cudaFree(p->d_xc);
+    cudaFree(p->d_xs);
+    cudaFree(p->d_ps);
     cudaFree(p->d_err);
     delete p;
 }
@@ -121,6 +123,14 @@ extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *
     g.v_hi = float_at_or_below((double)G.nv - 1.0 - 1e-6);
     g.v_clamp_lo = 0.5f;
     g.v_clamp_hi = (float)((double)G.nv - 1.5);
+    {
+        // RN(1/dv) (double then float: innocuous double rounding); a significand of all
+        // ones is the one case where the reciprocal-based quotient may misround
+        int ex;
+        const double m = std::frexp((double)G.dv, &ex);
+        const bool all_ones = (float)m == (float)(1.0 - std::ldexp(1.0, -24));
+        g.rdv = all_ones ? 0.0f : (float)(1.0 / (double)G.dv);
+    }
 
     // per-view table, geom/cbct/cbct_proj.c:256-265, cbct_back.c:47-52
     std::vector<View> views(G.noviews);
@@ -173,14 +183,16 @@ extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *
     const double stretch = G.detector_type == 1 ? 1.0 + (umm / G.sdd) * (umm / G.sdd) : 1.0;
     p->margin = (float)std::ceil(0.5 * diag * G.sdd / dmin / G.du * stretch) + 2.0f;
     if (p->zinc_max > 9.0f) {
+        // the kernels integrate the axial footprint exactly; the reference truncates
+        // footprints wider than 10 rows (cbct_proj.c:395), which they do not reproduce
         p->fwd_ok = false;
-        p->fwd_reason = "forward projection needs every voxel's axial footprint within 10 detector rows (dz/dv*SDD/dist <= 9)";
+        p->fwd_reason = "distance-driven/separable-footprint projectors need every voxel's axial footprint within 10 detector rows (dz/dv*SDD/dist <= 9)";
     }
     if (G.nx > proj_max_lines() || G.ny > proj_max_lines()) {
         p->fwd_ok = false;
         p->fwd_reason = "forward projection supports nx, ny <= 2048";
     }
-    if (proj_smem_bytes(G.nv) > 190 * 1024) {
+    if (proj_smem_bytes(G.nv, G.nx, G.ny) > 200 * 1024) {
         p->fwd_ok = false;
         p->fwd_reason = "forward projection supports nv <= 6080";
     }
@@ -189,8 +201,10 @@ extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *
         int mz = std::min(8, pow2_at_least((G.nz + 31) / 32));
         int qcap = 0;
         for (;; mz >>= 1) {
-            qcap = std::min(G.nv, (int)std::ceil(32.0 * mz * p->zinc_max) + 3);
-            if ((size_t)8 * qcap * sizeof(float) <= 200 * 1024 || mz == 1) break;
+            // rows of one z pass (+2 partial rows, +3 for the 4-row alignment), in 128-row passes
+            const int rows = std::min(G.nv, (int)std::ceil(32.0 * mz * p->zinc_max) + 2) + 4;
+            qcap = (rows + 127) / 128 * 128;
+            if (back_smem_bytes(qcap) <= 200 * 1024 || mz == 1) break;
         }
         p->back_mz = mz;
         p->back_qcap = qcap;
@@ -212,7 +226,10 @@ extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *
     CTSIM_ALLOC(p->d_ampv, sizeof(float) * ampv.size());
     CTSIM_ALLOC(p->d_map, mp.size());
     CTSIM_ALLOC(p->d_err, sizeof(int));
-    if (p->fwd_ok) CTSIM_ALLOC(p->d_xc, sizeof(float) * (size_t)nxy * (G.nz + 1));
+    if (p->fwd_ok) {
+        CTSIM_ALLOC(p->d_xs, sizeof(float) * (size_t)nxy * (G.nz + 1));
+        CTSIM_ALLOC(p->d_ps, sizeof(float) * (size_t)G.nu * G.nv * G.noviews);
+    }
 #undef CTSIM_ALLOC
     p->bytes = bytes;
     if ((e = cudaMemcpy(p->d_views, views.data(), sizeof(View) * G.noviews, cudaMemcpyHostToDevice)) != cudaSuccess ||
@@ -248,9 +265,9 @@ extern "C" ctsim_status ctsim_plan_project(ctsim_plan *p, int method, const floa
     if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
     cudaStream_t st = (cudaStream_t)stream;
     const int nxy = p->g.nx * p->g.ny;
-    cudaError_t e = launch_prefix(d_image, p->d_xc, nxy, p->g.nz, st);
+    cudaError_t e = launch_prefix(d_image, p->d_xs, nxy, p->g.nz, st);
     if (e != cudaSuccess) return cuda_fail(e, "prefix kernel");
-    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->g, p->d_views, p->d_xc, p->d_ampv, p->d_map, d_proj,
+    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
                     view_begin, view_stride, view_count, p->margin, st);
     if (e != cudaSuccess) return cuda_fail(e, "forward projection kernel");
     return CTSIM_OK;
@@ -266,10 +283,15 @@ extern "C" ctsim_status ctsim_plan_backproject(ctsim_plan *p, int method, const 
     cudaError_t e;
     switch (method) {
     case CTSIM_BACK_DD:
-    case CTSIM_BACK_TF:
-        e = launch_back(method == CTSIM_BACK_DD ? kDD : kTF, p->back_mz, p->g, p->d_views, d_proj, p->d_ampv,
-                        p->d_map, d_image, view_begin, view_stride, view_count, scale, p->back_qcap, p->d_err, st);
+    case CTSIM_BACK_TF: {
+        if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
+        const size_t nuv = (size_t)p->g.nu * p->g.nv;
+        e = launch_prescale(d_proj, p->d_ampv, p->d_ps, nuv, nuv * view_count, st);
+        if (e != cudaSuccess) return cuda_fail(e, "prescale kernel");
+        e = launch_back(method == CTSIM_BACK_DD ? kDD : kTF, p->back_mz, p->g, p->d_views, p->d_ps, p->d_map,
+                        d_image, view_begin, view_stride, view_count, scale, p->back_qcap, p->d_err, st);
         break;
+    }
     case CTSIM_BACK_PD:
     case CTSIM_BACK_HPD:
         e = launch_pd(method == CTSIM_BACK_PD, p->pd_mz, p->g, p->d_views, d_proj, p->d_map, d_image, view_begin,

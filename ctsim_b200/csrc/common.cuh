@@ -32,6 +32,7 @@ struct Geom {
     // u < 1e-6 (double) <=> u < u_lo ; u > nu-1-1e-6 (double) <=> u > u_hi (floats).
     float u_lo, u_hi, v_lo, v_hi;
     float v_clamp_lo, v_clamp_hi; // hpd clamps 0.5 and nv - 1.5 as floats (cbct_back.c:110-111)
+    float rdv;                    // RN(1/dv) for the correctly rounded division by dv, 0 = use IEEE division
 };
 
 // Per-view constants, geom/cbct/cbct_proj.c:256-265 and cbct_back.c:50-52.
@@ -47,6 +48,30 @@ __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// floor() of x in [0, 2^23) without conversion instructions (which run on the
+// narrow XU pipe): x + 2^23 rounded toward -inf has ulp 1, so its bit pattern is
+// 0x4B000000 + floor(x).  Returns the integer; *fl receives floor(x) as a float.
+constexpr float kTwo23 = 8388608.0f;
+__device__ __forceinline__ int floor_pos(float x, float *fl) {
+    const float t = __fadd_rd(x, kTwo23);
+    *fl = __fsub_rn(t, kTwo23);
+    return __float_as_int(t) - 0x4B000000;
+}
+__device__ __forceinline__ int floor_pos(float x) { return __float_as_int(__fadd_rd(x, kTwo23)) - 0x4B000000; }
+// (float)i for 0 <= i < 2^23, exact, without a conversion instruction.
+__device__ __forceinline__ float small_int_to_float(int i) { return __fsub_rn(__int_as_float(i + 0x4B000000), kTwo23); }
+
+// Correctly rounded a / d given r = RN(1/d) (Markstein): q = RN(a r), e = a - q d
+// (exact by FMA), RN(q + e r).  Valid when d's significand is not all ones and no
+// overflow/underflow occurs -- the host checks d and otherwise passes r = 0, which
+// selects the IEEE division.
+__device__ __forceinline__ float div_by(float a, float d, float r) {
+    if (r == 0.0f) return __fdiv_rn(a, d);
+    const float q = __fmul_rn(a, r);
+    const float e = __fmaf_rn(-q, d, a);
+    return __fmaf_rn(e, r, q);
+}
 
 // Footprint of one voxel column in one view.
 struct ColumnFP {
@@ -150,14 +175,14 @@ __device__ __forceinline__ float u_weight(int iu, int iumin, int iumax, float p0
         float xl = bl > p0 ? bl : p0, xr = br < p1 ? br : p1;
         if (xr > xl) {
             float a = fsub(xr, p0), b = fsub(xl, p0);
-            w = fadd(w, fdiv(fdiv(fsub(fmul(a, a), fmul(b, b)), fsub(p1, p0)), 2.0f));
+            w = fadd(w, fmul(fdiv(fsub(fmul(a, a), fmul(b, b)), fsub(p1, p0)), 0.5f));  // /2 is exact
         }
         xl = bl > p1 ? bl : p1; xr = br < p2 ? br : p2;
         if (xr > xl) w = fadd(w, fsub(xr, xl));
         xl = bl > p2 ? bl : p2; xr = br < p3 ? br : p3;
         if (xr > xl) {
             float a = fsub(xl, p3), b = fsub(xr, p3);
-            w = fadd(w, fdiv(fdiv(fsub(fmul(a, a), fmul(b, b)), fsub(p3, p2)), 2.0f));
+            w = fadd(w, fmul(fdiv(fsub(fmul(a, a), fmul(b, b)), fsub(p3, p2)), 0.5f));
         }
         return w;
     }

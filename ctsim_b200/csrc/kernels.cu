@@ -15,21 +15,26 @@ constexpr unsigned kFull = 0xffffffffu;
 
 // ---------------------------------------------------------------------------
 // A^T: one warp per voxel column, lanes along z; 8 columns (consecutive ix) per block.
-// For each view the warp forms the u-weighted detector column
-//     Q[iv] = sum_iu w_u(iu) * (proj[iu][iv] * ampv[iu][iv])
-// over the rows the column's voxels can touch, in shared memory, then every lane
-// gathers its voxels' axial footprints from Q with the reference's exact weights
-// (geom/cbct/cbct_back.c:316-359).  Accumulation over views stays in registers.
+// For each view the warp forms, in shared memory, the u-weighted detector column
+//     q[iv] = sum_iu w_u(iu) * ps[iu][iv]        (ps = proj * ampv, pre-scaled)
+// over the rows the column's voxels can touch (4 rows per lane, float4 loads), and
+// its running sum C.  The distance-driven axial weights of a voxel are the overlaps
+// of its extent [t_iz, t_iz+1] with the detector rows (geom/cbct/cbct_back.c:318-357),
+// so its value is the integral of the piecewise-constant q over that extent:
+//     F(t_iz+1) - F(t_iz),   F(t) = C[k] + (t - k - 1) q[k],  k = floor(t)
+// Adjacent voxels share their common edge (warp shuffles), so each voxel costs one
+// edge evaluation.  Accumulation over views stays in registers; no atomics.
 // ---------------------------------------------------------------------------
-template <int METHOD, int MZ>
+template <int METHOD, int MZ, bool VEC>
 __global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restrict__ views,
-                                                   const float *__restrict__ proj, const float *__restrict__ ampv,
-                                                   const uint8_t *__restrict__ map, float *__restrict__ image,
-                                                   int view_begin, int view_stride, int view_count, float scale,
-                                                   int qcap, int *__restrict__ err) {
+                                                   const float *__restrict__ ps, const uint8_t *__restrict__ map,
+                                                   float *__restrict__ image, int view_begin, int view_stride,
+                                                   int view_count, float scale, int qcap, int *__restrict__ err) {
     extern __shared__ float smem[];
+    constexpr int kWS = 17;  // row stride of the per-warp weight table (conflict-free writes)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float *Q = smem + warp * qcap;
+    float *wtab = smem + warp * (32 * kWS + 2 * qcap);   // [32 views][17] u weights of the view chunk
+    float2 *CQ = reinterpret_cast<float2 *>(wtab + 32 * kWS);  // [qcap] (running sum, q) per row
     const int tiles_x = (g.nx + 7) >> 3;
     const int iy = blockIdx.x / tiles_x;
     const int ix = (blockIdx.x % tiles_x) * 8 + warp;
@@ -37,84 +42,122 @@ __global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restric
     const size_t nxy = (size_t)g.nx * g.ny;
     const size_t nuv = (size_t)g.nu * g.nv;
     const bool on = map[iy * g.nx + ix] != 0;
+    const float fnv = (float)g.nv;
     const int zpass = 32 * MZ;
     for (int iz0 = 0; iz0 < g.nz; iz0 += zpass) {
         const int izn = min(zpass, g.nz - iz0);
-        float acc[MZ];
+        const float fz_first = (float)iz0, fz_last = (float)(iz0 + izn - 1);
+        const float fz_top = (float)(iz0 + zpass);
+        float acc[MZ], izf[MZ];
 #pragma unroll
-        for (int m = 0; m < MZ; m++) acc[m] = 0.0f;
+        for (int m = 0; m < MZ; m++) {
+            acc[m] = 0.0f;
+            izf[m] = (float)(iz0 + lane + 32 * m);
+        }
         if (on) {
             for (int k0 = 0; k0 < view_count; k0 += 32) {
                 ColumnFP my;
                 my.hit = false;
                 const int kl = k0 + lane;
                 if (kl < view_count) my = column_footprint<METHOD>(g, views[view_begin + kl * view_stride], ix, iy);
+                // lane-parallel u weights of this lane's view (geom/cbct/cbct_back.c:288-301, :549-578)
+                if (my.hit) {
+                    const int nb = my.iumax - my.iumin + 1;
+                    for (int b = 0; b < nb; b++)
+                        wtab[lane * kWS + b] = u_weight<METHOD>(my.iumin + b, my.iumin, my.iumax, my.p0, my.p1, my.p2, my.p3);
+                }
+                __syncwarp();
                 const int nk = min(32, view_count - k0);
                 for (int j = 0; j < nk; j++) {
                     if (!__shfl_sync(kFull, (int)my.hit, j)) continue;
                     const int iumin = __shfl_sync(kFull, my.iumin, j);
                     const int iumax = __shfl_sync(kFull, my.iumax, j);
-                    const float p0 = __shfl_sync(kFull, my.p0, j), p1 = __shfl_sync(kFull, my.p1, j);
-                    float p2 = 0.f, p3 = 0.f;
-                    if (METHOD == kTF) { p2 = __shfl_sync(kFull, my.p2, j); p3 = __shfl_sync(kFull, my.p3, j); }
                     const float ampu = __shfl_sync(kFull, my.ampu, j);
                     const float zinc = __shfl_sync(kFull, my.zinc, j);
                     const float vstart = __shfl_sync(kFull, my.vstart, j);
-                    // rows reachable by voxels [iz0, iz0+izn): monotone in iz
-                    float a0, b0, a1, b1;
-                    voxel_v_extent(g, vstart, zinc, iz0, a0, b0);
-                    voxel_v_extent(g, vstart, zinc, iz0 + izn - 1, a1, b1);
-                    if (!(a0 < (float)g.nv)) continue;  // whole pass above the detector
-                    const int r_lo = (int)floorf(a0);
-                    int r_hi = min((int)floorf(b1), g.nv - 1);
+                    // rows reachable by voxels [iz0, iz0+izn) (the reference's clamped extents, monotone in iz)
+                    float a0 = fadd(fadd(vstart, fmul(fz_first, zinc)), 0.5f);
+                    a0 = fmaxf(a0, 0.0f);
+                    float b1 = fadd(fadd(fadd(vstart, fmul(fz_last, zinc)), zinc), 0.5f);
+                    b1 = fminf(b1, fnv);
+                    if (!(a0 < fnv) || !(b1 >= 0.0f)) continue;
+                    const int r_lo = floor_pos(a0);
+                    int r_hi = min(floor_pos(b1), g.nv - 1);
                     if (r_lo > r_hi) continue;
-                    if (r_hi - r_lo + 1 > qcap) {
+                    const int rbase = r_lo & ~3;
+                    if (r_hi - rbase + 2 > qcap) {  // rows rbase..r_hi+1 must fit
                         if (lane == 0) atomicOr(err, 1);
-                        r_hi = r_lo + qcap - 1;
+                        r_hi = rbase + qcap - 2;
                     }
+                    // q and its running sum over rows [rbase, r_hi], 128 rows per pass
                     const int nb = iumax - iumin + 1;
-                    const float wl = lane < nb ? u_weight<METHOD>(iumin + lane, iumin, iumax, p0, p1, p2, p3) : 0.0f;
-                    const float *pv = proj + (size_t)(k0 + j) * nuv + (size_t)iumin * g.nv;
-                    const float *av = ampv + (size_t)iumin * g.nv;
-                    for (int rb = r_lo; rb <= r_hi; rb += 32) {
-                        const int r = rb + lane;
-                        const bool ok = r <= r_hi;
-                        float q = 0.0f;
-                        for (int b = 0; b < nb; b++) {
-                            const float w = __shfl_sync(kFull, wl, b);
-                            if (ok) {
-                                const size_t o = (size_t)b * g.nv + r;
-                                q = fmaf(__ldg(pv + o) * __ldg(av + o), w, q);
+                    const float *wj = wtab + j * kWS;
+                    const float *pv = ps + (size_t)(k0 + j) * nuv + (size_t)iumin * g.nv;
+                    // Rows outside [r_lo, r_hi] only shift C by a constant (below) or are never
+                    // read past (above r_hi + 1), so no row masks are needed.
+                    float carry = 0.0f;
+                    for (int c = rbase; c <= r_hi + 1; c += 128) {
+                        const int r0 = c + 4 * lane;
+                        float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f;
+                        if (r0 <= r_hi) {
+                            for (int b = 0; b < nb; b++) {
+                                const float w = wj[b];
+                                const float *pr = pv + (size_t)b * g.nv + r0;
+                                float4 p;
+                                if (VEC) {
+                                    p = __ldg(reinterpret_cast<const float4 *>(pr));
+                                } else {
+                                    p.x = __ldg(pr);
+                                    p.y = r0 + 1 < g.nv ? __ldg(pr + 1) : 0.f;
+                                    p.z = r0 + 2 < g.nv ? __ldg(pr + 2) : 0.f;
+                                    p.w = r0 + 3 < g.nv ? __ldg(pr + 3) : 0.f;
+                                }
+                                q0 = fmaf(w, p.x, q0); q1 = fmaf(w, p.y, q1);
+                                q2 = fmaf(w, p.z, q2); q3 = fmaf(w, p.w, q3);
                             }
                         }
-                        if (ok) Q[r - r_lo] = q;
+                        const float s1 = q0 + q1, s2 = s1 + q2, s3 = s2 + q3;
+                        float incl = s3;
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const float n = __shfl_up_sync(kFull, incl, o);
+                            if (lane >= o) incl += n;
+                        }
+                        const float base = carry + (incl - s3);
+                        float4 *dst = reinterpret_cast<float4 *>(CQ + (r0 - rbase));
+                        dst[0] = make_float4(base + q0, q0, base + s1, q1);
+                        dst[1] = make_float4(base + s2, q2, base + s3, q3);
+                        carry += __shfl_sync(kFull, incl, 31);
                     }
                     __syncwarp();
+                    // F at every voxel edge t = vstart + 0.5 + iz*zinc, clamped to the covered rows
+                    const float fr_lo = small_int_to_float(r_lo);
+                    const float fr_top = small_int_to_float(r_hi + 1);
+                    const float vs_half = vstart + 0.5f;
+                    const float2 *cqb = CQ - rbase;
+                    auto edge = [&](float izv) -> float {
+                        // F(t) = C[k] - (k + 1 - t) q[k] with k = floor(t); at t = r_hi + 1 the row
+                        // r_hi + 1 entry gives C[r_hi] exactly
+                        const float t = fminf(fmaxf(fmaf(izv, zinc, vs_half), fr_lo), fr_top);
+                        const float tt = __fadd_rd(t, kTwo23);
+                        const int k = __float_as_int(tt) - 0x4B000000;
+                        const float2 cq = cqb[k];
+                        return fmaf(t - (tt - (kTwo23 - 1.0f)), cq.y, cq.x);
+                    };
+                    float Fl[MZ];
+#pragma unroll
+                    for (int m = 0; m < MZ; m++) Fl[m] = edge(izf[m]);
+                    const float Ftop = edge(fz_top);
 #pragma unroll
                     for (int m = 0; m < MZ; m++) {
-                        const int dz = lane + 32 * m;
-                        if (dz < izn) {
-                            float vmin, vmax;
-                            voxel_v_extent(g, vstart, zinc, iz0 + dz, vmin, vmax);
-                            if (!(vmin > vmax)) {
-                                const int lo = (int)floorf(vmin);
-                                const int hi = min(min(min((int)floorf(vmax), g.nv - 1), lo + kMaxRowsV - 1), r_hi);
-                                if (lo <= hi) {
-                                    float val;
-                                    if (lo == hi) {
-                                        val = fsub(vmax, vmin) * Q[lo - r_lo];
-                                    } else {
-                                        val = fsub((float)(lo + 1), vmin) * Q[lo - r_lo];
-                                        for (int r = lo + 1; r < hi; r++) val += Q[r - r_lo];
-                                        val = fmaf(fsub(vmax, (float)hi), Q[hi - r_lo], val);
-                                    }
-                                    acc[m] = fmaf(ampu, val, acc[m]);
-                                }
-                            }
-                        }
+                        float Fh = __shfl_down_sync(kFull, Fl[m], 1);
+                        const float nxt = __shfl_sync(kFull, m + 1 < MZ ? Fl[m + 1 < MZ ? m + 1 : m] : Ftop, 0);
+                        if (lane == 31) Fh = (m + 1 < MZ) ? nxt : Ftop;
+                        acc[m] = fmaf(ampu, Fh - Fl[m], acc[m]);
                     }
                     __syncwarp();
                 }
+                __syncwarp();
             }
         }
 #pragma unroll
@@ -125,20 +168,29 @@ __global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restric
     }
 }
 
+// ps = proj * ampv (the axial amplitude the reference applies to the backprojected
+// view in place, geom/cbct/cbct_back.c:196-214), into scratch.
+__global__ void prescale_kernel(const float *__restrict__ proj, const float *__restrict__ ampv,
+                                float *__restrict__ ps, size_t nuv, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        ps[i] = proj[i] * ampv[i % nuv];
+}
+
 // ---------------------------------------------------------------------------
 // Axial prefix sums of every voxel column (input of the forward projector):
-//   xc[col*(nz+1) + k] = sum_{j<k} image[j][col],  col = iy*nx + ix.
-// 32 columns per block; a 32x32 tile is transposed through shared memory so that
-// both the image reads and the prefix writes are coalesced.
+//   xc[col*(nz+1) + k] = sum_{j<k} image[j][col],  col = iy*nx + ix,  k = 0..nz,
+// so that X(s) = xc[k] + (s - k)(xc[k+1] - xc[k]) integrates the column up to axial
+// position s.  32 columns per block; a 32x32 tile is transposed through shared memory
+// so that the image reads and the prefix writes are coalesced.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) prefix_kernel(const float *__restrict__ image, float *__restrict__ xc, int nxy,
-                                                     int nz) {
+__global__ void __launch_bounds__(256) prefix_kernel(const float *__restrict__ image, float *__restrict__ xc,
+                                                     int nxy, int nz) {
     __shared__ float tile[32][33];
     __shared__ float carry[32];
     const int c0 = blockIdx.x * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-    if (threadIdx.x < 32) carry[threadIdx.x] = 0.0f;
     const size_t stride = (size_t)nz + 1;
+    if (threadIdx.x < 32) carry[threadIdx.x] = 0.0f;
     for (int z0 = 0; z0 < nz; z0 += 32) {
         __syncthreads();
         for (int zz = ty; zz < 32; zz += 8) {
@@ -149,7 +201,6 @@ __global__ void __launch_bounds__(256) prefix_kernel(const float *__restrict__ i
         // warp ty scans columns ty, ty+8, ty+16, ty+24 along z (lane = z)
         for (int cc = ty; cc < 32; cc += 8) {
             float v = tile[tx][cc];
-            // sequential-order inclusive scan (Hillis-Steele gives the same rounding for all columns)
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const float n = __shfl_up_sync(kFull, v, o);
@@ -166,43 +217,67 @@ __global__ void __launch_bounds__(256) prefix_kernel(const float *__restrict__ i
     if (threadIdx.x < 32 && c0 + threadIdx.x < nxy) xc[(size_t)(c0 + threadIdx.x) * stride] = 0.0f;
 }
 
-// ---------------------------------------------------------------------------
-// A: one block per (group of kTU detector columns, view).  Candidate voxel columns
-// are enumerated line by line (lines across the ray direction; the projected
-// column centre is monotone along a line, so the candidates of a line form one
-// interval found by binary search).  Each candidate's footprint is evaluated
-// exactly; a thread owns detector rows and adds
-//     w_u(iu) * ampu * zinc * (X(iv+1) - X(iv))
-// where X is the linear interpolation of the column's axial prefix sums at the
-// row boundaries -- the integral form of the distance-driven axial weights
-// (geom/cbct/cbct_proj.c:382-420).  Accumulators are thread-private shared-memory
-// cells: no atomics, deterministic.
-// ---------------------------------------------------------------------------
 constexpr int kTU = 8;
-constexpr int kProjThreads = 256;
+constexpr int kProjMaxThreads = 256;
 constexpr int kMaxLines = 2048;
 
+// X(s): integral of a voxel column from its bottom edge to axial position s
+// (in voxels, clamped to [0, nz]) from its prefix sums.
+__device__ __forceinline__ float column_integral(const float *__restrict__ x, float s, int nzm1, float fnzm1) {
+    float fl;
+    int k = floor_pos(s, &fl);
+    if (k > nzm1) { k = nzm1; fl = fnzm1; }
+    const float a = __ldg(x + k), b = __ldg(x + k + 1);
+    return fmaf(s - fl, b - a, a);
+}
+
+// Dynamic shared-memory layout of proj_kernel.
+struct ProjSmem {
+    int nq, nt, nlines;
+    __host__ __device__ size_t acc_bytes() const { return (size_t)kTU * nq * 16; }
+    __host__ __device__ size_t bytes() const {
+        return acc_bytes() + (size_t)nt * (6 + kTU) * 4 + (size_t)(2 * nlines + 1 + 32) * 4;
+    }
+};
+
+// A: one block per (group of kTU detector columns, view).  Candidate voxel columns
+// are enumerated line by line (lines across the ray direction; the projected column
+// centre is monotone along a line, so a line's candidates form one interval found by
+// binary search).  Each candidate's footprint is evaluated exactly.  Thread t owns
+// detector rows 4t..4t+3 and adds, for every candidate hitting its group,
+//     w_u(iu) * ampu * zinc * (X(iv+1) - X(iv))
+// -- the integral form of the distance-driven axial weights
+// (geom/cbct/cbct_proj.c:382-420) -- into float4 shared-memory accumulators that only
+// it touches: no atomics, deterministic.
 template <int METHOD>
-__global__ void __launch_bounds__(kProjThreads) proj_kernel(Geom g, const View *__restrict__ views,
-                                                            const float *__restrict__ xc,
-                                                            const float *__restrict__ ampv,
-                                                            const uint8_t *__restrict__ map, float *__restrict__ proj,
-                                                            int view_begin, int view_stride, float margin) {
-    extern __shared__ float acc_s[];  // [kTU][nv]
-    __shared__ int line_start[kMaxLines];
-    __shared__ int line_off[kMaxLines + 1];
-    __shared__ int s_col[kProjThreads];
-    __shared__ float s_b0[kProjThreads], s_iz[kProjThreads];
-    __shared__ int s_rlo[kProjThreads], s_rhi[kProjThreads], s_j[kProjThreads];
-    __shared__ float s_w[kProjThreads][kTU];
-    __shared__ int s_warp_tot[kProjThreads / 32];
+__global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const View *__restrict__ views,
+                                                               const float *__restrict__ xs,
+                                                               const float *__restrict__ ampv,
+                                                               const uint8_t *__restrict__ map,
+                                                               float *__restrict__ proj, int view_begin,
+                                                               int view_stride, float margin) {
+    extern __shared__ float4 acc4[];  // [kTU][nq] row quads, then the arrays below
+    const int NT = blockDim.x;
+    const int nq0 = (g.nv + 3) >> 2;
+    const int nlines0 = max(g.nx, g.ny);
+    int *s_col = reinterpret_cast<int *>(acc4 + kTU * nq0);
+    float *s_b0 = reinterpret_cast<float *>(s_col + NT);
+    float *s_iz = s_b0 + NT;
+    int *s_rlo = reinterpret_cast<int *>(s_iz + NT);
+    int *s_rhi = s_rlo + NT;
+    int *s_j = s_rhi + NT;
+    float *s_wf = reinterpret_cast<float *>(s_j + NT);  // [NT][kTU]
+    int *line_start = reinterpret_cast<int *>(s_wf + NT * kTU);
+    int *line_off = line_start + nlines0;
+    int *s_warp_tot = line_off + nlines0 + 1;
 
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int iu0 = blockIdx.x * kTU;
     const int k = blockIdx.y;
     const View v = views[view_begin + k * view_stride];
     const int nv = g.nv;
-    for (int i = t; i < kTU * nv; i += kProjThreads) acc_s[i] = 0.0f;
+    const int nq = (nv + 3) >> 2;
+    for (int i = t; i < kTU * nq; i += NT) acc4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 
     // lines of constant iy when the rays run mostly along y, else lines of constant ix
     const bool rows = fabsf(v.cos_a) >= fabsf(v.sin_a);
@@ -215,39 +290,34 @@ __global__ void __launch_bounds__(kProjThreads) proj_kernel(Geom g, const View *
         const float ycf = ((float)iy + g.wy) * g.dy;
         const float tp = xcf * v.cos_a - ycf * v.sin_a;
         const float ds = g.sad + xcf * v.sin_a + ycf * v.cos_a;
-        const float r = tp / ds;
+        const float r = __fdividef(tp, ds);
         return (g.det == 1 ? g.sdd_du * r : g.sdd_du * atanf(r)) - g.wu + 0.5f;
     };
 
-    // 1. candidate interval of every line
-    int my_count_total = 0;
-    for (int L = t; L < nlines; L += kProjThreads) {
+    // 1. candidate interval of every line (binary search on the monotone centre projection)
+    for (int L = t; L < nlines; L += NT) {
         auto f = [&](int p) { return rows ? centre_u(p, L) : centre_u(L, p); };
-        const float fa = f(0), fb = f(npos - 1);
-        const bool inc = fb >= fa;
-        // first position with f inside [ulo, uhi] and last one (f monotone)
-        int lo = 0, hi = npos;  // lower bound of "not before the window"
+        const bool inc = f(npos - 1) >= f(0);
+        int lo = 0, hi = npos;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
             const float fm = f(mid);
-            const bool before = inc ? (fm < ulo) : (fm > uhi);
-            if (before) lo = mid + 1; else hi = mid;
+            if (inc ? (fm < ulo) : (fm > uhi)) lo = mid + 1; else hi = mid;
         }
         const int first = lo;
-        lo = first; hi = npos;  // first position beyond the window
+        hi = npos;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
             const float fm = f(mid);
-            const bool beyond = inc ? (fm > uhi) : (fm < ulo);
-            if (beyond) hi = mid; else lo = mid + 1;
+            if (inc ? (fm > uhi) : (fm < ulo)) hi = mid; else lo = mid + 1;
         }
         line_start[L] = first;
         line_off[L] = lo - first;  // count, turned into offsets below
     }
     __syncthreads();
-    // 2. exclusive scan of the counts (lines <= kMaxLines)
+    // 2. exclusive scan of the counts
     {
-        const int per = (nlines + kProjThreads - 1) / kProjThreads;
+        const int per = (nlines + NT - 1) / NT;
         const int b = t * per, e = min(b + per, nlines);
         int sum = 0;
         for (int L = b; L < e; L++) sum += line_off[L];
@@ -268,16 +338,17 @@ __global__ void __launch_bounds__(kProjThreads) proj_kernel(Geom g, const View *
             line_off[L] = run;
             run += c;
         }
-        if (t == kProjThreads - 1) line_off[nlines] = run;
-        my_count_total = 0;
+        if (t == NT - 1) line_off[nlines] = run;
     }
     __syncthreads();
     const int ncand = line_off[nlines];
-    const size_t zstride = (size_t)g.nz + 1;
     const float fnz = (float)g.nz;
+    const int nzm1 = g.nz - 1;
+    const float fnzm1 = (float)nzm1;
+    const int rows_per_pass = 4 * NT;
 
-    for (int c0 = 0; c0 < ncand; c0 += kProjThreads) {
-        // 3. footprints of this chunk of candidates
+    for (int c0 = 0; c0 < ncand; c0 += NT) {
+        // 3. exact footprints of this chunk of candidates
         {
             const int c = c0 + t;
             bool valid = false;
@@ -300,7 +371,7 @@ __global__ void __launch_bounds__(kProjThreads) proj_kernel(Geom g, const View *
                             float w = 0.0f;
                             if (j >= jlo && j <= jhi)
                                 w = u_weight<METHOD>(iu0 + j, fp.iumin, fp.iumax, fp.p0, fp.p1, fp.p2, fp.p3) * scl;
-                            s_w[t][j] = w;
+                            s_wf[t * kTU + j] = w;
                         }
                         const float b0 = fp.vstart + 0.5f;
                         const float btop = fmaf(fnz, fp.zinc, b0);
@@ -321,29 +392,37 @@ __global__ void __launch_bounds__(kProjThreads) proj_kernel(Geom g, const View *
             if (!valid) s_j[t] = -1;
         }
         __syncthreads();
-        // 4. accumulate rows
-        const int nslot = min(kProjThreads, ncand - c0);
+        // 4. row quads: R(iv) = X(iv+1) - X(iv) from the column's prefix pairs
+        const int nslot = min(NT, ncand - c0);
         for (int s = 0; s < nslot; s++) {
             const int jj = s_j[s];
             if (jj < 0) continue;
             const int rlo = s_rlo[s], rhi = s_rhi[s];
-            const float b0 = s_b0[s], iz = s_iz[s];
-            const float *x = xc + (size_t)s_col[s] * zstride;
+            const float b0 = s_b0[s], izc = s_iz[s];
+            const float *x = xs + (size_t)s_col[s] * (g.nz + 1);
             const int jlo = jj & 0xff, jhi = jj >> 8;
-            for (int rbase = warp * 32; rbase < nv; rbase += kProjThreads) {
-                if (rbase > rhi || rbase + 31 < rlo) continue;  // warp-uniform
-                const int iv = rbase + lane;
-                // X at the row's two boundaries
-                float sl = fminf(fmaxf(((float)iv - b0) * iz, 0.0f), fnz);
-                float sh = fminf(fmaxf(((float)(iv + 1) - b0) * iz, 0.0f), fnz);
-                int kl = min((int)sl, g.nz - 1), kh = min((int)sh, g.nz - 1);
-                const float xl0 = __ldg(x + kl), xl1 = __ldg(x + kl + 1);
-                const float xh0 = __ldg(x + kh), xh1 = __ldg(x + kh + 1);
-                const float Xl = fmaf(sl - (float)kl, xl1 - xl0, xl0);
-                const float Xh = fmaf(sh - (float)kh, xh1 - xh0, xh0);
-                const float R = Xh - Xl;
-                if (iv < nv && iv >= rlo && iv <= rhi) {
-                    for (int j = jlo; j <= jhi; j++) acc_s[j * nv + iv] = fmaf(s_w[s][j], R, acc_s[j * nv + iv]);
+            for (int pbase = 0; pbase < nv; pbase += rows_per_pass) {
+                const int wrow = pbase + 128 * warp;  // first row of this warp's 128
+                if (wrow > rhi || wrow + 127 < rlo) continue;  // warp-uniform
+                const int iv0 = wrow + 4 * lane;
+                const float f0 = small_int_to_float(iv0) - b0;
+                float X0, X1, X2, X3;
+                X0 = column_integral(x, fminf(fmaxf(f0 * izc, 0.0f), fnz), nzm1, fnzm1);
+                X1 = column_integral(x, fminf(fmaxf((f0 + 1.0f) * izc, 0.0f), fnz), nzm1, fnzm1);
+                X2 = column_integral(x, fminf(fmaxf((f0 + 2.0f) * izc, 0.0f), fnz), nzm1, fnzm1);
+                X3 = column_integral(x, fminf(fmaxf((f0 + 3.0f) * izc, 0.0f), fnz), nzm1, fnzm1);
+                float X4 = __shfl_down_sync(kFull, X0, 1);
+                if (lane == 31) X4 = column_integral(x, fminf(fmaxf((f0 + 4.0f) * izc, 0.0f), fnz), nzm1, fnzm1);
+                if (iv0 <= rhi && iv0 + 3 >= rlo && iv0 < nv) {
+                    const float R0 = X1 - X0, R1 = X2 - X1, R2 = X3 - X2, R3 = X4 - X3;
+                    float4 *a = acc4 + (iv0 >> 2);
+                    for (int j = jlo; j <= jhi; j++) {
+                        const float w = s_wf[s * kTU + j];
+                        float4 r = a[j * nq];
+                        r.x = fmaf(w, R0, r.x); r.y = fmaf(w, R1, r.y);
+                        r.z = fmaf(w, R2, r.z); r.w = fmaf(w, R3, r.w);
+                        a[j * nq] = r;
+                    }
                 }
             }
         }
@@ -351,13 +430,12 @@ __global__ void __launch_bounds__(kProjThreads) proj_kernel(Geom g, const View *
     }
     // 5. axial amplitude and store
     float *out = proj + (size_t)k * g.nu * nv;
+    const float *accf = reinterpret_cast<const float *>(acc4);
     for (int j = 0; j < kTU; j++) {
         const int iu = iu0 + j;
         if (iu >= g.nu) break;
-        for (int iv = t; iv < nv; iv += kProjThreads)
-            out[(size_t)iu * nv + iv] = acc_s[j * nv + iv] * ampv[(size_t)iu * nv + iv];
+        for (int iv = t; iv < nv; iv += NT) out[(size_t)iu * nv + iv] = accf[j * 4 * nq + iv] * ampv[(size_t)iu * nv + iv];
     }
-    (void)my_count_total;
 }
 
 // ---------------------------------------------------------------------------
@@ -388,7 +466,7 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
 #pragma unroll
         for (int m = 0; m < MZ; m++) {
             acc[m] = 0.0f;
-            zc0[m] = fmul(fadd((float)(iz0 + lane + 32 * m), g.wz_pd), g.dz);
+            zc0[m] = fmul(fadd((float)(iz0 + lane + 32 * m), g.wz_pd), g.dz);  // (iz + wz) * dz, cbct_back.c:100
         }
         if (on) {
             for (int k0 = 0; k0 < view_count; k0 += 32) {
@@ -399,11 +477,11 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
                     const float xr = fsub(fmul(xc, v.cos_a), fmul(yc, v.sin_a));
                     const float yr = fadd(fmul(xc, v.sin_a), fmul(yc, v.cos_a));
                     const float den = fadd(g.sad, yr);
-                    if (g.det == 1) {
+                    if (g.det == 1) {  // cbct_back.c:68-77
                         w2 = fdiv(g.sdd, den);
                         w2s = fmul(w2, w2);
                         u = fsub(fdiv(fmul(xr, w2), g.du), g.wu);
-                    } else {
+                    } else {           // cbct_back.c:78-88
                         const float xo = fsub(xr, g.roff);
                         const double at = atan((double)fdiv(xo, den));
                         u = (float)__dsub_rn(__ddiv_rn(__dmul_rn(at, (double)g.sdd), (double)g.du), (double)g.wu);
@@ -418,30 +496,33 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
                     const float w2j = __shfl_sync(kFull, w2, j);
                     const float w2sj = __shfl_sync(kFull, w2s, j);
                     const float cj = __shfl_sync(kFull, couch, j);
-                    if (uj < g.u_lo || uj > g.u_hi) continue;  // cbct_back.c:90
-                    const int iu = (int)floorf(uj);
-                    const float wul = fsub(uj, (float)iu);
+                    if (!(uj >= g.u_lo && uj <= g.u_hi)) continue;  // cbct_back.c:90
+                    float fiu;
+                    const int iu = floor_pos(uj, &fiu);
+                    const float wul = fsub(uj, fiu);
+                    const float omu = fsub(1.0f, wul);
                     const float *pv = proj + (size_t)(k0 + j) * nuv + (size_t)iu * g.nv;
 #pragma unroll
                     for (int m = 0; m < MZ; m++) {
                         if (lane + 32 * m < izn) {
                             const float zc = fadd(zc0[m], cj);
-                            float vv = fsub(fdiv(fmul(zc, w2j), g.dv), g.wv);
+                            float vv = fsub(div_by(fmul(zc, w2j), g.dv, g.rdv), g.wv);  // cbct_back.c:102
                             bool use = true;
                             if (OFF) {
-                                use = !(vv < g.v_lo) && !(vv > g.v_hi);
+                                use = vv >= g.v_lo && vv <= g.v_hi;  // cbct_back.c:105-108
                             } else {
-                                vv = vv > 0.5f ? vv : 0.5f;
+                                vv = vv > 0.5f ? vv : 0.5f;          // cbct_back.c:110-111
                                 vv = vv < g.v_clamp_hi ? vv : g.v_clamp_hi;
                             }
                             if (use) {
-                                const int iv = (int)floorf(vv);
-                                const float wvl = fsub(vv, (float)iv);
+                                float fiv;
+                                const int iv = min(floor_pos(vv, &fiv), g.nv - 2);
+                                const float wvl = fsub(vv, fiv);
                                 const float omv = fsub(1.0f, wvl);
                                 const float *p = pv + iv;
                                 const float s0 = fadd(fmul(omv, __ldg(p)), fmul(wvl, __ldg(p + 1)));
                                 const float s1 = fadd(fmul(omv, __ldg(p + g.nv)), fmul(wvl, __ldg(p + g.nv + 1)));
-                                const float val = fadd(fmul(fsub(1.0f, wul), s0), fmul(wul, s1));
+                                const float val = fadd(fmul(omu, s0), fmul(wul, s1));
                                 acc[m] = fadd(acc[m], fmul(w2sj, val));
                             }
                         }
@@ -469,52 +550,69 @@ __global__ void scale_kernel(float *__restrict__ y, size_t n, float s) {
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
-template <int METHOD, int MZ>
-static cudaError_t launch_back_mz(const Geom &g, const View *views, const float *proj, const float *ampv,
-                                  const uint8_t *map, float *image, int vb, int vs, int vc, float scale, int qcap,
-                                  int *err, cudaStream_t st) {
+size_t back_smem_bytes(int qcap) { return (size_t)8 * (32 * 17 + 2 * qcap) * sizeof(float); }
+
+template <int METHOD, int MZ, bool VEC>
+static cudaError_t launch_back_mz(const Geom &g, const View *views, const float *ps, const uint8_t *map,
+                                  float *image, int vb, int vs, int vc, float scale, int qcap, int *err,
+                                  cudaStream_t st) {
     const int blocks = g.ny * ((g.nx + 7) / 8);
-    const size_t sm = (size_t)8 * qcap * sizeof(float);
-    auto kfn = back_kernel<METHOD, MZ>;
+    const size_t sm = back_smem_bytes(qcap);
+    auto kfn = back_kernel<METHOD, MZ, VEC>;
     cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    kfn<<<blocks, 256, sm, st>>>(g, views, proj, ampv, map, image, vb, vs, vc, scale, qcap, err);
+    kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, vb, vs, vc, scale, qcap, err);
     return cudaGetLastError();
 }
 
-cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *proj, const float *ampv,
-                        const uint8_t *map, float *image, int vb, int vs, int vc, float scale, int qcap, int *err,
-                        cudaStream_t st) {
-#define CTSIM_BACK_CASE(M, Z) \
-    if (method == M && mz == Z) return launch_back_mz<M, Z>(g, views, proj, ampv, map, image, vb, vs, vc, scale, qcap, err, st);
+cudaError_t launch_prescale(const float *proj, const float *ampv, float *ps, size_t nuv, size_t n, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 32);
+    prescale_kernel<<<blocks, 256, 0, st>>>(proj, ampv, ps, nuv, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *ps, const uint8_t *map,
+                        float *image, int vb, int vs, int vc, float scale, int qcap, int *err, cudaStream_t st) {
+    const bool vec = (g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(ps) % 16) == 0;
+#define CTSIM_BACK_CASE(M, Z)                                                                                 \
+    if (method == M && mz == Z)                                                                               \
+        return vec ? launch_back_mz<M, Z, true>(g, views, ps, map, image, vb, vs, vc, scale, qcap, err, st)  \
+                   : launch_back_mz<M, Z, false>(g, views, ps, map, image, vb, vs, vc, scale, qcap, err, st);
     CTSIM_BACK_CASE(kDD, 1) CTSIM_BACK_CASE(kDD, 2) CTSIM_BACK_CASE(kDD, 4) CTSIM_BACK_CASE(kDD, 8)
     CTSIM_BACK_CASE(kTF, 1) CTSIM_BACK_CASE(kTF, 2) CTSIM_BACK_CASE(kTF, 4) CTSIM_BACK_CASE(kTF, 8)
 #undef CTSIM_BACK_CASE
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_prefix(const float *image, float *xc, int nxy, int nz, cudaStream_t st) {
+cudaError_t launch_prefix(const float *image, float *xs, int nxy, int nz, cudaStream_t st) {
     const int blocks = (nxy + 31) / 32;
-    prefix_kernel<<<blocks, 256, 0, st>>>(image, xc, nxy, nz);
+    prefix_kernel<<<blocks, 256, 0, st>>>(image, xs, nxy, nz);
     return cudaGetLastError();
 }
 
-size_t proj_smem_bytes(int nv) { return (size_t)kTU * nv * sizeof(float); }
+static int proj_threads(int nv) { return std::min(kProjMaxThreads, std::max(32, ((nv + 3) / 4 + 31) / 32 * 32)); }
+size_t proj_smem_bytes(int nv, int nx, int ny) {
+    ProjSmem L{(nv + 3) / 4, proj_threads(nv), std::max(nx, ny)};
+    return L.bytes();
+}
 int proj_group_width() { return kTU; }
 int proj_max_lines() { return kMaxLines; }
 
 cudaError_t launch_proj(int method, const Geom &g, const View *views, const float *xc, const float *ampv,
                         const uint8_t *map, float *proj, int vb, int vs, int vc, float margin, cudaStream_t st) {
-    const size_t sm = proj_smem_bytes(g.nv);
+    const size_t sm = proj_smem_bytes(g.nv, g.nx, g.ny);
     dim3 grid((g.nu + kTU - 1) / kTU, vc);
+    // one thread per 4 detector rows (up to 256 threads per block, more rows loop)
+    const int nt = proj_threads(g.nv);
     if (method == kDD) {
         cudaError_t e = cudaFuncSetAttribute(proj_kernel<kDD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        proj_kernel<kDD><<<grid, kProjThreads, sm, st>>>(g, views, xc, ampv, map, proj, vb, vs, margin);
+        proj_kernel<kDD><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, vb, vs, margin);
     } else {
         cudaError_t e = cudaFuncSetAttribute(proj_kernel<kTF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        proj_kernel<kTF><<<grid, kProjThreads, sm, st>>>(g, views, xc, ampv, map, proj, vb, vs, margin);
+        proj_kernel<kTF><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, vb, vs, margin);
     }
     return cudaGetLastError();
 }

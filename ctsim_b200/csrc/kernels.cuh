@@ -10,13 +10,16 @@
 
 namespace ctsim {
 
-cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *proj, const float *ampv,
-                        const uint8_t *map, float *image, int view_begin, int view_stride, int view_count,
-                        float scale, int qcap, int *err, cudaStream_t st);
+cudaError_t launch_prescale(const float *proj, const float *ampv, float *ps, size_t nuv, size_t n, cudaStream_t st);
 
-cudaError_t launch_prefix(const float *image, float *xc, int nxy, int nz, cudaStream_t st);
+cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *ps, const uint8_t *map,
+                        float *image, int view_begin, int view_stride, int view_count, float scale, int qcap,
+                        int *err, cudaStream_t st);
+size_t back_smem_bytes(int qcap);
 
-cudaError_t launch_proj(int method, const Geom &g, const View *views, const float *xc, const float *ampv,
+cudaError_t launch_prefix(const float *image, float *xs, int nxy, int nz, cudaStream_t st);
+
+cudaError_t launch_proj(int method, const Geom &g, const View *views, const float *xs, const float *ampv,
                         const uint8_t *map, float *proj, int view_begin, int view_stride, int view_count,
                         float margin, cudaStream_t st);
 
@@ -26,7 +29,7 @@ cudaError_t launch_pd(bool off_boundary, int mz, const Geom &g, const View *view
 
 cudaError_t launch_scale(float *y, size_t n, float s, cudaStream_t st);
 
-size_t proj_smem_bytes(int nv);
+size_t proj_smem_bytes(int nv, int nx, int ny);
 int proj_group_width();
 int proj_max_lines();
 
