@@ -21,7 +21,7 @@ METHODS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3, "back,pd": 4,
 # symbols declared in include/ctsim_b200.h
 EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd", "ctsim_proj_tf", "ctsim_back_tf",
             "ctsim_back_pd", "ctsim_cbct_geom", "ctsim_plan_create", "ctsim_plan_destroy", "ctsim_plan_device_bytes",
-            "ctsim_plan_project", "ctsim_plan_backproject", "ctsim_plan_check"]
+            "ctsim_plan_project", "ctsim_plan_backproject", "ctsim_plan_check", "ctsim_back_dd_noalloc"]
 
 
 class CtsimGeom(C.Structure):
@@ -81,6 +81,8 @@ def load():
     L.ctsim_plan_backproject.restype = _i
     L.ctsim_plan_check.argtypes = [_p]
     L.ctsim_plan_check.restype = _i
+    L.ctsim_back_dd_noalloc.argtypes = [C.POINTER(CtsimGeom), _p, _p, _p, _p, _p, _p]
+    L.ctsim_back_dd_noalloc.restype = _i
     _lib = L
     return L
 

@@ -68,6 +68,10 @@ struct ctsim_plan {
 };
 
 extern "C" const char *ctsim_last_error(void) { return g_last_error.c_str(); }
+
+// Records the calling thread's last-error message for entry points defined in other
+// translation units (noalloc.cu).
+ctsim_status ctsim_set_last_error(ctsim_status s, const char *msg) { return fail(s, msg); }
 extern "C" const char *ctsim_version(void) { return "ctsim_b200 0.1 (sm_100a)"; }
 
 static void free_plan(ctsim_plan *p) {

@@ -25,11 +25,12 @@ constexpr unsigned kFull = 0xffffffffu;
 // Adjacent voxels share their common edge (warp shuffles), so each voxel costs one
 // edge evaluation.  Accumulation over views stays in registers; no atomics.
 // ---------------------------------------------------------------------------
-template <int METHOD, int MZ, bool VEC>
+template <int METHOD, int MZ, bool VEC, bool PRESCALED = true>
 __global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restrict__ views,
                                                    const float *__restrict__ ps, const uint8_t *__restrict__ map,
                                                    float *__restrict__ image, int view_begin, int view_stride,
-                                                   int view_count, float scale, int qcap, int *__restrict__ err) {
+                                                   int view_count, float scale, int qcap, int *__restrict__ err,
+                                                   const float *__restrict__ ampv = nullptr) {
     extern __shared__ float smem[];
     constexpr int kWS = 17;  // row stride of the per-warp weight table (conflict-free writes)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -111,6 +112,13 @@ __global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restric
                                     p.y = r0 + 1 < g.nv ? __ldg(pr + 1) : 0.f;
                                     p.z = r0 + 2 < g.nv ? __ldg(pr + 2) : 0.f;
                                     p.w = r0 + 3 < g.nv ? __ldg(pr + 3) : 0.f;
+                                }
+                                if (!PRESCALED) {  // axial amplitude applied here instead of in a scratch copy
+                                    const float *ar = ampv + (size_t)(iumin + b) * g.nv + r0;
+                                    p.x *= __ldg(ar);
+                                    p.y *= r0 + 1 < g.nv ? __ldg(ar + 1) : 0.f;
+                                    p.z *= r0 + 2 < g.nv ? __ldg(ar + 2) : 0.f;
+                                    p.w *= r0 + 3 < g.nv ? __ldg(ar + 3) : 0.f;
                                 }
                                 q0 = fmaf(w, p.x, q0); q1 = fmaf(w, p.y, q1);
                                 q2 = fmaf(w, p.z, q2); q3 = fmaf(w, p.w, q3);
@@ -561,7 +569,7 @@ static cudaError_t launch_back_mz(const Geom &g, const View *views, const float 
     auto kfn = back_kernel<METHOD, MZ, VEC>;
     cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, vb, vs, vc, scale, qcap, err);
+    kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, vb, vs, vc, scale, qcap, err, nullptr);
     return cudaGetLastError();
 }
 
@@ -640,6 +648,32 @@ cudaError_t launch_scale(float *y, size_t n, float s, cudaStream_t st) {
     const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
     scale_kernel<<<blocks, 256, 0, st>>>(y, n, s);
     return cudaGetLastError();
+}
+
+// A^T reading the unscaled sinogram (axial amplitude applied on the fly); used by the
+// entry point that allocates nothing (noalloc.cu).
+template <int METHOD, int MZ>
+static cudaError_t launch_back_unscaled_mz(const Geom &g, const View *views, const float *proj, const float *ampv,
+                                           const uint8_t *map, float *image, int vc, int qcap, int *err,
+                                           cudaStream_t st) {
+    const int blocks = g.ny * ((g.nx + 7) / 8);
+    const size_t sm = back_smem_bytes(qcap);
+    auto kfn = back_kernel<METHOD, MZ, false, false>;
+    cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    kfn<<<blocks, 256, sm, st>>>(g, views, proj, map, image, 0, 1, vc, 1.0f, qcap, err, ampv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const float *proj, const float *ampv,
+                                 const uint8_t *map, float *image, int vc, int qcap, int *err, cudaStream_t st) {
+    switch (mz) {
+    case 1: return launch_back_unscaled_mz<kDD, 1>(g, views, proj, ampv, map, image, vc, qcap, err, st);
+    case 2: return launch_back_unscaled_mz<kDD, 2>(g, views, proj, ampv, map, image, vc, qcap, err, st);
+    case 4: return launch_back_unscaled_mz<kDD, 4>(g, views, proj, ampv, map, image, vc, qcap, err, st);
+    case 8: return launch_back_unscaled_mz<kDD, 8>(g, views, proj, ampv, map, image, vc, qcap, err, st);
+    }
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace ctsim

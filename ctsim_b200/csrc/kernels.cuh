@@ -16,6 +16,9 @@ cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, co
                         float *image, int view_begin, int view_stride, int view_count, float scale, int qcap,
                         int *err, cudaStream_t st);
 size_t back_smem_bytes(int qcap);
+cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const float *proj, const float *ampv,
+                                 const uint8_t *map, float *image, int view_count, int qcap, int *err,
+                                 cudaStream_t st);
 
 cudaError_t launch_prefix(const float *image, float *xs, int nxy, int nz, cudaStream_t st);
 

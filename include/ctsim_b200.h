@@ -156,6 +156,28 @@ ctsim_status ctsim_plan_backproject(ctsim_plan *plan, int method, const float *d
  * footprint larger than its buffers (a device-side flag; never expected for a valid plan). */
 ctsim_status ctsim_plan_check(ctsim_plan *plan);
 
+/* Matched distance-driven backprojection (same result as CTSIM_BACK_DD, within float
+ * rounding) that allocates no device memory.  No counterpart in the reference: its MEX
+ * back ends cudaMalloc and cudaFree on every call.
+ *
+ * For callers that must not allocate: a host framework that owns all device memory
+ * through its own pool, a serving loop with a fixed memory budget, or code that cannot
+ * afford the implicit device synchronisation of cudaMalloc/cudaFree.  d_proj
+ * ([noviews][nu][nv]) and d_image ([nz][ny][nx], overwritten) are device pointers the
+ * caller owns; betas, couchz and map (NULL = all columns on) are host arrays.
+ *
+ * Limit: the per-view table, the detector amplitude table and the map live in one
+ * fixed 8 MiB array in device memory (each GPU that loads the library holds it until
+ * the process exits); the call returns CTSIM_ERR_ARGUMENT when
+ * noviews*44 + nu*nv*4 + nx*ny bytes (each part rounded up to 256) + 256 exceed it.
+ * The first call on a device looks up that array's device address (set-up, once per
+ * device); make that first call before any stream capture.  Every call rewrites the
+ * shared array, so calls that overlap on the GPU (other streams, other host threads)
+ * race; serialise them.  Asynchronous on `stream` (the geometry copies from pageable
+ * host memory are synchronous). */
+ctsim_status ctsim_back_dd_noalloc(const ctsim_geom *geom, const double *betas, const float *couchz,
+                                   const bool *map, const float *d_proj, float *d_image, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
