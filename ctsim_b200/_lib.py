@@ -21,7 +21,10 @@ METHODS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3, "back,pd": 4,
 # symbols declared in include/ctsim_b200.h
 EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd", "ctsim_proj_tf", "ctsim_back_tf",
             "ctsim_back_pd", "ctsim_cbct_geom", "ctsim_plan_create", "ctsim_plan_destroy", "ctsim_plan_device_bytes",
-            "ctsim_plan_project", "ctsim_plan_backproject", "ctsim_plan_check", "ctsim_back_dd_noalloc"]
+            "ctsim_plan_project", "ctsim_plan_backproject", "ctsim_plan_check", "ctsim_back_dd_noalloc",
+            "ctsim_fdk_create", "ctsim_fdk_destroy", "ctsim_fdk_filter", "ctsim_fdk_run", "ctsim_fdk_dbeta",
+            "ctsim_fdk_design_filter", "ctsim_pwls_weights", "ctsim_pwls_residual", "ctsim_sqdiff",
+            "ctsim_penalty", "ctsim_sqs_update"]
 
 
 class CtsimGeom(C.Structure):
@@ -83,6 +86,29 @@ def load():
     L.ctsim_plan_check.restype = _i
     L.ctsim_back_dd_noalloc.argtypes = [C.POINTER(CtsimGeom), _p, _p, _p, _p, _p, _p]
     L.ctsim_back_dd_noalloc.restype = _i
+    L.ctsim_fdk_create.argtypes = [_p, C.c_char_p, _f, _i, C.POINTER(_p)]
+    L.ctsim_fdk_create.restype = _i
+    L.ctsim_fdk_destroy.argtypes = [_p]
+    L.ctsim_fdk_destroy.restype = _i
+    L.ctsim_fdk_filter.argtypes = [_p, _p, _p, _p]
+    L.ctsim_fdk_filter.restype = _i
+    L.ctsim_fdk_run.argtypes = [_p, _p, _p, _p]
+    L.ctsim_fdk_run.restype = _i
+    L.ctsim_fdk_dbeta.argtypes = [_p]
+    L.ctsim_fdk_dbeta.restype = _f
+    L.ctsim_fdk_design_filter.argtypes = [_i, _f, _f, _i, C.c_char_p, _f, _p, C.POINTER(_i)]
+    L.ctsim_fdk_design_filter.restype = _i
+    _sz = C.c_size_t
+    L.ctsim_pwls_weights.argtypes = [_p, _f, _f, _p, _sz, _p]
+    L.ctsim_pwls_weights.restype = _i
+    L.ctsim_pwls_residual.argtypes = [_p, _p, _p, _p, _sz, _p, _p]
+    L.ctsim_pwls_residual.restype = _i
+    L.ctsim_sqdiff.argtypes = [_p, _p, _sz, _p, _p]
+    L.ctsim_sqdiff.restype = _i
+    L.ctsim_penalty.argtypes = [_i, _i, _f, _i, _i, _i, _p, _p, _p, _p]
+    L.ctsim_penalty.restype = _i
+    L.ctsim_sqs_update.argtypes = [_i, _f, _f, _i, _i, _i, _p, _p, _p, _p, _p]
+    L.ctsim_sqs_update.restype = _i
     _lib = L
     return L
 

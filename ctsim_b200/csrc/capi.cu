@@ -65,7 +65,12 @@ struct ctsim_plan {
     int back_mz = 1, back_qcap = 0, pd_mz = 1;
     bool fwd_ok = true;
     std::string fwd_reason;
+    std::vector<double> betas;  // host copy of the view angles (FDK weights need them)
 };
+
+// Plan internals for other translation units (fdk.cu).
+const double *ctsim_plan_betas(const ctsim_plan *p) { return p->betas.data(); }
+const ctsim_geom *ctsim_plan_geom(const ctsim_plan *p) { return &p->geom; }
 
 extern "C" const char *ctsim_last_error(void) { return g_last_error.c_str(); }
 
@@ -110,6 +115,7 @@ extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *
     ctsim_plan *p = new ctsim_plan();
     p->geom = G;
     p->device = dev;
+    p->betas.assign(betas, betas + G.noviews);
     Geom &g = p->g;
     g.nx = G.nx; g.ny = G.ny; g.nz = G.nz; g.nu = G.nu; g.nv = G.nv; g.det = G.detector_type;
     g.dx = G.dx; g.dy = G.dy; g.dz = G.dz; g.sad = G.sad; g.sdd = G.sdd; g.du = G.du; g.dv = G.dv;

@@ -1,0 +1,331 @@
+// FDK reconstruction (fbp/reconFDK.m) on the device:
+//   1. cosine weight per detector pixel and, for short scans, Parker weight per
+//      (view, detector column)                                   reconFDK.m:38-60
+//   2. ramp x window filter along every detector row, by FFT with the zero padding
+//      of filterFreq.m (length max(64, 2^nextpow2(2 nu - 1)))     reconFDK.m:62-71
+//   3. back,hpd backprojection, times dbeta, times 10             reconFDK.m:78-84
+// The filter itself is built on the host by the reference's design
+// (fbp/filter/designFilter2.m flat, designEquiangularFilter2.m curved).
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ctsim_b200.h"
+#include "kernels.cuh"
+
+using namespace ctsim;
+
+extern ctsim_status ctsim_set_last_error(ctsim_status s, const char *msg);
+// plan internals shared with capi.cu
+extern const double *ctsim_plan_betas(const ctsim_plan *p);
+extern const ctsim_geom *ctsim_plan_geom(const ctsim_plan *p);
+
+namespace {
+
+constexpr int kFiltRows = 8;  // detector rows per block (4 complex FFTs)
+
+int fft_order(int nu) {
+    // order = max(64, 2^nextpow2(2*len-1)), designFilter2.m:18
+    int L = 1;
+    while (L < 2 * nu - 1) L <<= 1;
+    return L < 64 ? 64 : L;
+}
+
+bool window_known(const std::string &w) {
+    static const char *names[] = {"ram-lak", "shepp-logan", "cosine", "hamming", "hann", "hann50", "hann75",
+                                  "hann80", "B50", "B75", "B80", "C50", "C75", "C80"};
+    for (auto n : names)
+        if (w == n) return true;
+    return false;
+}
+
+// designFilter2.m:18-78 (flat) / designEquiangularFilter2.m:19-78 (curved), in double.
+// gamma = du; SDD used by the equiangular kernel.  Returns H[order].
+std::vector<double> design_filter(int nu, double du, double sdd, bool flat, const std::string &window, double crop) {
+    const int order = fft_order(nu);
+    // h over index = -order/2+1 .. order/2-1, then h(order) = 0 (zero padding)
+    std::vector<double> h(order, 0.0);
+    for (int n = 0; n < order - 1; n++) {
+        const int index = -order / 2 + 1 + n;
+        if (index == 0) {
+            h[n] = 1.0 / (4.0 * du * du);
+        } else if (((index % 2) + 2) % 2 == 1) {  // MATLAB mod(index,2)==1 (odd, either sign)
+            const double d = flat ? (index * M_PI * du) : (sdd * M_PI * std::sin(index * du / sdd));
+            h[n] = -1.0 / (d * d);
+        }
+    }
+    // filt = abs(fft(h)), first order/2+1 bins (direct DFT in double; once per plan)
+    const int half = order / 2 + 1;
+    std::vector<double> filt(half);
+    for (int k = 0; k < half; k++) {
+        double re = 0.0, im = 0.0;
+        for (int n = 0; n < order; n++) {
+            if (h[n] == 0.0) continue;
+            const double a = -2.0 * M_PI * (double)((long long)k * n % order) / order;
+            re += h[n] * std::cos(a);
+            im += h[n] * std::sin(a);
+        }
+        filt[k] = std::sqrt(re * re + im * im);
+    }
+    std::string win = window;
+    if (win == "hann50" || win == "B50" || win == "C50") crop = 0.5;
+    if (win == "hann75" || win == "B75" || win == "C75") crop = 0.75;
+    if (win == "hann80" || win == "B80" || win == "C80") crop = 0.80;
+    for (int k = 1; k < half; k++) {
+        const double w = 2.0 * M_PI * k / order;
+        if (win == "shepp-logan") filt[k] *= std::sin(w / (2 * crop)) / (w / (2 * crop));
+        else if (win == "cosine" || win == "C50" || win == "C75" || win == "C80") filt[k] *= std::cos(w / (2 * crop));
+        else if (win == "hamming") filt[k] *= 0.54 + 0.46 * std::cos(w / crop);
+        else if (win == "hann" || win == "hann50" || win == "hann75" || win == "hann80")
+            filt[k] *= (1.0 + std::cos(w / crop)) / 2.0;
+    }
+    for (int k = 0; k < half; k++)
+        if (2.0 * M_PI * k / order > M_PI * crop) filt[k] = 0.0;  // crop, designFilter2.m:77
+    // symmetric extension [filt ; filt(end-1:-1:2)]
+    std::vector<double> H(order);
+    for (int k = 0; k < half; k++) H[k] = filt[k];
+    for (int k = half; k < order; k++) H[k] = filt[order - k];
+    return H;
+}
+
+// MATLAB S-function of fbp/weights/shortScanParkerWeight.m:243-252
+double parker_s(double b) {
+    if (b <= -0.5) return 0.0;
+    if (std::fabs(b) < 0.5) return 0.5 * (1.0 + std::sin(M_PI * b));
+    return 1.0;
+}
+
+// ---------------------------------------------------------------------------
+// Row filter: block = (group of 8 detector rows, view).  Rows 2p and 2p+1 are the
+// real and imaginary parts of complex signal p (the filter is real and even, so the
+// two filtered rows come back as the real and imaginary parts).  Forward FFT:
+// radix-2 decimation in time on bit-reversed input; inverse: decimation in
+// frequency from natural order, read back bit-reversed.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) fdk_filter_kernel(const float *__restrict__ sino, float *__restrict__ out,
+                                                         const float *__restrict__ wcos,
+                                                         const float *__restrict__ parker,
+                                                         const float *__restrict__ H, const float2 *__restrict__ tw,
+                                                         int nu, int nv, int L, int log2L) {
+    extern __shared__ float2 buf[];  // [4][L]
+    const int k = blockIdx.y;
+    const int iv0 = blockIdx.x * kFiltRows;
+    const size_t nuv = (size_t)nu * nv;
+    const float *sv = sino + (size_t)k * nuv;
+    float *ov = out + (size_t)k * nuv;
+    const int t = threadIdx.x;
+    const int sh = 32 - log2L;
+    // load, weight, scatter to bit-reversed positions (zero padding beyond nu)
+    for (int i = t; i < L * kFiltRows; i += blockDim.x) {
+        const int iu = i >> 3, r = i & 7;
+        float x = 0.0f;
+        if (iu < nu && iv0 + r < nv) {
+            const size_t o = (size_t)iu * nv + iv0 + r;
+            x = sv[o] * wcos[o];  // reconFDK.m:54
+            if (parker) x = x * parker[(size_t)k * nu + iu];  // reconFDK.m:66-68
+        }
+        const int pos = __brev(iu) >> sh;
+        float *dst = reinterpret_cast<float *>(buf + (size_t)(r >> 1) * L + pos);
+        dst[r & 1] = x;
+    }
+    __syncthreads();
+    const int nb = 4 * (L >> 1);  // butterflies per stage over the 4 signals
+    // forward DIT
+    for (int s = 0; s < log2L; s++) {
+        const int half = 1 << s;
+        for (int b = t; b < nb; b += blockDim.x) {
+            const int sig = b / (L >> 1), bb = b % (L >> 1);
+            const int pos = bb & (half - 1), grp = bb >> s;
+            const int i = (grp << (s + 1)) + pos, j = i + half;
+            float2 *x = buf + (size_t)sig * L;
+            const float2 w = tw[pos << (log2L - 1 - s)];  // exp(-2 pi i pos / (2 half))
+            const float2 a = x[i], c = x[j];
+            const float2 cw = make_float2(c.x * w.x - c.y * w.y, c.x * w.y + c.y * w.x);
+            x[i] = make_float2(a.x + cw.x, a.y + cw.y);
+            x[j] = make_float2(a.x - cw.x, a.y - cw.y);
+        }
+        __syncthreads();
+    }
+    // multiply by the (real) filter
+    for (int i = t; i < 4 * L; i += blockDim.x) {
+        const float h = H[i % L];
+        float2 v = buf[i];
+        buf[i] = make_float2(v.x * h, v.y * h);
+    }
+    __syncthreads();
+    // inverse DIF (twiddles conjugated), natural in, bit-reversed out
+    for (int s = log2L - 1; s >= 0; s--) {
+        const int half = 1 << s;
+        for (int b = t; b < nb; b += blockDim.x) {
+            const int sig = b / (L >> 1), bb = b % (L >> 1);
+            const int pos = bb & (half - 1), grp = bb >> s;
+            const int i = (grp << (s + 1)) + pos, j = i + half;
+            float2 *x = buf + (size_t)sig * L;
+            const float2 w = tw[pos << (log2L - 1 - s)];
+            const float2 a = x[i], c = x[j];
+            const float2 d = make_float2(a.x - c.x, a.y - c.y);
+            x[i] = make_float2(a.x + c.x, a.y + c.y);
+            x[j] = make_float2(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y);  // d * conj(w)
+        }
+        __syncthreads();
+    }
+    const float inv = 1.0f / (float)L;
+    for (int i = t; i < nu * kFiltRows; i += blockDim.x) {
+        const int iu = i >> 3, r = i & 7;
+        if (iv0 + r >= nv) continue;
+        const int pos = __brev(iu) >> sh;
+        const float2 v = buf[(size_t)(r >> 1) * L + pos];
+        ov[(size_t)iu * nv + iv0 + r] = ((r & 1) ? v.y : v.x) * inv;
+    }
+}
+
+}  // namespace
+
+struct ctsim_fdk {
+    ctsim_plan *plan = nullptr;
+    int nu = 0, nv = 0, nviews = 0, L = 0, log2L = 0;
+    float dbeta = 0.f;
+    float *d_H = nullptr, *d_wcos = nullptr, *d_parker = nullptr, *d_filtered = nullptr;
+    float2 *d_tw = nullptr;
+};
+
+extern "C" ctsim_status ctsim_fdk_design_filter(int nu, float du, float sdd, int detector_type, const char *window,
+                                                float crop, double *H, int *order) {
+    if (!window || !window_known(window)) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "Invalid window selected.");
+    if (nu < 1 || !(du > 0) || !(sdd > 0)) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "invalid detector");
+    const int L = fft_order(nu);
+    if (order) *order = L;
+    if (H) {
+        std::vector<double> h = design_filter(nu, du, sdd, detector_type == 1, window, crop);
+        std::memcpy(H, h.data(), sizeof(double) * L);
+    }
+    return CTSIM_OK;
+}
+
+static void free_fdk(ctsim_fdk *f) {
+    if (!f) return;
+    cudaFree(f->d_H);
+    cudaFree(f->d_wcos);
+    cudaFree(f->d_parker);
+    cudaFree(f->d_filtered);
+    cudaFree(f->d_tw);
+    delete f;
+}
+
+extern "C" ctsim_status ctsim_fdk_create(ctsim_plan *plan, const char *window, float crop, int short_scan,
+                                         ctsim_fdk **out) {
+    if (!plan || !out) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    if (!window || !window_known(window)) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "Invalid window selected.");
+    const ctsim_geom &G = *ctsim_plan_geom(plan);
+    const double *betas = ctsim_plan_betas(plan);
+    const bool flat = G.detector_type == 1;
+    ctsim_fdk *f = new ctsim_fdk();
+    f->plan = plan;
+    f->nu = G.nu;
+    f->nv = G.nv;
+    f->nviews = G.noviews;
+    f->L = fft_order(G.nu);
+    while ((1 << f->log2L) < f->L) f->log2L++;
+    const double SAD = G.sad, SDD = G.sdd, du = G.du, dv = G.dv;
+    // detector coordinates u, v in mm (reconFDK.m:33-34)
+    std::vector<double> u(G.nu), v(G.nv);
+    for (int i = 0; i < G.nu; i++) u[i] = ((-(G.nu - 1) / 2.0 + i) + G.offset_u) * du;
+    for (int i = 0; i < G.nv; i++) v[i] = ((-(G.nv - 1) / 2.0 + i) + G.offset_v) * dv;
+    // cosine weight (reconFDK.m:39 flat, :44 curved), stored [iu][iv] like the sinogram
+    std::vector<float> wcos((size_t)G.nu * G.nv);
+    for (int iu = 0; iu < G.nu; iu++)
+        for (int iv = 0; iv < G.nv; iv++) {
+            double w;
+            if (flat) w = SAD * std::sqrt(1.0 + u[iu] * u[iu] / (SDD * SDD)) / std::sqrt(u[iu] * u[iu] + v[iv] * v[iv] + SDD * SDD);
+            else w = SAD / SDD * std::cos(u[iu] / std::sqrt(SDD * SDD + v[iv] * v[iv]));
+            wcos[(size_t)iu * G.nv + iv] = (float)w;
+        }
+    std::vector<double> Hd = design_filter(G.nu, du, SDD, flat, window, crop);
+    std::vector<float> H(f->L);
+    for (int i = 0; i < f->L; i++) H[i] = (float)(du * Hd[i]);  // H = du * designFilter2(...), reconFDK.m:40
+    std::vector<float2> tw(f->L / 2);
+    for (int i = 0; i < f->L / 2; i++) {
+        const double a = -2.0 * M_PI * i / f->L;
+        tw[i] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    // Parker short-scan weights (reconFDK.m:41-42, :56-60; shortScanParkerWeight.m)
+    std::vector<float> parker;
+    double bmin = betas[0], bmax = betas[0];
+    for (int k = 0; k < G.noviews; k++) {
+        bmin = std::min(bmin, betas[k]);
+        bmax = std::max(bmax, betas[k]);
+    }
+    if (short_scan) {
+        const double Tau = flat ? std::fabs(betas[G.noviews - 1] - betas[0]) - M_PI : std::fabs(bmax - bmin) - M_PI;
+        parker.resize((size_t)G.noviews * G.nu);
+        for (int k = 0; k < G.noviews; k++) {
+            const double beta = betas[k] - bmin;
+            for (int iu = 0; iu < G.nu; iu++) {
+                const double gammas = flat ? std::atan(-u[iu] / SDD) : -u[iu] / SDD;
+                const double gamma = -gammas;
+                const double w = parker_s(beta / (Tau - 2 * gamma) - 0.5) -
+                                 parker_s((beta - M_PI + 2 * gamma) / (Tau + 2 * gamma) - 0.5);
+                parker[(size_t)k * G.nu + iu] = (float)w;
+            }
+        }
+    }
+    // dbeta (reconFDK.m:78-81)
+    double dbeta = G.noviews > 1 ? std::fabs(betas[G.noviews - 1] - betas[0]) / (G.noviews - 1) : 0.0;
+    if (!short_scan) dbeta /= 2.0;
+    f->dbeta = (float)dbeta;
+
+    cudaError_t e;
+    const size_t nsino = (size_t)G.nu * G.nv * G.noviews;
+    if ((e = cudaMalloc(&f->d_H, sizeof(float) * f->L)) != cudaSuccess ||
+        (e = cudaMalloc(&f->d_wcos, sizeof(float) * wcos.size())) != cudaSuccess ||
+        (e = cudaMalloc(&f->d_tw, sizeof(float2) * tw.size())) != cudaSuccess ||
+        (e = cudaMalloc(&f->d_filtered, sizeof(float) * nsino)) != cudaSuccess ||
+        (short_scan && (e = cudaMalloc(&f->d_parker, sizeof(float) * parker.size())) != cudaSuccess)) {
+        free_fdk(f);
+        return ctsim_set_last_error(CTSIM_ERR_ALLOC, cudaGetErrorString(e));
+    }
+    if ((e = cudaMemcpy(f->d_H, H.data(), sizeof(float) * f->L, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(f->d_wcos, wcos.data(), sizeof(float) * wcos.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(f->d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (short_scan &&
+         (e = cudaMemcpy(f->d_parker, parker.data(), sizeof(float) * parker.size(), cudaMemcpyHostToDevice)) != cudaSuccess)) {
+        free_fdk(f);
+        return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
+    }
+    *out = f;
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_fdk_destroy(ctsim_fdk *f) {
+    free_fdk(f);
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_fdk_filter(ctsim_fdk *f, const float *d_sino, float *d_filtered, void *stream) {
+    if (!f || !d_sino || !d_filtered) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    const size_t sm = sizeof(float2) * 4 * f->L;
+    if (sm > 200 * 1024) return ctsim_set_last_error(CTSIM_ERR_UNSUPPORTED, "detector too wide for the row filter");
+    cudaError_t e = cudaFuncSetAttribute(fdk_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
+    dim3 grid((f->nv + kFiltRows - 1) / kFiltRows, f->nviews);
+    fdk_filter_kernel<<<grid, 256, sm, (cudaStream_t)stream>>>(d_sino, d_filtered, f->d_wcos, f->d_parker, f->d_H,
+                                                                f->d_tw, f->nu, f->nv, f->L, f->log2L);
+    if ((e = cudaGetLastError()) != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_fdk_run(ctsim_fdk *f, const float *d_sino, float *d_image, void *stream) {
+    ctsim_status s = ctsim_fdk_filter(f, d_sino, f->d_filtered, stream);
+    if (s != CTSIM_OK) return s;
+    // img = backProjectMex(sino, geom, 1, 0, 'back,hpd') * dbeta * 10  (reconFDK.m:84)
+    s = ctsim_plan_backproject(f->plan, CTSIM_BACK_HPD, f->d_filtered, d_image, 0, 1, f->nviews, f->dbeta, stream);
+    if (s != CTSIM_OK) return s;
+    const ctsim_geom &G = *ctsim_plan_geom(f->plan);
+    cudaError_t e = launch_scale(d_image, (size_t)G.nx * G.ny * G.nz, 10.0f, (cudaStream_t)stream);
+    if (e != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
+    return CTSIM_OK;
+}
+
+extern "C" float ctsim_fdk_dbeta(const ctsim_fdk *f) { return f ? f->dbeta : 0.0f; }

@@ -156,6 +156,65 @@ ctsim_status ctsim_plan_backproject(ctsim_plan *plan, int method, const float *d
  * footprint larger than its buffers (a device-side flag; never expected for a valid plan). */
 ctsim_status ctsim_plan_check(ctsim_plan *plan);
 
+/* ---------------------------------------------------------------------------
+ * FDK reconstruction (fbp/reconFDK.m) on a plan.
+ * ------------------------------------------------------------------------- */
+
+typedef struct ctsim_fdk ctsim_fdk;
+
+/* Replaces fbp/reconFDK.m:19-84 for one geometry: builds the cosine weights
+ * (reconFDK.m:38-48), the ramp x window filter of fbp/filter/designFilter2.m (flat) or
+ * designEquiangularFilter2.m (curved) with window "ram-lak" "shepp-logan" "cosine"
+ * "hamming" "hann" "hann50|75|80" "B50|75|80" "C50|75|80" and crop, the Parker
+ * short-scan weights (fbp/weights/shortScanParkerWeight.m) when short_scan != 0, and
+ * dbeta (reconFDK.m:78-81).  Holds a filtered-sinogram scratch buffer. */
+ctsim_status ctsim_fdk_create(ctsim_plan *plan, const char *window, float crop, int short_scan, ctsim_fdk **fdk);
+ctsim_status ctsim_fdk_destroy(ctsim_fdk *fdk);
+
+/* Weighted, ramp-filtered sinogram (reconFDK.m:51-76), device pointers, all views. */
+ctsim_status ctsim_fdk_filter(ctsim_fdk *fdk, const float *d_sino, float *d_filtered, void *stream);
+
+/* Full FDK: filter, back,hpd, times dbeta, times 10 (reconFDK.m:84).  Image overwritten. */
+ctsim_status ctsim_fdk_run(ctsim_fdk *fdk, const float *d_sino, float *d_image, void *stream);
+
+/* The dbeta the FDK scaling uses. */
+float ctsim_fdk_dbeta(const ctsim_fdk *fdk);
+
+/* Host-only: the frequency response H[order] of fbp/filter/designFilter2.m (detector_type 1)
+ * or designEquiangularFilter2.m (0) for gamma = du, in double; order = max(64,
+ * 2^nextpow2(2 nu - 1)) is returned in *order (H may be NULL to query it). */
+ctsim_status ctsim_fdk_design_filter(int nu, float du, float sdd, int detector_type, const char *window, float crop,
+                                     double *H, int *order);
+
+/* ---------------------------------------------------------------------------
+ * OS-PWLS building blocks (device pointers, asynchronous on stream).
+ * ------------------------------------------------------------------------- */
+
+/* statsrecon/pwls/computeWeightsPwls.m:8-9: w = (s - r)^2 / (s + v), w = 0 where s <= r. */
+ctsim_status ctsim_pwls_weights(const float *d_counts, float r, float v, float *d_w, size_t n, void *stream);
+
+/* Subset data term of statsrecon/pwls/reconPwlsSeSqs.m:57-74: d = ax - y, wd = w d, and
+ * *d_phi += sum(w d^2) in FP64 (d_phi may be NULL). */
+ctsim_status ctsim_pwls_residual(const float *d_ax, const float *d_y, const float *d_w, float *d_wd, size_t n,
+                                 double *d_phi, void *stream);
+
+/* *d_acc += sum((a - b)^2) in FP64 (the iteration rmsd, reconPwlsSeSqs.m:81). */
+ctsim_status ctsim_sqdiff(const float *d_a, const float *d_b, size_t n, double *d_acc, void *stream);
+
+/* penalty/huberPenalty.m (kind 0, parameter delta) and penalty/quadPenalty.m (kind 1) in 3-D:
+ * mode 0 adds the value to *d_value (FP64), mode 1 writes the gradient, mode 2 the curvature
+ * into d_out ([nz][ny][nx]).  The quadratic gradient uses dQuad(d) = d (the reference's
+ * dQuad has an empty body, penalty/quadPenalty.m:350-352). */
+ctsim_status ctsim_penalty(int kind, int mode, float delta, int nx, int ny, int nz, const float *d_x, float *d_out,
+                           double *d_value, void *stream);
+
+/* One separable-quadratic-surrogate update (reconPwlsSeSqs.m:59-66):
+ * x_new = x - (num + beta S(x)) / (precom + beta T(x)), negatives, NaN and Inf set to 0; the
+ * penalty gradient S and curvature T are gathered inline; the denominator and step are
+ * formed in FP64.  d_x and d_xnew must differ. */
+ctsim_status ctsim_sqs_update(int kind, float beta, float delta, int nx, int ny, int nz, const float *d_x,
+                              float *d_xnew, const float *d_num, const float *d_precom, void *stream);
+
 /* Matched distance-driven backprojection (same result as CTSIM_BACK_DD, within float
  * rounding) that allocates no device memory.  No counterpart in the reference: its MEX
  * back ends cudaMalloc and cudaFree on every call.

@@ -1,0 +1,124 @@
+"""Oracle for the OS-PWLS path (TEST INFRASTRUCTURE ONLY): numpy restatements of
+the reference's MATLAB in single precision, with the projectors of the C oracle.
+
+    compute_weights_pwls   statsrecon/pwls/computeWeightsPwls.m:8-9
+    huber_penalty          penalty/huberPenalty.m:101-217 (3-D), :222-238
+    quad_penalty           penalty/quadPenalty.m:296-352 (3-D), with dQuad(d) = d
+    recon_pwls_se_sqs      statsrecon/pwls/reconPwlsSeSqs.m:36-110
+
+Arrays follow the package layout [nz, ny, nx]; the MATLAB code indexes x(i,j,k)
+with i along x, so the slicing below is written on the transposed view.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .bindings import oracle_cbct
+
+F32 = np.float32
+AXY = F32(1 / np.sqrt(2))
+AZ = F32(0.5)
+
+
+def compute_weights_pwls(sino, r=0.0, v=0.0):
+    s = np.asarray(sino, dtype=F32)
+    w = ((s - F32(r)) ** 2 / (s + F32(v))).astype(F32)
+    w[s <= F32(r)] = 0
+    return w
+
+
+def _mat(x):
+    return np.asarray(x, dtype=F32).transpose(2, 1, 0)  # x(i,j,k)
+
+
+def _sum_huber(d, delta):
+    d = np.abs(d.astype(np.float64))
+    t = d ** 2 / 2
+    big = d > delta
+    t[big] = delta * d[big] - delta ** 2 / 2
+    return float(t.sum())
+
+
+def _dhuber(d, delta):
+    d = d.copy()
+    d[d > delta] = F32(delta)
+    d[d < -delta] = F32(-delta)
+    return d
+
+
+def _chuber(d, delta):
+    return (np.abs(d) <= delta).astype(F32)
+
+
+def _penalty(x, mode, f_sum, f_grad, f_curv):
+    X = _mat(x)
+    pairs = [((slice(0, -1), slice(None), slice(None)), (slice(1, None), slice(None), slice(None)), F32(1)),
+             ((slice(None), slice(0, -1), slice(None)), (slice(None), slice(1, None), slice(None)), F32(1)),
+             ((slice(0, -1), slice(0, -1), slice(None)), (slice(1, None), slice(1, None), slice(None)), AXY),
+             ((slice(1, None), slice(0, -1), slice(None)), (slice(0, -1), slice(1, None), slice(None)), AXY),
+             ((slice(None), slice(None), slice(0, -1)), (slice(None), slice(None), slice(1, None)), AZ)]
+    if mode == 0:
+        return sum(float(c) * f_sum(X[p] - X[q]) for p, q, c in pairs)
+    y = np.zeros(X.shape, dtype=F32)
+    for n, (p, q, c) in enumerate(pairs):
+        d = X[p] - X[q]
+        g = f_grad(d) if mode == 1 else f_curv(d)
+        if n >= 2:
+            g = (c * g).astype(F32)
+        y[p] = y[p] + g
+        y[q] = (y[q] - g) if mode == 1 else (y[q] + g)
+    return y.transpose(2, 1, 0).copy()
+
+
+def huber_penalty(x, mode, delta=0.001):
+    return _penalty(x, mode, lambda d: _sum_huber(d, delta), lambda d: _dhuber(d, delta),
+                    lambda d: _chuber(d, delta))
+
+
+def quad_penalty(x, mode):
+    if mode == 2:
+        return np.full(np.asarray(x).shape, F32(4 + 4 * AXY + 2 * AZ), dtype=F32)
+    return _penalty(x, mode, lambda d: float((d.astype(np.float64) ** 2 / 2).sum()), lambda d: d, None)
+
+
+def recon_pwls_se_sqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0):
+    """reconPwlsSeSqs.m with the SF projectors of loadPojectors.m; returns (x, phis, rmsds)."""
+    if pfun == "huber":
+        R = lambda x: huber_penalty(x, 0, delta)
+        S = lambda x: huber_penalty(x, 1, delta)
+        T = lambda x: huber_penalty(x, 2, delta)
+    else:
+        R = lambda x: quad_penalty(x, 0)
+        S = lambda x: quad_penalty(x, 1)
+        T = lambda x: quad_penalty(x, 2)
+    M = numos
+    x = np.asarray(img0, dtype=F32).copy()
+    a = oracle_cbct("proj,tf", geom, np.ones_like(x))
+    precom = oracle_cbct("back,tf", geom, (w * a).astype(F32))
+    phis, rmsds = [], []
+    for itn in range(1, itnlim + 1):
+        xold = x.copy()
+        phi = 0.0
+        for isub in range(1, M + 1):
+            g = geom.subset(M, isub)
+            start = isub % M if M > 1 else 0
+            ys = y[start::M] if M > 1 else y
+            ws = w[start::M] if M > 1 else w
+            d = (oracle_cbct("proj,tf", g, x) - ys).astype(F32)
+            num = oracle_cbct("back,tf", g, (ws * d).astype(F32))
+            if M != 1:
+                num = (F32(M) * num).astype(F32)
+            num = (num + F32(beta) * S(x)).astype(F32)
+            den = (precom + F32(beta) * T(x)).astype(F32)
+            x = (x - num / den).astype(F32)
+            x[x < 0] = 0
+            x[np.isnan(x)] = 0
+            x[np.isinf(x)] = 0
+            phi += float((ws.astype(np.float64) * d.astype(np.float64) ** 2).sum()) / 2
+        phi += beta * R(x)
+        rmsd = float(np.sqrt(np.mean((x.astype(np.float64) - xold) ** 2)))
+        phis.append(phi)
+        rmsds.append(rmsd)
+        if itn > 5 and rmsd < 1e-5:
+            break
+    return x, np.array(phis), np.array(rmsds)
