@@ -24,7 +24,8 @@ EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd
             "ctsim_plan_project", "ctsim_plan_backproject", "ctsim_plan_check", "ctsim_back_dd_noalloc",
             "ctsim_fdk_create", "ctsim_fdk_destroy", "ctsim_fdk_filter", "ctsim_fdk_run", "ctsim_fdk_dbeta",
             "ctsim_fdk_design_filter", "ctsim_pwls_weights", "ctsim_pwls_residual", "ctsim_sqdiff",
-            "ctsim_penalty", "ctsim_sqs_update"]
+            "ctsim_penalty", "ctsim_sqs_update", "ctsim_plan_project_ex", "ctsim_plan_backproject_ex",
+            "ctsim_pwls_residual_ex"]
 
 
 class CtsimGeom(C.Structure):
@@ -82,6 +83,10 @@ def load():
     L.ctsim_plan_project.restype = _i
     L.ctsim_plan_backproject.argtypes = [_p, _i, _p, _p, _i, _i, _i, _f, _p]
     L.ctsim_plan_backproject.restype = _i
+    L.ctsim_plan_project_ex.argtypes = [_p, _i, _p, _i, _p, _i, _i, _i, _i, _p]
+    L.ctsim_plan_project_ex.restype = _i
+    L.ctsim_plan_backproject_ex.argtypes = [_p, _i, _p, _i, _p, _i, _i, _i, _i, _f, _p]
+    L.ctsim_plan_backproject_ex.restype = _i
     L.ctsim_plan_check.argtypes = [_p]
     L.ctsim_plan_check.restype = _i
     L.ctsim_back_dd_noalloc.argtypes = [C.POINTER(CtsimGeom), _p, _p, _p, _p, _p, _p]
@@ -103,6 +108,8 @@ def load():
     L.ctsim_pwls_weights.restype = _i
     L.ctsim_pwls_residual.argtypes = [_p, _p, _p, _p, _sz, _p, _p]
     L.ctsim_pwls_residual.restype = _i
+    L.ctsim_pwls_residual_ex.argtypes = [_p, _p, _p, _i, _f, _p, _sz, _p, _p]
+    L.ctsim_pwls_residual_ex.restype = _i
     L.ctsim_sqdiff.argtypes = [_p, _p, _sz, _p, _p]
     L.ctsim_sqdiff.restype = _i
     L.ctsim_penalty.argtypes = [_i, _i, _f, _i, _i, _i, _p, _p, _p, _p]

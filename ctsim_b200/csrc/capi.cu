@@ -236,10 +236,8 @@ extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *
     CTSIM_ALLOC(p->d_ampv, sizeof(float) * ampv.size());
     CTSIM_ALLOC(p->d_map, mp.size());
     CTSIM_ALLOC(p->d_err, sizeof(int));
-    if (p->fwd_ok) {
-        CTSIM_ALLOC(p->d_xs, sizeof(float) * (size_t)nxy * (G.nz + 1));
-        CTSIM_ALLOC(p->d_ps, sizeof(float) * (size_t)G.nu * G.nv * G.noviews);
-    }
+    if (p->fwd_ok) CTSIM_ALLOC(p->d_xs, sizeof(float) * (size_t)nxy * (G.nz + 1));
+    CTSIM_ALLOC(p->d_ps, sizeof(float) * (size_t)G.nu * G.nv * G.noviews);
 #undef CTSIM_ALLOC
     p->bytes = bytes;
     if ((e = cudaMemcpy(p->d_views, views.data(), sizeof(View) * G.noviews, cudaMemcpyHostToDevice)) != cudaSuccess ||
@@ -266,52 +264,77 @@ static ctsim_status check_views(const ctsim_plan *p, int vb, int vs, int vc) {
     return CTSIM_OK;
 }
 
-extern "C" ctsim_status ctsim_plan_project(ctsim_plan *p, int method, const float *d_image, float *d_proj,
-                                           int view_begin, int view_stride, int view_count, void *stream) {
+static bool dtype_ok(int d) { return d == CTSIM_F32 || d == CTSIM_BF16 || d == CTSIM_F16; }
+
+extern "C" ctsim_status ctsim_plan_project_ex(ctsim_plan *p, int method, const void *d_image, int image_dtype,
+                                              void *d_proj, int proj_dtype, int view_begin, int view_stride,
+                                              int view_count, void *stream) {
     if (!p || !d_image || !d_proj) return fail(CTSIM_ERR_ARGUMENT, "null argument");
     if (method != CTSIM_PROJ_DD && method != CTSIM_PROJ_TF) return fail(CTSIM_ERR_ARGUMENT, "unknown forward method");
+    if (!dtype_ok(image_dtype) || !dtype_ok(proj_dtype)) return fail(CTSIM_ERR_ARGUMENT, "unknown storage type");
     ctsim_status s = check_views(p, view_begin, view_stride, view_count);
     if (s != CTSIM_OK) return s;
     if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
     cudaStream_t st = (cudaStream_t)stream;
     const int nxy = p->g.nx * p->g.ny;
-    cudaError_t e = launch_prefix(d_image, p->d_xs, nxy, p->g.nz, st);
+    cudaError_t e = launch_prefix(d_image, image_dtype, p->d_xs, nxy, p->g.nz, st);
     if (e != cudaSuccess) return cuda_fail(e, "prefix kernel");
     e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
-                    view_begin, view_stride, view_count, p->margin, st);
+                    proj_dtype, view_begin, view_stride, view_count, p->margin, st);
     if (e != cudaSuccess) return cuda_fail(e, "forward projection kernel");
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_plan_project(ctsim_plan *p, int method, const float *d_image, float *d_proj,
+                                           int view_begin, int view_stride, int view_count, void *stream) {
+    return ctsim_plan_project_ex(p, method, d_image, CTSIM_F32, d_proj, CTSIM_F32, view_begin, view_stride,
+                                 view_count, stream);
+}
+
+extern "C" ctsim_status ctsim_plan_backproject_ex(ctsim_plan *p, int method, const void *d_proj, int proj_dtype,
+                                                  void *d_image, int image_dtype, int view_begin, int view_stride,
+                                                  int view_count, float scale, void *stream) {
+    if (!p || !d_image || !d_proj) return fail(CTSIM_ERR_ARGUMENT, "null argument");
+    if (!dtype_ok(image_dtype) || !dtype_ok(proj_dtype)) return fail(CTSIM_ERR_ARGUMENT, "unknown storage type");
+    ctsim_status s = check_views(p, view_begin, view_stride, view_count);
+    if (s != CTSIM_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t nuv = (size_t)p->g.nu * p->g.nv;
+    cudaError_t e;
+    switch (method) {
+    case CTSIM_BACK_DD:
+    case CTSIM_BACK_TF: {
+        if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
+        e = launch_prescale(d_proj, proj_dtype, p->d_ampv, p->d_ps, nuv, nuv * view_count, st);
+        if (e != cudaSuccess) return cuda_fail(e, "prescale kernel");
+        e = launch_back(method == CTSIM_BACK_DD ? kDD : kTF, p->back_mz, p->g, p->d_views, p->d_ps, p->d_map,
+                        d_image, image_dtype, view_begin, view_stride, view_count, scale, p->back_qcap, p->d_err, st);
+        break;
+    }
+    case CTSIM_BACK_PD:
+    case CTSIM_BACK_HPD: {
+        const float *src = static_cast<const float *>(d_proj);
+        if (proj_dtype != CTSIM_F32) {  // FP32 copy of the views in scratch
+            e = launch_prescale(d_proj, proj_dtype, nullptr, p->d_ps, nuv, nuv * view_count, st);
+            if (e != cudaSuccess) return cuda_fail(e, "conversion kernel");
+            src = p->d_ps;
+        }
+        e = launch_pd(method == CTSIM_BACK_PD, p->pd_mz, p->g, p->d_views, src, p->d_map, d_image, image_dtype,
+                      view_begin, view_stride, view_count, scale, st);
+        break;
+    }
+    default:
+        return fail(CTSIM_ERR_ARGUMENT, "unknown backprojection method");
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "backprojection kernel");
     return CTSIM_OK;
 }
 
 extern "C" ctsim_status ctsim_plan_backproject(ctsim_plan *p, int method, const float *d_proj, float *d_image,
                                                int view_begin, int view_stride, int view_count, float scale,
                                                void *stream) {
-    if (!p || !d_image || !d_proj) return fail(CTSIM_ERR_ARGUMENT, "null argument");
-    ctsim_status s = check_views(p, view_begin, view_stride, view_count);
-    if (s != CTSIM_OK) return s;
-    cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e;
-    switch (method) {
-    case CTSIM_BACK_DD:
-    case CTSIM_BACK_TF: {
-        if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
-        const size_t nuv = (size_t)p->g.nu * p->g.nv;
-        e = launch_prescale(d_proj, p->d_ampv, p->d_ps, nuv, nuv * view_count, st);
-        if (e != cudaSuccess) return cuda_fail(e, "prescale kernel");
-        e = launch_back(method == CTSIM_BACK_DD ? kDD : kTF, p->back_mz, p->g, p->d_views, p->d_ps, p->d_map,
-                        d_image, view_begin, view_stride, view_count, scale, p->back_qcap, p->d_err, st);
-        break;
-    }
-    case CTSIM_BACK_PD:
-    case CTSIM_BACK_HPD:
-        e = launch_pd(method == CTSIM_BACK_PD, p->pd_mz, p->g, p->d_views, d_proj, p->d_map, d_image, view_begin,
-                      view_stride, view_count, scale, st);
-        break;
-    default:
-        return fail(CTSIM_ERR_ARGUMENT, "unknown backprojection method");
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "backprojection kernel");
-    return CTSIM_OK;
+    return ctsim_plan_backproject_ex(p, method, d_proj, CTSIM_F32, d_image, CTSIM_F32, view_begin, view_stride,
+                                     view_count, scale, stream);
 }
 
 // Synchronous check of the plan's device error flag (set if a kernel met a

@@ -8,9 +8,27 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace ctsim {
+
+// Storage types of volumes and sinograms (all arithmetic is FP32): CTSIM_F32 = 0,
+// CTSIM_BF16 = 1, CTSIM_F16 = 2 in the C ABI.
+enum DType { kF32 = 0, kBF16 = 1, kF16 = 2 };
+
+__device__ __forceinline__ float load_as_float(const void *p, size_t i, int dtype) {
+    if (dtype == kBF16) return __bfloat162float(static_cast<const __nv_bfloat16 *>(p)[i]);
+    if (dtype == kF16) return __half2float(static_cast<const __half *>(p)[i]);
+    return static_cast<const float *>(p)[i];
+}
+
+__device__ __forceinline__ void store_from_float(void *p, size_t i, float v, int dtype) {
+    if (dtype == kBF16) static_cast<__nv_bfloat16 *>(p)[i] = __float2bfloat16_rn(v);
+    else if (dtype == kF16) static_cast<__half *>(p)[i] = __float2half_rn(v);
+    else static_cast<float *>(p)[i] = v;
+}
 
 enum Method { kDD = 0, kTF = 1 };
 

@@ -28,9 +28,9 @@ constexpr unsigned kFull = 0xffffffffu;
 template <int METHOD, int MZ, bool VEC, bool PRESCALED = true>
 __global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restrict__ views,
                                                    const float *__restrict__ ps, const uint8_t *__restrict__ map,
-                                                   float *__restrict__ image, int view_begin, int view_stride,
-                                                   int view_count, float scale, int qcap, int *__restrict__ err,
-                                                   const float *__restrict__ ampv = nullptr) {
+                                                   void *__restrict__ image, int out_dtype, int view_begin,
+                                                   int view_stride, int view_count, float scale, int qcap,
+                                                   int *__restrict__ err, const float *__restrict__ ampv) {
     extern __shared__ float smem[];
     constexpr int kWS = 17;  // row stride of the per-warp weight table (conflict-free writes)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -171,17 +171,19 @@ __global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restric
 #pragma unroll
         for (int m = 0; m < MZ; m++) {
             const int dz = lane + 32 * m;
-            if (dz < izn) image[(size_t)(iz0 + dz) * nxy + (size_t)iy * g.nx + ix] = on ? acc[m] * scale : 0.0f;
+            if (dz < izn)
+                store_from_float(image, (size_t)(iz0 + dz) * nxy + (size_t)iy * g.nx + ix, on ? acc[m] * scale : 0.0f,
+                                 out_dtype);
         }
     }
 }
 
 // ps = proj * ampv (the axial amplitude the reference applies to the backprojected
 // view in place, geom/cbct/cbct_back.c:196-214), into scratch.
-__global__ void prescale_kernel(const float *__restrict__ proj, const float *__restrict__ ampv,
+__global__ void prescale_kernel(const void *__restrict__ proj, int in_dtype, const float *__restrict__ ampv,
                                 float *__restrict__ ps, size_t nuv, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        ps[i] = proj[i] * ampv[i % nuv];
+        ps[i] = load_as_float(proj, i, in_dtype) * (ampv ? ampv[i % nuv] : 1.0f);
 }
 
 // ---------------------------------------------------------------------------
@@ -191,8 +193,8 @@ __global__ void prescale_kernel(const float *__restrict__ proj, const float *__r
 // position s.  32 columns per block; a 32x32 tile is transposed through shared memory
 // so that the image reads and the prefix writes are coalesced.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) prefix_kernel(const float *__restrict__ image, float *__restrict__ xc,
-                                                     int nxy, int nz) {
+__global__ void __launch_bounds__(256) prefix_kernel(const void *__restrict__ image, int in_dtype,
+                                                     float *__restrict__ xc, int nxy, int nz) {
     __shared__ float tile[32][33];
     __shared__ float carry[32];
     const int c0 = blockIdx.x * 32;
@@ -203,7 +205,7 @@ __global__ void __launch_bounds__(256) prefix_kernel(const float *__restrict__ i
         __syncthreads();
         for (int zz = ty; zz < 32; zz += 8) {
             const int z = z0 + zz, c = c0 + tx;
-            tile[zz][tx] = (z < nz && c < nxy) ? image[(size_t)z * nxy + c] : 0.0f;
+            tile[zz][tx] = (z < nz && c < nxy) ? load_as_float(image, (size_t)z * nxy + c, in_dtype) : 0.0f;
         }
         __syncthreads();
         // warp ty scans columns ty, ty+8, ty+16, ty+24 along z (lane = z)
@@ -262,8 +264,8 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
                                                                const float *__restrict__ xs,
                                                                const float *__restrict__ ampv,
                                                                const uint8_t *__restrict__ map,
-                                                               float *__restrict__ proj, int view_begin,
-                                                               int view_stride, float margin) {
+                                                               void *__restrict__ proj, int out_dtype,
+                                                               int view_begin, int view_stride, float margin) {
     extern __shared__ float4 acc4[];  // [kTU][nq] row quads, then the arrays below
     const int NT = blockDim.x;
     const int nq0 = (g.nv + 3) >> 2;
@@ -437,12 +439,14 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
         __syncthreads();
     }
     // 5. axial amplitude and store
-    float *out = proj + (size_t)k * g.nu * nv;
+    const size_t obase = (size_t)k * g.nu * nv;
     const float *accf = reinterpret_cast<const float *>(acc4);
     for (int j = 0; j < kTU; j++) {
         const int iu = iu0 + j;
         if (iu >= g.nu) break;
-        for (int iv = t; iv < nv; iv += NT) out[(size_t)iu * nv + iv] = accf[j * 4 * nq + iv] * ampv[(size_t)iu * nv + iv];
+        for (int iv = t; iv < nv; iv += NT)
+            store_from_float(proj, obase + (size_t)iu * nv + iv, accf[j * 4 * nq + iv] * ampv[(size_t)iu * nv + iv],
+                             out_dtype);
     }
 }
 
@@ -455,8 +459,8 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
 template <bool OFF, int MZ>
 __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict__ views,
                                                  const float *__restrict__ proj, const uint8_t *__restrict__ map,
-                                                 float *__restrict__ image, int view_begin, int view_stride,
-                                                 int view_count, float scale) {
+                                                 void *__restrict__ image, int out_dtype, int view_begin,
+                                                 int view_stride, int view_count, float scale) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tiles_x = (g.nx + 7) >> 3;
     const int iy = blockIdx.x / tiles_x;
@@ -544,7 +548,7 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
             if (dz < izn) {
                 float r = on ? acc[m] : 0.0f;
                 if (scale != 1.0f) r = r * scale;
-                image[(size_t)(iz0 + dz) * nxy + (size_t)iy * g.nx + ix] = r;
+                store_from_float(image, (size_t)(iz0 + dz) * nxy + (size_t)iy * g.nx + ix, r, out_dtype);
             }
         }
     }
@@ -562,40 +566,44 @@ size_t back_smem_bytes(int qcap) { return (size_t)8 * (32 * 17 + 2 * qcap) * siz
 
 template <int METHOD, int MZ, bool VEC>
 static cudaError_t launch_back_mz(const Geom &g, const View *views, const float *ps, const uint8_t *map,
-                                  float *image, int vb, int vs, int vc, float scale, int qcap, int *err,
-                                  cudaStream_t st) {
+                                  void *image, int out_dtype, int vb, int vs, int vc, float scale, int qcap,
+                                  int *err, cudaStream_t st) {
     const int blocks = g.ny * ((g.nx + 7) / 8);
     const size_t sm = back_smem_bytes(qcap);
     auto kfn = back_kernel<METHOD, MZ, VEC>;
     cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, vb, vs, vc, scale, qcap, err, nullptr);
+    kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap, err, nullptr);
     return cudaGetLastError();
 }
 
-cudaError_t launch_prescale(const float *proj, const float *ampv, float *ps, size_t nuv, size_t n, cudaStream_t st) {
+cudaError_t launch_prescale(const void *proj, int in_dtype, const float *ampv, float *ps, size_t nuv, size_t n,
+                            cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 32);
-    prescale_kernel<<<blocks, 256, 0, st>>>(proj, ampv, ps, nuv, n);
+    prescale_kernel<<<blocks, 256, 0, st>>>(proj, in_dtype, ampv, ps, nuv, n);
     return cudaGetLastError();
 }
 
 cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *ps, const uint8_t *map,
-                        float *image, int vb, int vs, int vc, float scale, int qcap, int *err, cudaStream_t st) {
+                        void *image, int out_dtype, int vb, int vs, int vc, float scale, int qcap, int *err,
+                        cudaStream_t st) {
     const bool vec = (g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(ps) % 16) == 0;
-#define CTSIM_BACK_CASE(M, Z)                                                                                 \
-    if (method == M && mz == Z)                                                                               \
-        return vec ? launch_back_mz<M, Z, true>(g, views, ps, map, image, vb, vs, vc, scale, qcap, err, st)  \
-                   : launch_back_mz<M, Z, false>(g, views, ps, map, image, vb, vs, vc, scale, qcap, err, st);
+#define CTSIM_BACK_CASE(M, Z)                                                                                      \
+    if (method == M && mz == Z)                                                                                    \
+        return vec ? launch_back_mz<M, Z, true>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap, err, \
+                                                st)                                                                \
+                   : launch_back_mz<M, Z, false>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap,     \
+                                                 err, st);
     CTSIM_BACK_CASE(kDD, 1) CTSIM_BACK_CASE(kDD, 2) CTSIM_BACK_CASE(kDD, 4) CTSIM_BACK_CASE(kDD, 8)
     CTSIM_BACK_CASE(kTF, 1) CTSIM_BACK_CASE(kTF, 2) CTSIM_BACK_CASE(kTF, 4) CTSIM_BACK_CASE(kTF, 8)
 #undef CTSIM_BACK_CASE
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_prefix(const float *image, float *xs, int nxy, int nz, cudaStream_t st) {
+cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, cudaStream_t st) {
     const int blocks = (nxy + 31) / 32;
-    prefix_kernel<<<blocks, 256, 0, st>>>(image, xs, nxy, nz);
+    prefix_kernel<<<blocks, 256, 0, st>>>(image, in_dtype, xs, nxy, nz);
     return cudaGetLastError();
 }
 
@@ -608,7 +616,8 @@ int proj_group_width() { return kTU; }
 int proj_max_lines() { return kMaxLines; }
 
 cudaError_t launch_proj(int method, const Geom &g, const View *views, const float *xc, const float *ampv,
-                        const uint8_t *map, float *proj, int vb, int vs, int vc, float margin, cudaStream_t st) {
+                        const uint8_t *map, void *proj, int out_dtype, int vb, int vs, int vc, float margin,
+                        cudaStream_t st) {
     const size_t sm = proj_smem_bytes(g.nv, g.nx, g.ny);
     dim3 grid((g.nu + kTU - 1) / kTU, vc);
     // one thread per 4 detector rows (up to 256 threads per block, more rows loop)
@@ -616,27 +625,27 @@ cudaError_t launch_proj(int method, const Geom &g, const View *views, const floa
     if (method == kDD) {
         cudaError_t e = cudaFuncSetAttribute(proj_kernel<kDD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        proj_kernel<kDD><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, vb, vs, margin);
+        proj_kernel<kDD><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin);
     } else {
         cudaError_t e = cudaFuncSetAttribute(proj_kernel<kTF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        proj_kernel<kTF><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, vb, vs, margin);
+        proj_kernel<kTF><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin);
     }
     return cudaGetLastError();
 }
 
 template <bool OFF, int MZ>
 static cudaError_t launch_pd_mz(const Geom &g, const View *views, const float *proj, const uint8_t *map,
-                                float *image, int vb, int vs, int vc, float scale, cudaStream_t st) {
+                                void *image, int out_dtype, int vb, int vs, int vc, float scale, cudaStream_t st) {
     const int blocks = g.ny * ((g.nx + 7) / 8);
-    pd_kernel<OFF, MZ><<<blocks, 256, 0, st>>>(g, views, proj, map, image, vb, vs, vc, scale);
+    pd_kernel<OFF, MZ><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pd(bool off, int mz, const Geom &g, const View *views, const float *proj, const uint8_t *map,
-                      float *image, int vb, int vs, int vc, float scale, cudaStream_t st) {
+                      void *image, int out_dtype, int vb, int vs, int vc, float scale, cudaStream_t st) {
 #define CTSIM_PD_CASE(O, Z) \
-    if (off == O && mz == Z) return launch_pd_mz<O, Z>(g, views, proj, map, image, vb, vs, vc, scale, st);
+    if (off == O && mz == Z) return launch_pd_mz<O, Z>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale, st);
     CTSIM_PD_CASE(true, 1) CTSIM_PD_CASE(true, 2) CTSIM_PD_CASE(true, 4) CTSIM_PD_CASE(true, 8)
     CTSIM_PD_CASE(false, 1) CTSIM_PD_CASE(false, 2) CTSIM_PD_CASE(false, 4) CTSIM_PD_CASE(false, 8)
 #undef CTSIM_PD_CASE
@@ -661,7 +670,7 @@ static cudaError_t launch_back_unscaled_mz(const Geom &g, const View *views, con
     auto kfn = back_kernel<METHOD, MZ, false, false>;
     cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    kfn<<<blocks, 256, sm, st>>>(g, views, proj, map, image, 0, 1, vc, 1.0f, qcap, err, ampv);
+    kfn<<<blocks, 256, sm, st>>>(g, views, proj, map, image, kF32, 0, 1, vc, 1.0f, qcap, err, ampv);
     return cudaGetLastError();
 }
 

@@ -10,25 +10,27 @@
 
 namespace ctsim {
 
-cudaError_t launch_prescale(const float *proj, const float *ampv, float *ps, size_t nuv, size_t n, cudaStream_t st);
+// ps = proj (any storage type) * ampv (ampv may be null: plain conversion to FP32)
+cudaError_t launch_prescale(const void *proj, int in_dtype, const float *ampv, float *ps, size_t nuv, size_t n,
+                            cudaStream_t st);
 
 cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *ps, const uint8_t *map,
-                        float *image, int view_begin, int view_stride, int view_count, float scale, int qcap,
-                        int *err, cudaStream_t st);
+                        void *image, int out_dtype, int view_begin, int view_stride, int view_count, float scale,
+                        int qcap, int *err, cudaStream_t st);
 size_t back_smem_bytes(int qcap);
 cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const float *proj, const float *ampv,
                                  const uint8_t *map, float *image, int view_count, int qcap, int *err,
                                  cudaStream_t st);
 
-cudaError_t launch_prefix(const float *image, float *xs, int nxy, int nz, cudaStream_t st);
+cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, cudaStream_t st);
 
 cudaError_t launch_proj(int method, const Geom &g, const View *views, const float *xs, const float *ampv,
-                        const uint8_t *map, float *proj, int view_begin, int view_stride, int view_count,
-                        float margin, cudaStream_t st);
+                        const uint8_t *map, void *proj, int out_dtype, int view_begin, int view_stride,
+                        int view_count, float margin, cudaStream_t st);
 
 cudaError_t launch_pd(bool off_boundary, int mz, const Geom &g, const View *views, const float *proj,
-                      const uint8_t *map, float *image, int view_begin, int view_stride, int view_count, float scale,
-                      cudaStream_t st);
+                      const uint8_t *map, void *image, int out_dtype, int view_begin, int view_stride,
+                      int view_count, float scale, cudaStream_t st);
 
 cudaError_t launch_scale(float *y, size_t n, float s, cudaStream_t st);
 

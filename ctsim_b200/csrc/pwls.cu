@@ -35,13 +35,14 @@ __global__ void weights_kernel(const float *__restrict__ s, float r, float v, fl
     }
 }
 
-__global__ void residual_kernel(const float *__restrict__ ax, const float *__restrict__ y,
-                                const float *__restrict__ w, float *__restrict__ wd, size_t n,
-                                double *__restrict__ phi) {
+__global__ void residual_kernel(const float *__restrict__ ax, const void *__restrict__ y,
+                                const void *__restrict__ w, int dtype, float w_scale, float *__restrict__ wd,
+                                size_t n, double *__restrict__ phi) {
     double acc = 0.0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const float d = ax[i] - y[i];
-        const float wi = w[i];
+        // the residual is formed in FP32 whatever the storage type of y and w
+        const float d = ax[i] - load_as_float(y, i, dtype);
+        const float wi = load_as_float(w, i, dtype) * w_scale;
         wd[i] = wi * d;
         acc += (double)wi * (double)d * (double)d;
     }
@@ -188,13 +189,19 @@ extern "C" ctsim_status ctsim_pwls_weights(const float *d_counts, float r, float
     return e == cudaSuccess ? CTSIM_OK : ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
 }
 
-extern "C" ctsim_status ctsim_pwls_residual(const float *d_ax, const float *d_y, const float *d_w, float *d_wd,
-                                            size_t n, double *d_phi, void *stream) {
+extern "C" ctsim_status ctsim_pwls_residual_ex(const float *d_ax, const void *d_y, const void *d_w, int dtype,
+                                               float w_scale, float *d_wd, size_t n, double *d_phi, void *stream) {
     if (!d_ax || !d_y || !d_w || !d_wd) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    if (dtype < kF32 || dtype > kF16) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "unknown storage type");
     if (n == 0) return CTSIM_OK;
-    residual_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d_ax, d_y, d_w, d_wd, n, d_phi);
+    residual_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d_ax, d_y, d_w, dtype, w_scale, d_wd, n, d_phi);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? CTSIM_OK : ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
+}
+
+extern "C" ctsim_status ctsim_pwls_residual(const float *d_ax, const float *d_y, const float *d_w, float *d_wd,
+                                            size_t n, double *d_phi, void *stream) {
+    return ctsim_pwls_residual_ex(d_ax, d_y, d_w, kF32, 1.0f, d_wd, n, d_phi, stream);
 }
 
 extern "C" ctsim_status ctsim_sqdiff(const float *d_a, const float *d_b, size_t n, double *d_acc, void *stream) {

@@ -25,6 +25,26 @@ from . import _lib
 from .geometry import CTGeometry
 
 PROJ_TYPES = ("proj,dd", "proj,tf")
+
+
+class _DTypeMap(dict):
+    """torch dtype -> ctsim_dtype, built lazily (torch is optional for the host API)."""
+
+    def _fill(self):
+        if not self:
+            import torch
+            self.update({torch.float32: 0, torch.bfloat16: 1, torch.float16: 2})
+
+    def __getitem__(self, k):
+        self._fill()
+        return dict.__getitem__(self, k)
+
+    def __contains__(self, k):
+        self._fill()
+        return dict.__contains__(self, k)
+
+
+_DTYPES = _DTypeMap()
 BACK_TYPES = ("back,dd", "back,tf", "back,pd", "back,hpd")
 
 
@@ -153,8 +173,8 @@ class Plan:
 
     def _check_tensor(self, t, shape, name):
         torch = _torch()
-        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32):
-            raise TypeError(f"{name} must be a float32 CUDA tensor")
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype in _DTYPES):
+            raise TypeError(f"{name} must be a float32, bfloat16 or float16 CUDA tensor")
         if t.device != self.device:
             raise ValueError(f"{name} is on {t.device}, the plan on {self.device}")
         if tuple(t.shape) != tuple(shape):
@@ -162,35 +182,38 @@ class Plan:
         return t.contiguous()
 
     def project(self, image, method: str = "dd", view_begin: int = 0, view_stride: int = 1, view_count=None,
-                out=None):
-        """A x for the selected views -> float32[view_count, nu, nv]."""
+                out=None, out_dtype=None):
+        """A x for the selected views -> [view_count, nu, nv] of ``out_dtype`` (default: the
+        image's storage type; float32, bfloat16 or float16, FP32 accumulation)."""
         torch = _torch()
         vb, vs, vc = self._views(view_begin, view_stride, view_count)
         image = self._check_tensor(image, self.geom.image_shape, "image")
         if out is None:
-            out = torch.empty((vc, self.geom.nu, self.geom.nv), dtype=torch.float32, device=self.device)
+            out = torch.empty((vc, self.geom.nu, self.geom.nv), dtype=out_dtype or image.dtype, device=self.device)
         else:
             out = self._check_tensor(out, (vc, self.geom.nu, self.geom.nv), "out")
         m = {"dd": 0, "tf": 1, "proj,dd": 0, "proj,tf": 1}[method]
         st = torch.cuda.current_stream(self.device).cuda_stream
-        _lib.check(self._L.ctsim_plan_project(self._h, m, image.data_ptr(), out.data_ptr(), vb, vs, vc, st),
-                   "ctsim_plan_project")
+        _lib.check(self._L.ctsim_plan_project_ex(self._h, m, image.data_ptr(), _DTYPES[image.dtype], out.data_ptr(),
+                                                 _DTYPES[out.dtype], vb, vs, vc, st), "ctsim_plan_project")
         return out
 
     def backproject(self, sino, method: str = "dd", view_begin: int = 0, view_stride: int = 1, view_count=None,
-                    scale: float = 1.0, out=None):
-        """scale * A^T y (or the FDK pd/hpd backprojection) -> float32[nz, ny, nx]."""
+                    scale: float = 1.0, out=None, out_dtype=None):
+        """scale * A^T y (or the FDK pd/hpd backprojection) -> [nz, ny, nx] of ``out_dtype``
+        (default: the sinogram's storage type)."""
         torch = _torch()
         vb, vs, vc = self._views(view_begin, view_stride, view_count)
         sino = self._check_tensor(sino, (vc, self.geom.nu, self.geom.nv), "sino")
         if out is None:
-            out = torch.empty(self.geom.image_shape, dtype=torch.float32, device=self.device)
+            out = torch.empty(self.geom.image_shape, dtype=out_dtype or sino.dtype, device=self.device)
         else:
             out = self._check_tensor(out, self.geom.image_shape, "out")
         m = {"dd": 2, "tf": 3, "pd": 4, "hpd": 5, "back,dd": 2, "back,tf": 3, "back,pd": 4, "back,hpd": 5}[method]
         st = torch.cuda.current_stream(self.device).cuda_stream
-        _lib.check(self._L.ctsim_plan_backproject(self._h, m, sino.data_ptr(), out.data_ptr(), vb, vs, vc,
-                                                  float(scale), st), "ctsim_plan_backproject")
+        _lib.check(self._L.ctsim_plan_backproject_ex(self._h, m, sino.data_ptr(), _DTYPES[sino.dtype],
+                                                     out.data_ptr(), _DTYPES[out.dtype], vb, vs, vc, float(scale),
+                                                     st), "ctsim_plan_backproject")
         return out
 
     def check(self):

@@ -89,7 +89,7 @@ class PwlsSolver:
     """
 
     def __init__(self, y, w, geom: CTGeometry, beta: float, pfun: str = "huber", delta: float = 0.001,
-                 numos: int = 1, img0=None, method: str = "tf"):
+                 numos: int = 1, img0=None, method: str = "tf", storage=None):
         torch = _torch()
         if pfun.lower() not in PENALTIES:
             raise ValueError("unknow penalty function")
@@ -99,17 +99,32 @@ class PwlsSolver:
         self.plan = plan_for(geom, y.device)
         self.dev = self.plan.device
         self.L = _lib.load()
-        y = y.to(self.dev, torch.float32).contiguous()
-        w = w.to(self.dev, torch.float32).contiguous()
+        # the measured data (y, w: the largest arrays) may be stored in bfloat16 or float16;
+        # the image, the surrogate denominator and every residual stay FP32
+        self.storage = storage or torch.float32
+        from .projector import _DTYPES
+        self.sdt = _DTYPES[self.storage]
+        y32 = y.to(self.dev, torch.float32).contiguous()
+        y = y.to(self.dev, self.storage).contiguous()
+        w32 = w.to(self.dev, torch.float32)
+        # weights are photon counts (1e5 and more): FP16 stores them divided by a power of two
+        self.w_scale = 1.0
+        if self.storage == torch.float16:
+            wmax = float(w32.max().item())
+            if wmax > 16384.0:
+                self.w_scale = float(2.0 ** math.ceil(math.log2(wmax / 16384.0)))
+        w = (w32 / self.w_scale).to(self.storage).contiguous()
+        del w32
         if img0 is None:
             from .fdk import reconFDK
-            img0 = reconFDK(y, geom)
+            img0 = reconFDK(y32, geom)
+        del y32
         self.x = img0.to(self.dev, torch.float32).clone().contiguous()
         self.xn = torch.empty_like(self.x)
         self.xold = torch.empty_like(self.x)
         # precompute (reconPwlsSeSqs.m:40-41): a = A(1), precom = At(w .* a)
         a = self.plan.project(torch.ones_like(self.x), method)
-        self.precom = self.plan.backproject((w * a).contiguous(), method)
+        self.precom = self.plan.backproject((w.float() * self.w_scale * a).contiguous(), method)
         del a
         # subsets 1+mod(isub,M):M:end for isub = 1..M (0-based start isub % M)
         self.subsets = []
@@ -136,8 +151,9 @@ class PwlsSolver:
             ax = self.ax[:count]
             wd = self.wd[:count]
             self.plan.project(self.x, self.method, start, stride, count, out=ax)
-            _lib.check(self.L.ctsim_pwls_residual(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), wd.data_ptr(),
-                                                  ax.numel(), acc, st), "ctsim_pwls_residual")
+            _lib.check(self.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), self.sdt,
+                                                     self.w_scale, wd.data_ptr(), ax.numel(), acc, st),
+                       "ctsim_pwls_residual")
             self.plan.backproject(wd, self.method, start, stride, count, scale=float(self.M), out=self.num)
             _lib.check(self.L.ctsim_sqs_update(self.kind, self.beta, self.delta, self.nx, self.ny, self.nz,
                                                self.x.data_ptr(), self.xn.data_ptr(), self.num.data_ptr(),
@@ -155,9 +171,10 @@ class PwlsSolver:
 
 
 def reconPwlsSeSqs(y, w, geom: CTGeometry, beta: float, pfun: str = "huber", itnlim: int = 10,
-                   delta: float = 0.001, numos: int = 1, img0=None, stopCrt: float = 1e-5):
-    """statsrecon/pwls/reconPwlsSeSqs.m: returns (x, phis, rmsds)."""
-    solver = PwlsSolver(y, w, geom, beta, pfun, delta, numos, img0)
+                   delta: float = 0.001, numos: int = 1, img0=None, stopCrt: float = 1e-5, storage=None):
+    """statsrecon/pwls/reconPwlsSeSqs.m: returns (x, phis, rmsds).  ``storage`` (torch dtype)
+    stores y and w in bfloat16/float16; arithmetic and the image stay FP32."""
+    solver = PwlsSolver(y, w, geom, beta, pfun, delta, numos, img0, storage=storage)
     phis, rmsds = np.zeros(itnlim), np.zeros(itnlim)
     for itn in range(1, itnlim + 1):
         phi, rmsd = solver.step()

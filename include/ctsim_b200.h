@@ -56,6 +56,13 @@ typedef enum {
     CTSIM_BACK_HPD = 5  /* "back,hpd" */
 } ctsim_method;
 
+/* Storage types of volumes and sinograms in the plan API (arithmetic is always FP32). */
+typedef enum {
+    CTSIM_F32 = 0,
+    CTSIM_BF16 = 1,  /* __nv_bfloat16 */
+    CTSIM_F16 = 2    /* __half */
+} ctsim_dtype;
+
 /* Last error message of the calling thread (never NULL). */
 const char *ctsim_last_error(void);
 
@@ -152,6 +159,15 @@ ctsim_status ctsim_plan_project(ctsim_plan *plan, int method, const float *d_ima
 ctsim_status ctsim_plan_backproject(ctsim_plan *plan, int method, const float *d_proj, float *d_image,
                                     int view_begin, int view_stride, int view_count, float scale, void *stream);
 
+/* The same with the storage type of the image and the sinogram given separately
+ * (ctsim_dtype): BF16/FP16 inputs are widened to FP32 on load, every footprint sum
+ * accumulates in FP32, outputs are rounded to their storage type on store. */
+ctsim_status ctsim_plan_project_ex(ctsim_plan *plan, int method, const void *d_image, int image_dtype, void *d_proj,
+                                   int proj_dtype, int view_begin, int view_stride, int view_count, void *stream);
+ctsim_status ctsim_plan_backproject_ex(ctsim_plan *plan, int method, const void *d_proj, int proj_dtype,
+                                       void *d_image, int image_dtype, int view_begin, int view_stride,
+                                       int view_count, float scale, void *stream);
+
 /* Synchronous: waits for the device and reports whether any kernel on this plan met a
  * footprint larger than its buffers (a device-side flag; never expected for a valid plan). */
 ctsim_status ctsim_plan_check(ctsim_plan *plan);
@@ -197,6 +213,12 @@ ctsim_status ctsim_pwls_weights(const float *d_counts, float r, float v, float *
  * *d_phi += sum(w d^2) in FP64 (d_phi may be NULL). */
 ctsim_status ctsim_pwls_residual(const float *d_ax, const float *d_y, const float *d_w, float *d_wd, size_t n,
                                  double *d_phi, void *stream);
+
+/* The same with y and w stored as `dtype` (ctsim_dtype) and the weights stored divided by
+ * w_scale (a power of two keeps FP16's range for photon-count weights); the residual is
+ * formed in FP32. */
+ctsim_status ctsim_pwls_residual_ex(const float *d_ax, const void *d_y, const void *d_w, int dtype, float w_scale,
+                                    float *d_wd, size_t n, double *d_phi, void *stream);
 
 /* *d_acc += sum((a - b)^2) in FP64 (the iteration rmsd, reconPwlsSeSqs.m:81). */
 ctsim_status ctsim_sqdiff(const float *d_a, const float *d_b, size_t n, double *d_acc, void *stream);

@@ -17,6 +17,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libcbct_oracle.so")
+ORACLE64_SO = os.path.join(HERE, "_build", "libcbct_oracle64.so")
 REF_SO = os.path.join(HERE, "_ref", "libcbct_ref.so")
 
 KINDS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3,
@@ -42,7 +43,7 @@ def _load(path):
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         lib = C.CDLL(path)
-        if path == ORACLE_SO:
+        if path in (ORACLE_SO, ORACLE64_SO):
             lib.orc_proj.argtypes = [_i] + _GEOM_ARGS
             lib.orc_back.argtypes = [_i] + _GEOM_ARGS
             lib.orc_back_pd.argtypes = _GEOM_ARGS + [_i]
@@ -61,18 +62,18 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
-def _prep(kind, geom, data):
+def _prep(kind, geom, data, dtype=np.float32):
     if kind not in KINDS:
         raise ValueError(f"unknown geom type {kind!r}")
-    data = np.ascontiguousarray(data, dtype=np.float32)
+    data = np.ascontiguousarray(data, dtype=dtype)
     if kind.startswith("proj"):
         if data.shape != geom.image_shape:
             raise ValueError("image must have shape (nz, ny, nx)")
-        out = np.zeros(geom.sino_shape, dtype=np.float32)
+        out = np.zeros(geom.sino_shape, dtype=dtype)
     else:
         if data.shape != geom.sino_shape:
             raise ValueError("sinogram must have shape (noViews, nu, nv)")
-        out = np.zeros(geom.image_shape, dtype=np.float32)
+        out = np.zeros(geom.image_shape, dtype=dtype)
     betas = np.ascontiguousarray(geom.betas, dtype=np.float64)
     couch = np.ascontiguousarray(geom.couchZ, dtype=np.float32)
     mp = np.ascontiguousarray(geom.map, dtype=np.bool_)
@@ -82,10 +83,11 @@ def _prep(kind, geom, data):
     return data, out, tuple(geom.scalars()) + tail, keep
 
 
-def oracle_cbct(kind: str, geom, data) -> np.ndarray:
-    """Run this project's CPU restatement of one reference projector."""
-    lib = _load(ORACLE_SO)
-    data, out, args, keep = _prep(kind, geom, data)
+def oracle_cbct(kind: str, geom, data, fp64: bool = False) -> np.ndarray:
+    """Run this project's CPU restatement of one reference projector (bit-exact FP32), or
+    with ``fp64`` the same control flow in double (float64 arrays in and out)."""
+    lib = _load(ORACLE64_SO if fp64 else ORACLE_SO)
+    data, out, args, keep = _prep(kind, geom, data, np.float64 if fp64 else np.float32)
     if kind.startswith("proj"):
         ok = lib.orc_proj(KINDS[kind], *args)
     elif kind in ("back,dd", "back,tf"):

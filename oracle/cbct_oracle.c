@@ -16,6 +16,11 @@
  *   proj [ib*nu*nv + iu*nv + iv]      float, v fastest
  *   map  [iy*nx + ix]                 bool
  *
+ * Compiled twice (oracle/Makefile): with ORC_REAL=float it is the bit-exact
+ * restatement above; with ORC_REAL=double the same control flow runs in double
+ * everywhere (sin/cos, footprints, weights, accumulation) -- the FP64 oracle that
+ * precision variants are measured against.
+ *
  * Deliberate differences from the reference:
  *   - inputs are const: the reference back-projectors scale their sinogram
  *     argument in place (geom/cbct/cbct_back.c:196-214); here a scaled copy of
@@ -31,6 +36,11 @@
 #include <stdlib.h>
 #include <string.h>
 
+#ifndef ORC_REAL
+#define ORC_REAL float
+#endif
+typedef ORC_REAL real;  /* float: the bit-exact oracle; double: the FP64 oracle */
+
 #define ORC_FP_DD_U 16 /* iumax <= iumin + 15   geom/cbct/cbct_proj.c:343 */
 #define ORC_FP_TF_U 10 /* iumax <= iumin + 9    geom/cbct/cbct_proj.c:612 (FOOTPRINT_SIZE_U = 10, :210) */
 #define ORC_FP_V 10    /* ivmax <= ivmin + 9    geom/cbct/cbct_proj.c:395 (FOOTPRINT_SIZE_V = 10, :211) */
@@ -39,23 +49,23 @@ enum { ORC_DD = 0, ORC_TF = 1 };
 
 typedef struct {
     int nx, ny, nz, nu, nv, detector_type;
-    float dx, dy, dz, sad, sdd, du, dv;
-    float wx, wy, wu, wv, sdd_du;
-    float oz;
+    real dx, dy, dz, sad, sdd, du, dv;
+    real wx, wy, wu, wv, sdd_du;
+    real oz;
 } orc_geom;
 
 /* Per-view constants (geom/cbct/cbct_proj.c:256-265). */
 typedef struct {
-    float sin_a, cos_a, wz;
-    float dx_sin_2, dx_cos_2, dy_sin_2, n_dy_cos_2;
+    real sin_a, cos_a, wz;
+    real dx_sin_2, dx_cos_2, dy_sin_2, n_dy_cos_2;
 } orc_view;
 
 /* Centre offset "- ( n - 1.0 ) / 2.0 + offset" evaluated in double, stored as float
  * (geom/cbct/cbct_proj.c:244-247). */
-static float orc_centre(int n, float offset) { return (float)(-((double)n - 1.0) / 2.0 + (double)offset); }
+static real orc_centre(int n, real offset) { return (real)(-((double)n - 1.0) / 2.0 + (double)offset); }
 
-static orc_geom orc_make_geom(int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy, float oz,
-                              int nu, int nv, float du, float dv, float ou, float ov, float sad, float sdd,
+static orc_geom orc_make_geom(int nx, int ny, int nz, real dx, real dy, real dz, real ox, real oy, real oz,
+                              int nu, int nv, real du, real dv, real ou, real ov, real sad, real sdd,
                               int detector_type)
 {
     orc_geom g;
@@ -70,19 +80,19 @@ static orc_geom orc_make_geom(int nx, int ny, int nz, float dx, float dy, float 
     return g;
 }
 
-static orc_view orc_make_view(const orc_geom *g, double beta, float couchz)
+static orc_view orc_make_view(const orc_geom *g, double beta, real couchz)
 {
     orc_view v;
-    v.sin_a = (float)sin(beta);
-    v.cos_a = (float)cos(beta);
+    v.sin_a = (real)sin(beta);
+    v.cos_a = (real)cos(beta);
     /* wz: geom/cbct/cbct_proj.c:256, the couch shift divided in float then added in double */
-    float cz = couchz / g->dz;
-    v.wz = (float)((-((double)g->nz - 1.0) / 2.0 + (double)g->oz) + (double)cz);
+    real cz = couchz / g->dz;
+    v.wz = (real)((-((double)g->nz - 1.0) / 2.0 + (double)g->oz) + (double)cz);
     /* halves are exact: (x * s) / 2.0   geom/cbct/cbct_proj.c:262-265 */
-    v.dx_sin_2 = (float)((double)(g->dx * v.sin_a) / 2.0);
-    v.dx_cos_2 = (float)((double)(g->dx * v.cos_a) / 2.0);
-    v.dy_sin_2 = (float)((double)(g->dy * v.sin_a) / 2.0);
-    v.n_dy_cos_2 = (float)((double)(-g->dy * v.cos_a) / 2.0);
+    v.dx_sin_2 = (real)((double)(g->dx * v.sin_a) / 2.0);
+    v.dx_cos_2 = (real)((double)(g->dx * v.cos_a) / 2.0);
+    v.dy_sin_2 = (real)((double)(g->dy * v.sin_a) / 2.0);
+    v.n_dy_cos_2 = (real)((double)(-g->dy * v.cos_a) / 2.0);
     return v;
 }
 
@@ -90,45 +100,45 @@ static orc_view orc_make_view(const orc_geom *g, double beta, float couchz)
 typedef struct {
     int hit;           /* 0: the column misses the detector                     */
     int iumin, iumax;  /* detector columns touched                              */
-    float w[ORC_FP_DD_U];
-    float ampu;        /* in-plane path-length factor dx/max(|cos|,|sin|)/10    */
-    float zinc, vstart;/* axial footprint: voxel height in rows, first edge     */
+    real w[ORC_FP_DD_U];
+    real ampu;        /* in-plane path-length factor dx/max(|cos|,|sin|)/10    */
+    real zinc, vstart;/* axial footprint: voxel height in rows, first edge     */
     int iz_start, iz_stop;
 } orc_column;
 
 /* Shared column geometry: rotated centre, distance to source, amplitude
  * (geom/cbct/cbct_proj.c:282-310 DD, :531-549 TF). */
-static void orc_column_centre(const orc_geom *g, const orc_view *v, int ix, int iy, float *tproj0, float *dsxy0,
-                              float *cos_phi, float *sin_phi)
+static void orc_column_centre(const orc_geom *g, const orc_view *v, int ix, int iy, real *tproj0, real *dsxy0,
+                              real *cos_phi, real *sin_phi)
 {
-    float xc = ((float)ix + g->wx) * g->dx;
-    float yc = ((float)iy + g->wy) * g->dy;
-    float t = xc * v->cos_a - yc * v->sin_a;
-    float d = g->sad + xc * v->sin_a + yc * v->cos_a;
-    float r = (float)sqrt((double)(t * t + d * d));
-    float cg = d / r;
-    float sg = t / r;
+    real xc = ((real)ix + g->wx) * g->dx;
+    real yc = ((real)iy + g->wy) * g->dy;
+    real t = xc * v->cos_a - yc * v->sin_a;
+    real d = g->sad + xc * v->sin_a + yc * v->cos_a;
+    real r = (real)sqrt((double)(t * t + d * d));
+    real cg = d / r;
+    real sg = t / r;
     *tproj0 = t;
     *dsxy0 = d;
-    *cos_phi = (float)fabs((double)(v->cos_a * cg - v->sin_a * sg));
-    *sin_phi = (float)fabs((double)(v->sin_a * cg + v->cos_a * sg));
+    *cos_phi = (real)fabs((double)(v->cos_a * cg - v->sin_a * sg));
+    *sin_phi = (real)fabs((double)(v->sin_a * cg + v->cos_a * sg));
 }
 
 /* Detector coordinate (in pixels, before the +0.5 shift) of the ray through (t, d). */
-static float orc_u_of(const orc_geom *g, float num, float den)
+static real orc_u_of(const orc_geom *g, real num, real den)
 {
     if (g->detector_type == 1) return g->sdd_du * num / den - g->wu;
     /* curved: sdd_du * atan(ratio) - wu in double, geom/cbct/cbct_proj.c:316 */
-    return (float)((double)g->sdd_du * atan((double)(num / den)) - (double)g->wu);
+    return (real)((double)g->sdd_du * atan((double)(num / den)) - (double)g->wu);
 }
 
 /* Axial part shared by DD and TF (geom/cbct/cbct_proj.c:361-372). */
-static int orc_column_axial(const orc_geom *g, const orc_view *v, float dsxy0, orc_column *c)
+static int orc_column_axial(const orc_geom *g, const orc_view *v, real dsxy0, orc_column *c)
 {
     c->zinc = g->dz / g->dv * g->sdd / dsxy0;
-    c->vstart = (float)(((double)v->wz - 0.5) * (double)c->zinc - (double)g->wv);
-    int s = (int)floorf((-1.0f - c->vstart) / c->zinc);
-    int e = (int)ceilf(((float)(g->nv + 1) - c->vstart) / c->zinc);
+    c->vstart = (real)(((double)v->wz - 0.5) * (double)c->zinc - (double)g->wv);
+    int s = (int)floor(((real)-1.0 - c->vstart) / c->zinc);
+    int e = (int)ceil(((real)(g->nv + 1) - c->vstart) / c->zinc);
     if (s < 0) s = 0;
     if (e > g->nz) e = g->nz;
     c->iz_start = s;
@@ -139,23 +149,23 @@ static int orc_column_axial(const orc_geom *g, const orc_view *v, float dsxy0, o
 /* Distance-driven u footprint (geom/cbct/cbct_proj.c:297-359). */
 static void orc_column_dd(const orc_geom *g, const orc_view *v, int ix, int iy, orc_column *c)
 {
-    float tproj0, dsxy0, cos_phi, sin_phi, umin, umax;
+    real tproj0, dsxy0, cos_phi, sin_phi, umin, umax;
     orc_column_centre(g, v, ix, iy, &tproj0, &dsxy0, &cos_phi, &sin_phi);
     c->hit = 0;
     if (cos_phi > sin_phi) {
-        c->ampu = (float)((double)(g->dx / cos_phi) / 10.0);
+        c->ampu = (real)((double)(g->dx / cos_phi) / 10.0);
         umin = orc_u_of(g, tproj0 + v->dx_cos_2, dsxy0 + v->dx_sin_2);
         umax = orc_u_of(g, tproj0 - v->dx_cos_2, dsxy0 - v->dx_sin_2);
     } else {
-        c->ampu = (float)((double)(g->dx / sin_phi) / 10.0);
+        c->ampu = (real)((double)(g->dx / sin_phi) / 10.0);
         umin = orc_u_of(g, tproj0 + v->dy_sin_2, dsxy0 + v->n_dy_cos_2);
         umax = orc_u_of(g, tproj0 - v->dy_sin_2, dsxy0 - v->n_dy_cos_2);
     }
-    if (umin >= umax) { float t = umax; umax = umin; umin = t; }
-    umin = umin + 0.5f; if (!(umin > 0.0f)) umin = 0.0f;
-    umax = umax + 0.5f; if (!(umax < (float)g->nu)) umax = (float)g->nu;
+    if (umin >= umax) { real t = umax; umax = umin; umin = t; }
+    umin = umin + (real)0.5; if (!(umin > (real)0.0)) umin = (real)0.0;
+    umax = umax + (real)0.5; if (!(umax < (real)g->nu)) umax = (real)g->nu;
     if (umin > umax) return;
-    int lo = (int)floorf(umin), hi = (int)floorf(umax);
+    int lo = (int)floor(umin), hi = (int)floor(umax);
     if (hi > g->nu - 1) hi = g->nu - 1;
     if (hi > lo + ORC_FP_DD_U - 1) hi = lo + ORC_FP_DD_U - 1;
     c->iumin = lo;
@@ -163,9 +173,9 @@ static void orc_column_dd(const orc_geom *g, const orc_view *v, int ix, int iy, 
     if (lo == hi) {
         c->w[0] = umax - umin;
     } else {
-        c->w[0] = (float)(lo + 1) - umin;
-        for (int k = 1; k < hi - lo; k++) c->w[k] = 1.0f;
-        c->w[hi - lo] = umax - (float)hi;
+        c->w[0] = (real)(lo + 1) - umin;
+        for (int k = 1; k < hi - lo; k++) c->w[k] = (real)1.0;
+        c->w[hi - lo] = umax - (real)hi;
     }
     if (orc_column_axial(g, v, dsxy0, c)) c->hit = 1;
 }
@@ -173,10 +183,10 @@ static void orc_column_dd(const orc_geom *g, const orc_view *v, int ix, int iy, 
 /* Separable-footprint (trapezoid) u footprint (geom/cbct/cbct_proj.c:545-643). */
 static void orc_column_tf(const orc_geom *g, const orc_view *v, int ix, int iy, orc_column *c)
 {
-    float tproj0, dsxy0, cos_phi, sin_phi, tau[4];
+    real tproj0, dsxy0, cos_phi, sin_phi, tau[4];
     orc_column_centre(g, v, ix, iy, &tproj0, &dsxy0, &cos_phi, &sin_phi);
     c->hit = 0;
-    c->ampu = (float)((double)(g->dx / (cos_phi > sin_phi ? cos_phi : sin_phi)) / 10.0);
+    c->ampu = (real)((double)(g->dx / (cos_phi > sin_phi ? cos_phi : sin_phi)) / 10.0);
     /* the four corner projections, in the reference's operand order */
     tau[0] = orc_u_of(g, tproj0 + v->dx_cos_2 + v->dy_sin_2, dsxy0 + v->dx_sin_2 + v->n_dy_cos_2);
     tau[1] = orc_u_of(g, tproj0 - v->dx_cos_2 + v->dy_sin_2, dsxy0 - v->dx_sin_2 + v->n_dy_cos_2);
@@ -186,25 +196,25 @@ static void orc_column_tf(const orc_geom *g, const orc_view *v, int ix, int iy, 
     static const int net[5][2] = {{0, 1}, {2, 3}, {0, 2}, {1, 3}, {1, 2}};
     for (int k = 0; k < 5; k++) {
         int a = net[k][0], b = net[k][1];
-        if (tau[a] > tau[b]) { float t = tau[a]; tau[a] = tau[b]; tau[b] = t; }
+        if (tau[a] > tau[b]) { real t = tau[a]; tau[a] = tau[b]; tau[b] = t; }
     }
-    float umin = tau[0] + 0.5f; if (!(umin > 0.0f)) umin = 0.0f;
-    float umax = tau[3] + 0.5f; if (!(umax < (float)g->nu)) umax = (float)g->nu;
+    real umin = tau[0] + (real)0.5; if (!(umin > (real)0.0)) umin = (real)0.0;
+    real umax = tau[3] + (real)0.5; if (!(umax < (real)g->nu)) umax = (real)g->nu;
     if (umin > umax) return;
-    int lo = (int)floorf(umin), hi = (int)floorf(umax);
+    int lo = (int)floor(umin), hi = (int)floor(umax);
     if (hi > g->nu - 1) hi = g->nu - 1;
     if (hi > lo + ORC_FP_TF_U - 1) hi = lo + ORC_FP_TF_U - 1;
     c->iumin = lo;
     c->iumax = hi;
     for (int iu = lo; iu <= hi; iu++) {
-        float w = 0.0f;
-        float bl = (float)((double)iu - 0.5), br = (float)((double)iu + 0.5);
-        float xl = bl > tau[0] ? bl : tau[0], xr = br < tau[1] ? br : tau[1];
-        if (xr > xl) w = w + (((xr - tau[0]) * (xr - tau[0]) - (xl - tau[0]) * (xl - tau[0])) / (tau[1] - tau[0])) / 2.0f;
+        real w = (real)0.0;
+        real bl = (real)((double)iu - 0.5), br = (real)((double)iu + 0.5);
+        real xl = bl > tau[0] ? bl : tau[0], xr = br < tau[1] ? br : tau[1];
+        if (xr > xl) w = w + (((xr - tau[0]) * (xr - tau[0]) - (xl - tau[0]) * (xl - tau[0])) / (tau[1] - tau[0])) / (real)2.0;
         xl = bl > tau[1] ? bl : tau[1]; xr = br < tau[2] ? br : tau[2];
         if (xr > xl) w = w + (xr - xl);
         xl = bl > tau[2] ? bl : tau[2]; xr = br < tau[3] ? br : tau[3];
-        if (xr > xl) w = w + (((xl - tau[3]) * (xl - tau[3]) - (xr - tau[3]) * (xr - tau[3])) / (tau[3] - tau[2])) / 2.0f;
+        if (xr > xl) w = w + (((xl - tau[3]) * (xl - tau[3]) - (xr - tau[3]) * (xr - tau[3])) / (tau[3] - tau[2])) / (real)2.0;
         c->w[iu - lo] = w;
     }
     if (orc_column_axial(g, v, dsxy0, c)) c->hit = 1;
@@ -212,35 +222,35 @@ static void orc_column_tf(const orc_geom *g, const orc_view *v, int ix, int iy, 
 
 /* Axial footprint of voxel iz (geom/cbct/cbct_proj.c:382-411): returns the
  * number of detector rows touched (0 = none) and their weights. */
-static int orc_voxel_v(const orc_geom *g, const orc_column *c, int iz, int *ivmin, float *wv)
+static int orc_voxel_v(const orc_geom *g, const orc_column *c, int iz, int *ivmin, real *wv)
 {
-    float vmin = c->vstart + (float)iz * c->zinc;
-    float vmax = vmin + c->zinc;
-    vmin = vmin + 0.5f; if (!(vmin > 0.0f)) vmin = 0.0f;
-    vmax = vmax + 0.5f; if (!(vmax < (float)g->nv)) vmax = (float)g->nv;
+    real vmin = c->vstart + (real)iz * c->zinc;
+    real vmax = vmin + c->zinc;
+    vmin = vmin + (real)0.5; if (!(vmin > (real)0.0)) vmin = (real)0.0;
+    vmax = vmax + (real)0.5; if (!(vmax < (real)g->nv)) vmax = (real)g->nv;
     if (vmin > vmax) return 0;
-    int lo = (int)floorf(vmin), hi = (int)floorf(vmax);
+    int lo = (int)floor(vmin), hi = (int)floor(vmax);
     if (hi > g->nv - 1) hi = g->nv - 1;
     if (hi > lo + ORC_FP_V - 1) hi = lo + ORC_FP_V - 1;
     *ivmin = lo;
     if (lo == hi) {
         wv[0] = vmax - vmin;
     } else {
-        wv[0] = (float)(lo + 1) - vmin;
-        for (int k = 1; k < hi - lo; k++) wv[k] = 1.0f;
-        wv[hi - lo] = vmax - (float)hi;
+        wv[0] = (real)(lo + 1) - vmin;
+        for (int k = 1; k < hi - lo; k++) wv[k] = (real)1.0;
+        wv[hi - lo] = vmax - (real)hi;
     }
     return hi - lo + 1;
 }
 
 /* Axial amplitude of detector pixel (iu, iv) (geom/cbct/cbct_proj.c:432-450). */
-static float orc_ampv(const orc_geom *g, int iu, int iv)
+static real orc_ampv(const orc_geom *g, int iu, int iv)
 {
-    float u = ((float)iu + g->wu) * g->du;
-    float uu = g->sdd * g->sdd + u * u;
-    float v = ((float)iv + g->wv) * g->dv;
-    if (g->detector_type == 1) return (float)sqrt((double)((uu + v * v) / uu));
-    return (float)(sqrt((double)(g->sdd * g->sdd + v * v)) / (double)g->sdd);
+    real u = ((real)iu + g->wu) * g->du;
+    real uu = g->sdd * g->sdd + u * u;
+    real v = ((real)iv + g->wv) * g->dv;
+    if (g->detector_type == 1) return (real)sqrt((double)((uu + v * v) / uu));
+    return (real)(sqrt((double)(g->sdd * g->sdd + v * v)) / (double)g->sdd);
 }
 
 static void orc_column_eval(int kind, const orc_geom *g, const orc_view *v, int ix, int iy, orc_column *c)
@@ -252,16 +262,16 @@ static void orc_column_eval(int kind, const orc_geom *g, const orc_view *v, int 
 /* Forward projection A (proj,dd / proj,tf), geom/cbct/cbct_proj.c:217-456, :464-744. */
 int orc_proj(int kind, int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy, float oz, int nu,
              int nv, float du, float dv, float ou, float ov, float sad, float add, float sdd, int noviews,
-             const double *betas, const float *couchz, int detector_type, const float *image, float *proj,
+             const double *betas, const float *couchz, int detector_type, const real *image, real *proj,
              const bool *map)
 {
     (void)add;
     orc_geom g = orc_make_geom(nx, ny, nz, dx, dy, dz, ox, oy, oz, nu, nv, du, dv, ou, ov, sad, sdd, detector_type);
     long nxy = (long)nx * ny, nuv = (long)nu * nv;
-    memset(proj, 0, sizeof(float) * nuv * noviews);
+    memset(proj, 0, sizeof(real) * nuv * noviews);
     for (int ib = 0; ib < noviews; ib++) {
         orc_view v = orc_make_view(&g, betas[ib], couchz[ib]);
-        float *pv = proj + nuv * ib;
+        real *pv = proj + nuv * ib;
         for (int iy = 0; iy < ny; iy++) {
             for (int ix = 0; ix < nx; ix++) {
                 if (!map[iy * nx + ix]) continue;
@@ -269,10 +279,10 @@ int orc_proj(int kind, int nx, int ny, int nz, float dx, float dy, float dz, flo
                 orc_column_eval(kind, &g, &v, ix, iy, &c);
                 if (!c.hit) continue;
                 for (int iz = c.iz_start; iz < c.iz_stop; iz++) {
-                    float x = image[iz * nxy + (long)iy * nx + ix];
-                    if (x == 0.0f) continue;
-                    float voxel = c.ampu * x;
-                    float wv[ORC_FP_V];
+                    real x = image[iz * nxy + (long)iy * nx + ix];
+                    if (x == (real)0.0) continue;
+                    real voxel = c.ampu * x;
+                    real wv[ORC_FP_V];
                     int ivmin = 0;
                     int nrow = orc_voxel_v(&g, &c, iz, &ivmin, wv);
                     for (int iu = c.iumin; iu <= c.iumax; iu++)
@@ -290,18 +300,18 @@ int orc_proj(int kind, int nx, int ny, int nz, float dx, float dy, float dz, flo
 /* Matched backprojection A^T (back,dd / back,tf), geom/cbct/cbct_back.c:136-372, :375-653. */
 int orc_back(int kind, int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy, float oz, int nu,
              int nv, float du, float dv, float ou, float ov, float sad, float add, float sdd, int noviews,
-             const double *betas, const float *couchz, int detector_type, const float *proj, float *image,
+             const double *betas, const float *couchz, int detector_type, const real *proj, real *image,
              const bool *map)
 {
     (void)add;
     orc_geom g = orc_make_geom(nx, ny, nz, dx, dy, dz, ox, oy, oz, nu, nv, du, dv, ou, ov, sad, sdd, detector_type);
     long nxy = (long)nx * ny, nuv = (long)nu * nv;
-    float *scaled = (float *)malloc(sizeof(float) * (nuv > 0 ? nuv : 1));
+    real *scaled = (real *)malloc(sizeof(real) * (nuv > 0 ? nuv : 1));
     if (!scaled) return 0;
-    memset(image, 0, sizeof(float) * nxy * nz);
+    memset(image, 0, sizeof(real) * nxy * nz);
     for (int ib = 0; ib < noviews; ib++) {
         orc_view v = orc_make_view(&g, betas[ib], couchz[ib]);
-        const float *pv = proj + nuv * ib;
+        const real *pv = proj + nuv * ib;
         for (int iu = 0; iu < nu; iu++)
             for (int iv = 0; iv < nv; iv++) scaled[(long)iu * nv + iv] = pv[(long)iu * nv + iv] * orc_ampv(&g, iu, iv);
         for (int iy = 0; iy < ny; iy++) {
@@ -311,11 +321,11 @@ int orc_back(int kind, int nx, int ny, int nz, float dx, float dy, float dz, flo
                 orc_column_eval(kind, &g, &v, ix, iy, &c);
                 if (!c.hit) continue;
                 for (int iz = c.iz_start; iz < c.iz_stop; iz++) {
-                    float wv[ORC_FP_V];
+                    real wv[ORC_FP_V];
                     int ivmin = 0;
                     int nrow = orc_voxel_v(&g, &c, iz, &ivmin, wv);
                     if (!nrow) continue;
-                    float voxel = 0.0f;
+                    real voxel = (real)0.0;
                     for (int iu = c.iumin; iu <= c.iumax; iu++)
                         for (int k = 0; k < nrow; k++)
                             voxel += scaled[(long)iu * nv + ivmin + k] * c.w[iu - c.iumin] * wv[k];
@@ -332,57 +342,57 @@ int orc_back(int kind, int nx, int ny, int nz, float dx, float dy, float dz, flo
  * and back,hpd (off_boundary = 0): geom/cbct/cbct_back.c:7-133. */
 int orc_back_pd(int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy, float oz, int nu, int nv,
                 float du, float dv, float ou, float ov, float sad, float add, float sdd, int noviews,
-                const double *betas, const float *couchz, int detector_type, const float *proj, float *image,
+                const double *betas, const float *couchz, int detector_type, const real *proj, real *image,
                 const bool *map, int off_boundary)
 {
     (void)add;
     orc_geom g = orc_make_geom(nx, ny, nz, dx, dy, dz, ox, oy, oz, nu, nv, du, dv, ou, ov, sad, sdd, detector_type);
     long nxy = (long)nx * ny, nuv = (long)nu * nv;
-    float wz = orc_centre(nz, oz); /* no couch term here: geom/cbct/cbct_back.c:47 */
-    memset(image, 0, sizeof(float) * nxy * nz);
+    real wz = orc_centre(nz, oz); /* no couch term here: geom/cbct/cbct_back.c:47 */
+    memset(image, 0, sizeof(real) * nxy * nz);
     for (int ib = 0; ib < noviews; ib++) {
-        float sin_a = (float)sin(betas[ib]);
-        float cos_a = (float)cos(betas[ib]);
+        real sin_a = (real)sin(betas[ib]);
+        real cos_a = (real)cos(betas[ib]);
         int couch = (int)couchz[ib]; /* truncated to int: geom/cbct/cbct_back.c:43,52 */
-        const float *pv = proj + nuv * ib;
+        const real *pv = proj + nuv * ib;
         for (int iy = 0; iy < ny; iy++) {
             for (int ix = 0; ix < nx; ix++) {
                 if (!map[iy * nx + ix]) continue;
-                float xc = ((float)ix + g.wx) * dx;
-                float yc = ((float)iy + g.wy) * dy;
-                float xr = xc * cos_a - yc * sin_a;
-                float yr = xc * sin_a + yc * cos_a;
-                float w2, w2s, u;
+                real xc = ((real)ix + g.wx) * dx;
+                real yc = ((real)iy + g.wy) * dy;
+                real xr = xc * cos_a - yc * sin_a;
+                real yr = xc * sin_a + yc * cos_a;
+                real w2, w2s, u;
                 if (detector_type == 1) {
                     w2 = sdd / (sad + yr);
                     w2s = w2 * w2;
                     u = xr * w2 / du - g.wu;
                 } else {
-                    float roff = ou * du * sad / sdd;
-                    u = (float)(atan((double)((xr - roff) / (sad + yr))) * (double)sdd / (double)du - (double)g.wu);
+                    real roff = ou * du * sad / sdd;
+                    u = (real)(atan((double)((xr - roff) / (sad + yr))) * (double)sdd / (double)du - (double)g.wu);
                     w2s = sdd * sdd / ((sad + yr) * (sad + yr) + (xr - roff) * (xr - roff));
                     w2 = sdd / (sad + yr);
                 }
                 if ((double)u < 1e-6 || (double)u > (double)nu - 1.0 - 1e-6) continue;
-                int iu = (int)floorf(u);
-                float wul = u - (float)iu;
+                int iu = (int)floor(u);
+                real wul = u - (real)iu;
                 for (int iz = 0; iz < nz; iz++) {
-                    float zc = ((float)iz + wz) * dz + (float)couch;
-                    float vv = zc * w2 / dv - g.wv;
+                    real zc = ((real)iz + wz) * dz + (real)couch;
+                    real vv = zc * w2 / dv - g.wv;
                     if (off_boundary) {
                         if ((double)vv < 1e-6) continue;
                         if ((double)vv > (double)nv - 1.0 - 1e-6) break;
                     } else {
-                        vv = (float)((double)vv > 0.5 ? (double)vv : 0.5);
-                        vv = (float)((double)vv < (double)nv - 1.5 ? (double)vv : (double)nv - 1.5);
+                        vv = (real)((double)vv > 0.5 ? (double)vv : 0.5);
+                        vv = (real)((double)vv < (double)nv - 1.5 ? (double)vv : (double)nv - 1.5);
                     }
-                    int iv = (int)floorf(vv);
-                    float wvl = vv - (float)iv;
-                    const float *p = pv + (long)iu * nv + iv;
-                    float s0 = (1.0f - wvl) * p[0] + wvl * p[1];
-                    float s1 = (1.0f - wvl) * p[nv] + wvl * p[nv + 1];
+                    int iv = (int)floor(vv);
+                    real wvl = vv - (real)iv;
+                    const real *p = pv + (long)iu * nv + iv;
+                    real s0 = ((real)1.0 - wvl) * p[0] + wvl * p[1];
+                    real s1 = ((real)1.0 - wvl) * p[nv] + wvl * p[nv + 1];
                     long idx = iz * nxy + (long)iy * nx + ix;
-                    image[idx] = image[idx] + w2s * ((1.0f - wul) * s0 + wul * s1);
+                    image[idx] = image[idx] + w2s * (((real)1.0 - wul) * s0 + wul * s1);
                 }
             }
         }

@@ -81,8 +81,12 @@ def quad_penalty(x, mode):
     return _penalty(x, mode, lambda d: float((d.astype(np.float64) ** 2 / 2).sum()), lambda d: d, None)
 
 
-def recon_pwls_se_sqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0):
-    """reconPwlsSeSqs.m with the SF projectors of loadPojectors.m; returns (x, phis, rmsds)."""
+def recon_pwls_se_sqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0, fp64=False, history=None):
+    """reconPwlsSeSqs.m with the SF projectors of loadPojectors.m; returns (x, phis, rmsds).
+    ``fp64`` runs the same iteration in double with the FP64 projectors (the FP64 oracle);
+    ``history``, if a list, receives a copy of x after every outer iteration."""
+    if fp64:
+        return _recon_pwls_fp64(y, w, geom, beta, pfun, itnlim, delta, numos, img0, history)
     if pfun == "huber":
         R = lambda x: huber_penalty(x, 0, delta)
         S = lambda x: huber_penalty(x, 1, delta)
@@ -120,5 +124,67 @@ def recon_pwls_se_sqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0):
         phis.append(phi)
         rmsds.append(rmsd)
         if itn > 5 and rmsd < 1e-5:
+            break
+    return x, np.array(phis), np.array(rmsds)
+
+
+def _penalty64(x, mode, kind, delta):
+    """huberPenalty.m / quadPenalty.m in double (same neighbourhood as _penalty)."""
+    X = np.asarray(x, dtype=np.float64).transpose(2, 1, 0)
+    pairs = [((slice(0, -1), slice(None), slice(None)), (slice(1, None), slice(None), slice(None)), 1.0),
+             ((slice(None), slice(0, -1), slice(None)), (slice(None), slice(1, None), slice(None)), 1.0),
+             ((slice(0, -1), slice(0, -1), slice(None)), (slice(1, None), slice(1, None), slice(None)), 1 / np.sqrt(2)),
+             ((slice(1, None), slice(0, -1), slice(None)), (slice(0, -1), slice(1, None), slice(None)), 1 / np.sqrt(2)),
+             ((slice(None), slice(None), slice(0, -1)), (slice(None), slice(None), slice(1, None)), 0.5)]
+    if kind == "quad" and mode == 2:
+        return np.full(np.asarray(x).shape, 4 + 4 / np.sqrt(2) + 1.0)
+    if mode == 0:
+        tot = 0.0
+        for p, q, c in pairs:
+            d = np.abs(X[p] - X[q])
+            h = d ** 2 / 2 if kind == "quad" else np.where(d > delta, delta * d - delta ** 2 / 2, d ** 2 / 2)
+            tot += c * h.sum()
+        return tot
+    y = np.zeros(X.shape)
+    for p, q, c in pairs:
+        d = X[p] - X[q]
+        if mode == 1:
+            g = d if kind == "quad" else np.clip(d, -delta, delta)
+            y[p] += c * g
+            y[q] -= c * g
+        else:
+            g = (np.abs(d) <= delta).astype(np.float64)
+            y[p] += c * g
+            y[q] += c * g
+    return y.transpose(2, 1, 0).copy()
+
+
+def _recon_pwls_fp64(y, w, geom, beta, pfun, itnlim, delta, M, img0, history):
+    x = np.asarray(img0, dtype=np.float64).copy()
+    y = np.asarray(y, dtype=np.float64)
+    w = np.asarray(w, dtype=np.float64)
+    a = oracle_cbct("proj,tf", geom, np.ones_like(x), fp64=True)
+    precom = oracle_cbct("back,tf", geom, w * a, fp64=True)
+    phis, rmsds = [], []
+    for itn in range(1, itnlim + 1):
+        xold = x.copy()
+        phi = 0.0
+        for isub in range(1, M + 1):
+            g = geom.subset(M, isub)
+            start = isub % M if M > 1 else 0
+            ys = y[start::M] if M > 1 else y
+            ws = w[start::M] if M > 1 else w
+            d = oracle_cbct("proj,tf", g, x, fp64=True) - ys
+            num = M * oracle_cbct("back,tf", g, ws * d, fp64=True) + beta * _penalty64(x, 1, pfun, delta)
+            den = precom + beta * _penalty64(x, 2, pfun, delta)
+            x = x - num / den
+            x[~np.isfinite(x) | (x < 0)] = 0
+            phi += float((ws * d ** 2).sum()) / 2
+        phi += beta * _penalty64(x, 0, pfun, delta)
+        phis.append(phi)
+        rmsds.append(float(np.sqrt(np.mean((x - xold) ** 2))))
+        if history is not None:
+            history.append(x.copy())
+        if itn > 5 and rmsds[-1] < 1e-5:
             break
     return x, np.array(phis), np.array(rmsds)
