@@ -370,6 +370,78 @@ def extras(plan, xd, yd, sino, img, vv):
     return out
 
 
+def run_serving(args):
+    """Served reconstruction: a seeded mix of FDK and OS-PWLS requests (random_geometry:
+    volumes 128^2x64 .. 384^2x160, 180-720 views, 20% short scan, 20% offset detector;
+    70% FDK, 30% OS-PWLS with 12 subsets x 10 iterations) through ReconServer, against the
+    plain single-instance FP32 path (serve_sequential: reconFDK / reconPwlsSeSqs one
+    request at a time, host arrays in and out).  Closed loop (all requests queued at 0)
+    for throughput, then Poisson arrivals at fractions of the served capacity for the
+    p50/p99 latency."""
+    import copy
+    import torch
+    from ctsim_b200.serving import ReconServer, latency_stats, make_requests, serve_sequential
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(args.seed)
+
+    def fresh(reqs, storage, arrivals=None):
+        out = []
+        for i, r in enumerate(reqs):
+            c = copy.copy(r)
+            c.storage = storage
+            c.arrival = 0.0 if arrivals is None else float(arrivals[i])
+            c.result = None
+            out.append(c)
+        return out
+
+    def served(reqs, **kw):
+        srv = ReconServer(max_active=args.slots, **kw)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        done = srv.run(reqs)
+        torch.cuda.synchronize()
+        return done, time.perf_counter() - t0, srv
+
+    warm = make_requests(4, seed=args.seed + 1, scale=0.25, iterations=2, subsets=4, fdk_fraction=0.5)
+    served(fresh(warm, "bfloat16"))
+    serve_sequential(fresh(warm, "float32"))
+    reqs = make_requests(args.requests, seed=args.seed, scale=args.scale, iterations=10, subsets=12)
+    kinds = [r.kind for r in reqs]
+    clocks = ClockSampler(0)
+    clocks.start()
+    plain = serve_sequential(fresh(reqs, "float32"))
+    t_plain = max(r.t_done for r in plain)
+    plain_rps = len(plain) / t_plain
+    done32, t32, _ = served(fresh(reqs, "float32"))
+    done16, t16, srv16 = served(fresh(reqs, "bfloat16"))
+    cap = len(done16) / t16
+    sweep = []
+    for frac in (0.5, 0.8):
+        rate = frac * cap
+        arr = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+        d, t, _ = served(fresh(reqs, "bfloat16", arr))
+        st = latency_stats(d, t)
+        st.update({"offered_req_per_s": rate, "load_fraction": frac})
+        sweep.append(st)
+    clk = clocks.stop()
+    closed = latency_stats(done16, t16)
+    line = {
+        "metric": "served reconstructions/s (FDK + OS-PWLS mix)", "value": cap, "unit": "req/s",
+        "impl": "serving", "n_gpus": 1, "higher_is_better": True, "dtype": "bf16 storage, fp32 arithmetic",
+        "data": "synthetic (seeded ellipsoid phantoms, Poisson counts)",
+        "config": {"workload": "random_geometry mix", "requests": len(reqs), "fdk": kinds.count("fdk"),
+                   "pwls": kinds.count("pwls"), "pwls_iterations": 10, "pwls_subsets": 12, "slots": args.slots,
+                   "scale": args.scale, "seed": args.seed},
+        "plain_fp32_single_instance_req_per_s": plain_rps,
+        "served_fp32_req_per_s": len(done32) / t32,
+        "speedup_vs_plain_fp32": cap / plain_rps,
+        "closed_loop": closed, "open_loop": sweep, "peak_hbm_admitted_bytes": srv16.peak_used,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -380,8 +452,15 @@ def main():
     ap.add_argument("--extras", action="store_true", help="also time SF A/A^T and FDK back,hpd")
     ap.add_argument("--views", type=int, default=0, help="keep only this many views (profiling captures)")
     ap.add_argument("--no-e2e", dest="no_e2e", action="store_true", help="skip the end-to-end host-buffer leg")
+    ap.add_argument("--serving", action="store_true", help="served FDK/OS-PWLS request mix instead of A/A^T")
+    ap.add_argument("--requests", type=int, default=24, help="requests of the serving run")
+    ap.add_argument("--slots", type=int, default=8, help="concurrent requests of the serving run")
+    ap.add_argument("--scale", type=float, default=1.0, help="size scale of the serving run's geometries")
+    ap.add_argument("--seed", type=int, default=7)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.serving:
+        run_serving(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

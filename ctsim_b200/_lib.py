@@ -25,7 +25,8 @@ EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd
             "ctsim_fdk_create", "ctsim_fdk_destroy", "ctsim_fdk_filter", "ctsim_fdk_run", "ctsim_fdk_dbeta",
             "ctsim_fdk_design_filter", "ctsim_pwls_weights", "ctsim_pwls_residual", "ctsim_sqdiff",
             "ctsim_penalty", "ctsim_sqs_update", "ctsim_plan_project_ex", "ctsim_plan_backproject_ex",
-            "ctsim_pwls_residual_ex"]
+            "ctsim_pwls_residual_ex", "ctsim_fdk_filter_ex", "ctsim_fdk_run_ex",
+            "ctsim_plan_create_async", "ctsim_pool_trim"]
 
 
 class CtsimGeom(C.Structure):
@@ -75,6 +76,10 @@ def load():
     L.ctsim_cbct_geom.restype = C.c_bool
     L.ctsim_plan_create.argtypes = [C.POINTER(CtsimGeom), _p, _p, _p, C.POINTER(_p)]
     L.ctsim_plan_create.restype = _i
+    L.ctsim_plan_create_async.argtypes = [C.POINTER(CtsimGeom), _p, _p, _p, _p, C.POINTER(_p)]
+    L.ctsim_plan_create_async.restype = _i
+    L.ctsim_pool_trim.argtypes = [C.c_size_t]
+    L.ctsim_pool_trim.restype = _i
     L.ctsim_plan_destroy.argtypes = [_p]
     L.ctsim_plan_destroy.restype = _i
     L.ctsim_plan_device_bytes.argtypes = [_p]
@@ -99,6 +104,10 @@ def load():
     L.ctsim_fdk_filter.restype = _i
     L.ctsim_fdk_run.argtypes = [_p, _p, _p, _p]
     L.ctsim_fdk_run.restype = _i
+    L.ctsim_fdk_filter_ex.argtypes = [_p, _p, _i, _p, _p]
+    L.ctsim_fdk_filter_ex.restype = _i
+    L.ctsim_fdk_run_ex.argtypes = [_p, _p, _i, _p, _p]
+    L.ctsim_fdk_run_ex.restype = _i
     L.ctsim_fdk_dbeta.argtypes = [_p]
     L.ctsim_fdk_dbeta.restype = _f
     L.ctsim_fdk_design_filter.argtypes = [_i, _f, _f, _i, C.c_char_p, _f, _p, C.POINTER(_i)]

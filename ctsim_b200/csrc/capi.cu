@@ -3,6 +3,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -66,6 +68,9 @@ struct ctsim_plan {
     bool fwd_ok = true;
     std::string fwd_reason;
     std::vector<double> betas;  // host copy of the view angles (FDK weights need them)
+    // stream-ordered plans allocate from the library pool on this stream and free there
+    bool stream_ordered = false;
+    cudaStream_t stream = nullptr;
 };
 
 // Plan internals for other translation units (fdk.cu).
@@ -79,19 +84,89 @@ extern "C" const char *ctsim_last_error(void) { return g_last_error.c_str(); }
 ctsim_status ctsim_set_last_error(ctsim_status s, const char *msg) { return fail(s, msg); }
 extern "C" const char *ctsim_version(void) { return "ctsim_b200 0.1 (sm_100a)"; }
 
+// Library memory pool of a device for stream-ordered plans: memory freed by a
+// finished request stays in the pool (release threshold: unlimited) and serves the
+// next request's allocations without a device-wide synchronisation.
+static cudaError_t library_pool(int dev, cudaMemPool_t *out) {
+    static std::mutex m;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(m);
+    auto it = pools.find(dev);
+    if (it != pools.end()) {
+        *out = it->second;
+        return cudaSuccess;
+    }
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = ~0ull;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+    pools[dev] = pool;
+    *out = pool;
+    return cudaSuccess;
+}
+
+// Allocation, release and upload for a plan and the objects built on it (FDK): the
+// runtime's synchronous calls, or stream-ordered ones on the plan's stream.
+cudaError_t ctsim_plan_alloc(const ctsim_plan *p, void **ptr, size_t n) {
+    if (!p->stream_ordered) return cudaMalloc(ptr, n);
+    cudaMemPool_t pool;
+    cudaError_t e = library_pool(p->device, &pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(ptr, n, pool, p->stream);
+}
+void ctsim_plan_release(const ctsim_plan *p, void *ptr) {
+    if (!ptr) return;
+    if (p->stream_ordered) cudaFreeAsync(ptr, p->stream);
+    else cudaFree(ptr);
+}
+// Host source may be released when this returns (pageable copies are staged).
+cudaError_t ctsim_plan_upload(const ctsim_plan *p, void *dst, const void *src, size_t n) {
+    if (!p->stream_ordered) return cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice);
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, p->stream);
+}
+
 static void free_plan(ctsim_plan *p) {
     if (!p) return;
-    cudaFree(p->d_views);
-    cudaFree(p->d_ampv);
-    cudaFree(p->d_map);
-    cudaFree(p->d_xs);
-    cudaFree(p->d_ps);
-    cudaFree(p->d_err);
+    ctsim_plan_release(p, p->d_views);
+    ctsim_plan_release(p, p->d_ampv);
+    ctsim_plan_release(p, p->d_map);
+    ctsim_plan_release(p, p->d_xs);
+    ctsim_plan_release(p, p->d_ps);
+    ctsim_plan_release(p, p->d_err);
     delete p;
 }
 
+static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, const float *couchz, const bool *map,
+                                bool stream_ordered, cudaStream_t stream, ctsim_plan **out);
+
 extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *betas, const float *couchz,
                                           const bool *map, ctsim_plan **out) {
+    return create_plan(geom, betas, couchz, map, false, nullptr, out);
+}
+
+extern "C" ctsim_status ctsim_plan_create_async(const ctsim_geom *geom, const double *betas, const float *couchz,
+                                                const bool *map, void *stream, ctsim_plan **out) {
+    return create_plan(geom, betas, couchz, map, true, (cudaStream_t)stream, out);
+}
+
+extern "C" ctsim_status ctsim_pool_trim(size_t keep_bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    cudaMemPool_t pool;
+    if ((e = library_pool(dev, &pool)) != cudaSuccess) return cuda_fail(e, "memory pool");
+    if ((e = cudaMemPoolTrimTo(pool, keep_bytes)) != cudaSuccess) return cuda_fail(e, "cudaMemPoolTrimTo");
+    return CTSIM_OK;
+}
+
+static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, const float *couchz, const bool *map,
+                                bool stream_ordered, cudaStream_t stream, ctsim_plan **out) {
     if (!geom || !betas || !couchz || !out) return fail(CTSIM_ERR_ARGUMENT, "null argument");
     *out = nullptr;
     const ctsim_geom G = *geom;
@@ -115,6 +190,8 @@ extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *
     ctsim_plan *p = new ctsim_plan();
     p->geom = G;
     p->device = dev;
+    p->stream_ordered = stream_ordered;
+    p->stream = stream;
     p->betas.assign(betas, betas + G.noviews);
     Geom &g = p->g;
     g.nx = G.nx; g.ny = G.ny; g.nz = G.nz; g.nu = G.nu; g.nv = G.nv; g.det = G.detector_type;
@@ -225,10 +302,10 @@ extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *
     size_t bytes = 0;
 #define CTSIM_ALLOC(ptr, n)                                                          \
     do {                                                                             \
-        e = cudaMalloc((void **)&(ptr), (n));                                        \
+        e = ctsim_plan_alloc(p, (void **)&(ptr), (n));                               \
         if (e != cudaSuccess) {                                                      \
             free_plan(p);                                                            \
-            return fail(CTSIM_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e)); \
+            return fail(CTSIM_ERR_ALLOC, std::string("device allocation: ") + cudaGetErrorString(e)); \
         }                                                                            \
         bytes += (n);                                                                \
     } while (0)
@@ -240,10 +317,11 @@ extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *
     CTSIM_ALLOC(p->d_ps, sizeof(float) * (size_t)G.nu * G.nv * G.noviews);
 #undef CTSIM_ALLOC
     p->bytes = bytes;
-    if ((e = cudaMemcpy(p->d_views, views.data(), sizeof(View) * G.noviews, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(p->d_ampv, ampv.data(), sizeof(float) * ampv.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(p->d_map, mp.data(), mp.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemset(p->d_err, 0, sizeof(int))) != cudaSuccess) {
+    if ((e = ctsim_plan_upload(p, p->d_views, views.data(), sizeof(View) * G.noviews)) != cudaSuccess ||
+        (e = ctsim_plan_upload(p, p->d_ampv, ampv.data(), sizeof(float) * ampv.size())) != cudaSuccess ||
+        (e = ctsim_plan_upload(p, p->d_map, mp.data(), mp.size())) != cudaSuccess ||
+        (e = stream_ordered ? cudaMemsetAsync(p->d_err, 0, sizeof(int), stream)
+                            : cudaMemset(p->d_err, 0, sizeof(int))) != cudaSuccess) {
         free_plan(p);
         return cuda_fail(e, "plan upload");
     }

@@ -21,6 +21,9 @@ extern ctsim_status ctsim_set_last_error(ctsim_status s, const char *msg);
 // plan internals shared with capi.cu
 extern const double *ctsim_plan_betas(const ctsim_plan *p);
 extern const ctsim_geom *ctsim_plan_geom(const ctsim_plan *p);
+extern cudaError_t ctsim_plan_alloc(const ctsim_plan *p, void **ptr, size_t n);
+extern void ctsim_plan_release(const ctsim_plan *p, void *ptr);
+extern cudaError_t ctsim_plan_upload(const ctsim_plan *p, void *dst, const void *src, size_t n);
 
 namespace {
 
@@ -41,6 +44,35 @@ bool window_known(const std::string &w) {
     return false;
 }
 
+// |DFT(h)|[0..count) by an iterative radix-2 FFT in double (size a power of two);
+// every twiddle is evaluated directly (no recurrence).
+std::vector<double> dft_magnitude(const std::vector<double> &h, int count) {
+    const int n = (int)h.size();
+    int lg = 0;
+    while ((1 << lg) < n) lg++;
+    std::vector<std::complex<double>> a(n);
+    for (int i = 0; i < n; i++) {
+        int r = 0;
+        for (int b = 0; b < lg; b++) r |= ((i >> b) & 1) << (lg - 1 - b);
+        a[r] = h[i];
+    }
+    for (int len = 2; len <= n; len <<= 1) {
+        const int hl = len / 2;
+        for (int j = 0; j < hl; j++) {
+            const double ang = -2.0 * M_PI * j / len;
+            const std::complex<double> w(std::cos(ang), std::sin(ang));
+            for (int i = 0; i < n; i += len) {
+                const std::complex<double> u = a[i + j], v = a[i + j + hl] * w;
+                a[i + j] = u + v;
+                a[i + j + hl] = u - v;
+            }
+        }
+    }
+    std::vector<double> m(count);
+    for (int k = 0; k < count; k++) m[k] = std::sqrt(a[k].real() * a[k].real() + a[k].imag() * a[k].imag());
+    return m;
+}
+
 // designFilter2.m:18-78 (flat) / designEquiangularFilter2.m:19-78 (curved), in double.
 // gamma = du; SDD used by the equiangular kernel.  Returns H[order].
 std::vector<double> design_filter(int nu, double du, double sdd, bool flat, const std::string &window, double crop) {
@@ -56,19 +88,9 @@ std::vector<double> design_filter(int nu, double du, double sdd, bool flat, cons
             h[n] = -1.0 / (d * d);
         }
     }
-    // filt = abs(fft(h)), first order/2+1 bins (direct DFT in double; once per plan)
+    // filt = abs(fft(h)), first order/2+1 bins
     const int half = order / 2 + 1;
-    std::vector<double> filt(half);
-    for (int k = 0; k < half; k++) {
-        double re = 0.0, im = 0.0;
-        for (int n = 0; n < order; n++) {
-            if (h[n] == 0.0) continue;
-            const double a = -2.0 * M_PI * (double)((long long)k * n % order) / order;
-            re += h[n] * std::cos(a);
-            im += h[n] * std::sin(a);
-        }
-        filt[k] = std::sqrt(re * re + im * im);
-    }
+    std::vector<double> filt = dft_magnitude(h, half);
     std::string win = window;
     if (win == "hann50" || win == "B50" || win == "C50") crop = 0.5;
     if (win == "hann75" || win == "B75" || win == "C75") crop = 0.75;
@@ -104,7 +126,8 @@ double parker_s(double b) {
 // radix-2 decimation in time on bit-reversed input; inverse: decimation in
 // frequency from natural order, read back bit-reversed.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) fdk_filter_kernel(const float *__restrict__ sino, float *__restrict__ out,
+__global__ void __launch_bounds__(256) fdk_filter_kernel(const void *__restrict__ sino, int in_dtype,
+                                                         float *__restrict__ out,
                                                          const float *__restrict__ wcos,
                                                          const float *__restrict__ parker,
                                                          const float *__restrict__ H, const float2 *__restrict__ tw,
@@ -113,7 +136,7 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(const float *__restrict
     const int k = blockIdx.y;
     const int iv0 = blockIdx.x * kFiltRows;
     const size_t nuv = (size_t)nu * nv;
-    const float *sv = sino + (size_t)k * nuv;
+    const size_t vbase = (size_t)k * nuv;
     float *ov = out + (size_t)k * nuv;
     const int t = threadIdx.x;
     const int sh = 32 - log2L;
@@ -123,7 +146,7 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(const float *__restrict
         float x = 0.0f;
         if (iu < nu && iv0 + r < nv) {
             const size_t o = (size_t)iu * nv + iv0 + r;
-            x = sv[o] * wcos[o];  // reconFDK.m:54
+            x = load_as_float(sino, vbase + o, in_dtype) * wcos[o];  // reconFDK.m:54
             if (parker) x = x * parker[(size_t)k * nu + iu];  // reconFDK.m:66-68
         }
         const int pos = __brev(iu) >> sh;
@@ -204,13 +227,15 @@ extern "C" ctsim_status ctsim_fdk_design_filter(int nu, float du, float sdd, int
     return CTSIM_OK;
 }
 
+// Device memory follows the plan's allocation mode (stream-ordered plans: on the
+// plan's stream), so an FDK object is destroyed before its plan.
 static void free_fdk(ctsim_fdk *f) {
     if (!f) return;
-    cudaFree(f->d_H);
-    cudaFree(f->d_wcos);
-    cudaFree(f->d_parker);
-    cudaFree(f->d_filtered);
-    cudaFree(f->d_tw);
+    ctsim_plan_release(f->plan, f->d_H);
+    ctsim_plan_release(f->plan, f->d_wcos);
+    ctsim_plan_release(f->plan, f->d_parker);
+    ctsim_plan_release(f->plan, f->d_filtered);
+    ctsim_plan_release(f->plan, f->d_tw);
     delete f;
 }
 
@@ -278,19 +303,19 @@ extern "C" ctsim_status ctsim_fdk_create(ctsim_plan *plan, const char *window, f
 
     cudaError_t e;
     const size_t nsino = (size_t)G.nu * G.nv * G.noviews;
-    if ((e = cudaMalloc(&f->d_H, sizeof(float) * f->L)) != cudaSuccess ||
-        (e = cudaMalloc(&f->d_wcos, sizeof(float) * wcos.size())) != cudaSuccess ||
-        (e = cudaMalloc(&f->d_tw, sizeof(float2) * tw.size())) != cudaSuccess ||
-        (e = cudaMalloc(&f->d_filtered, sizeof(float) * nsino)) != cudaSuccess ||
-        (short_scan && (e = cudaMalloc(&f->d_parker, sizeof(float) * parker.size())) != cudaSuccess)) {
+    const ctsim_plan *p = plan;
+    if ((e = ctsim_plan_alloc(p, (void **)&f->d_H, sizeof(float) * f->L)) != cudaSuccess ||
+        (e = ctsim_plan_alloc(p, (void **)&f->d_wcos, sizeof(float) * wcos.size())) != cudaSuccess ||
+        (e = ctsim_plan_alloc(p, (void **)&f->d_tw, sizeof(float2) * tw.size())) != cudaSuccess ||
+        (e = ctsim_plan_alloc(p, (void **)&f->d_filtered, sizeof(float) * nsino)) != cudaSuccess ||
+        (short_scan && (e = ctsim_plan_alloc(p, (void **)&f->d_parker, sizeof(float) * parker.size())) != cudaSuccess)) {
         free_fdk(f);
         return ctsim_set_last_error(CTSIM_ERR_ALLOC, cudaGetErrorString(e));
     }
-    if ((e = cudaMemcpy(f->d_H, H.data(), sizeof(float) * f->L, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(f->d_wcos, wcos.data(), sizeof(float) * wcos.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMemcpy(f->d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (short_scan &&
-         (e = cudaMemcpy(f->d_parker, parker.data(), sizeof(float) * parker.size(), cudaMemcpyHostToDevice)) != cudaSuccess)) {
+    if ((e = ctsim_plan_upload(p, f->d_H, H.data(), sizeof(float) * f->L)) != cudaSuccess ||
+        (e = ctsim_plan_upload(p, f->d_wcos, wcos.data(), sizeof(float) * wcos.size())) != cudaSuccess ||
+        (e = ctsim_plan_upload(p, f->d_tw, tw.data(), sizeof(float2) * tw.size())) != cudaSuccess ||
+        (short_scan && (e = ctsim_plan_upload(p, f->d_parker, parker.data(), sizeof(float) * parker.size())) != cudaSuccess)) {
         free_fdk(f);
         return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
     }
@@ -303,21 +328,29 @@ extern "C" ctsim_status ctsim_fdk_destroy(ctsim_fdk *f) {
     return CTSIM_OK;
 }
 
-extern "C" ctsim_status ctsim_fdk_filter(ctsim_fdk *f, const float *d_sino, float *d_filtered, void *stream) {
+extern "C" ctsim_status ctsim_fdk_filter_ex(ctsim_fdk *f, const void *d_sino, int sino_dtype, float *d_filtered,
+                                            void *stream) {
     if (!f || !d_sino || !d_filtered) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    if (sino_dtype < kF32 || sino_dtype > kF16) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "unknown storage type");
     const size_t sm = sizeof(float2) * 4 * f->L;
     if (sm > 200 * 1024) return ctsim_set_last_error(CTSIM_ERR_UNSUPPORTED, "detector too wide for the row filter");
-    cudaError_t e = cudaFuncSetAttribute(fdk_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = allow_dynamic_smem((const void *)fdk_filter_kernel, sm);
     if (e != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
     dim3 grid((f->nv + kFiltRows - 1) / kFiltRows, f->nviews);
-    fdk_filter_kernel<<<grid, 256, sm, (cudaStream_t)stream>>>(d_sino, d_filtered, f->d_wcos, f->d_parker, f->d_H,
+    fdk_filter_kernel<<<grid, 256, sm, (cudaStream_t)stream>>>(d_sino, sino_dtype, d_filtered, f->d_wcos, f->d_parker, f->d_H,
                                                                 f->d_tw, f->nu, f->nv, f->L, f->log2L);
     if ((e = cudaGetLastError()) != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
     return CTSIM_OK;
 }
 
-extern "C" ctsim_status ctsim_fdk_run(ctsim_fdk *f, const float *d_sino, float *d_image, void *stream) {
-    ctsim_status s = ctsim_fdk_filter(f, d_sino, f->d_filtered, stream);
+extern "C" ctsim_status ctsim_fdk_filter(ctsim_fdk *f, const float *d_sino, float *d_filtered, void *stream) {
+    return ctsim_fdk_filter_ex(f, d_sino, kF32, d_filtered, stream);
+}
+
+extern "C" ctsim_status ctsim_fdk_run_ex(ctsim_fdk *f, const void *d_sino, int sino_dtype, float *d_image,
+                                         void *stream) {
+    if (!f) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    ctsim_status s = ctsim_fdk_filter_ex(f, d_sino, sino_dtype, f->d_filtered, stream);
     if (s != CTSIM_OK) return s;
     // img = backProjectMex(sino, geom, 1, 0, 'back,hpd') * dbeta * 10  (reconFDK.m:84)
     s = ctsim_plan_backproject(f->plan, CTSIM_BACK_HPD, f->d_filtered, d_image, 0, 1, f->nviews, f->dbeta, stream);
@@ -326,6 +359,10 @@ extern "C" ctsim_status ctsim_fdk_run(ctsim_fdk *f, const float *d_sino, float *
     cudaError_t e = launch_scale(d_image, (size_t)G.nx * G.ny * G.nz, 10.0f, (cudaStream_t)stream);
     if (e != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
     return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_fdk_run(ctsim_fdk *f, const float *d_sino, float *d_image, void *stream) {
+    return ctsim_fdk_run_ex(f, d_sino, kF32, d_image, stream);
 }
 
 extern "C" float ctsim_fdk_dbeta(const ctsim_fdk *f) { return f ? f->dbeta : 0.0f; }

@@ -9,6 +9,10 @@
 // Layouts (reference MEX conventions): image[iz][iy][ix], proj[view][iu][iv].
 #include "kernels.cuh"
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 namespace ctsim {
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -562,6 +566,23 @@ __global__ void scale_kernel(float *__restrict__ y, size_t n, float s) {
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
+// The dynamic shared-memory limit is a per-function, per-device attribute shared by
+// every plan, stream and captured graph of the process; it is only ever raised, so
+// a launch recorded earlier (another request's stream, a CUDA graph) stays valid.
+cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes) {
+    static std::mutex m;
+    static std::map<std::pair<int, const void *>, size_t> granted;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(m);
+    size_t &g = granted[{dev, kfn}];
+    if (bytes <= g) return cudaSuccess;
+    e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) g = bytes;
+    return e;
+}
+
 size_t back_smem_bytes(int qcap) { return (size_t)8 * (32 * 17 + 2 * qcap) * sizeof(float); }
 
 template <int METHOD, int MZ, bool VEC>
@@ -571,7 +592,7 @@ static cudaError_t launch_back_mz(const Geom &g, const View *views, const float 
     const int blocks = g.ny * ((g.nx + 7) / 8);
     const size_t sm = back_smem_bytes(qcap);
     auto kfn = back_kernel<METHOD, MZ, VEC>;
-    cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = allow_dynamic_smem((const void *)kfn, sm);
     if (e != cudaSuccess) return e;
     kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap, err, nullptr);
     return cudaGetLastError();
@@ -623,11 +644,11 @@ cudaError_t launch_proj(int method, const Geom &g, const View *views, const floa
     // one thread per 4 detector rows (up to 256 threads per block, more rows loop)
     const int nt = proj_threads(g.nv);
     if (method == kDD) {
-        cudaError_t e = cudaFuncSetAttribute(proj_kernel<kDD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = allow_dynamic_smem((const void *)proj_kernel<kDD>, sm);
         if (e != cudaSuccess) return e;
         proj_kernel<kDD><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin);
     } else {
-        cudaError_t e = cudaFuncSetAttribute(proj_kernel<kTF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = allow_dynamic_smem((const void *)proj_kernel<kTF>, sm);
         if (e != cudaSuccess) return e;
         proj_kernel<kTF><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin);
     }
@@ -668,7 +689,7 @@ static cudaError_t launch_back_unscaled_mz(const Geom &g, const View *views, con
     const int blocks = g.ny * ((g.nx + 7) / 8);
     const size_t sm = back_smem_bytes(qcap);
     auto kfn = back_kernel<METHOD, MZ, false, false>;
-    cudaError_t e = cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = allow_dynamic_smem((const void *)kfn, sm);
     if (e != cudaSuccess) return e;
     kfn<<<blocks, 256, sm, st>>>(g, views, proj, map, image, kF32, 0, 1, vc, 1.0f, qcap, err, ampv);
     return cudaGetLastError();

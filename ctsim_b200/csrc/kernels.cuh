@@ -34,6 +34,9 @@ cudaError_t launch_pd(bool off_boundary, int mz, const Geom &g, const View *view
 
 cudaError_t launch_scale(float *y, size_t n, float s, cudaStream_t st);
 
+// Raises (never lowers) a kernel's dynamic shared-memory limit on the current device.
+cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes);
+
 size_t proj_smem_bytes(int nv, int nx, int ny);
 int proj_group_width();
 int proj_max_lines();

@@ -37,11 +37,11 @@ def design_filter(nu: int, du: float, sdd: float, flat: bool, window: str = "ham
 class FDK:
     """Device FDK reconstructor for one geometry, window and crop."""
 
-    def __init__(self, geom: CTGeometry, window: str = "hamming", crop: float = 1.0, device=None):
+    def __init__(self, geom: CTGeometry, window: str = "hamming", crop: float = 1.0, device=None, plan=None):
         if window not in WINDOWS:
             raise ValueError("Invalid window selected.")
         self.geom = geom
-        self.plan = plan_for(geom, device)
+        self.plan = plan if plan is not None else plan_for(geom, device)
         L = _lib.load()
         h = C.c_void_p()
         import torch
@@ -71,9 +71,11 @@ class FDK:
         import torch
         sino = self.plan._check_tensor(sino, self.geom.sino_shape, "sino")
         if out is None:
-            out = torch.empty_like(sino)
+            out = torch.empty(sino.shape, dtype=torch.float32, device=sino.device)
         st = torch.cuda.current_stream(self.plan.device).cuda_stream
-        _lib.check(self._L.ctsim_fdk_filter(self._h, sino.data_ptr(), out.data_ptr(), st), "ctsim_fdk_filter")
+        from .projector import _DTYPES
+        _lib.check(self._L.ctsim_fdk_filter_ex(self._h, sino.data_ptr(), _DTYPES[sino.dtype], out.data_ptr(), st),
+                   "ctsim_fdk_filter")
         return out
 
     def __call__(self, sino, out=None):
@@ -83,7 +85,9 @@ class FDK:
         if out is None:
             out = torch.empty(self.geom.image_shape, dtype=torch.float32, device=self.plan.device)
         st = torch.cuda.current_stream(self.plan.device).cuda_stream
-        _lib.check(self._L.ctsim_fdk_run(self._h, sino.data_ptr(), out.data_ptr(), st), "ctsim_fdk_run")
+        from .projector import _DTYPES
+        _lib.check(self._L.ctsim_fdk_run_ex(self._h, sino.data_ptr(), _DTYPES[sino.dtype], out.data_ptr(), st),
+                   "ctsim_fdk_run")
         return out
 
 

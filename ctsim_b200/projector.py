@@ -132,9 +132,13 @@ class Plan:
 
     Holds the per-view tables and scratch on one GPU; ``project``/``backproject``
     take and return torch CUDA tensors and run on the current torch stream.
+    With ``stream`` (a torch.cuda.Stream) the plan is stream-ordered: its memory is
+    allocated and freed on that stream from the library pool, without a device-wide
+    synchronisation (ctsim_plan_create_async); all work on it must then be ordered
+    on that stream.
     """
 
-    def __init__(self, geom: CTGeometry, device=None):
+    def __init__(self, geom: CTGeometry, device=None, stream=None):
         torch = _torch()
         self.geom = geom
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else
@@ -145,9 +149,15 @@ class Plan:
         self._couch = np.ascontiguousarray(geom.couchZ, dtype=np.float32)
         self._map = np.ascontiguousarray(geom.map, dtype=np.bool_)
         h = C.c_void_p()
+        self.stream = stream
         with torch.cuda.device(self.device):
-            _lib.check(L.ctsim_plan_create(C.byref(g), self._betas.ctypes.data, self._couch.ctypes.data,
-                                           self._map.ctypes.data, C.byref(h)), "ctsim_plan_create")
+            if stream is None:
+                _lib.check(L.ctsim_plan_create(C.byref(g), self._betas.ctypes.data, self._couch.ctypes.data,
+                                               self._map.ctypes.data, C.byref(h)), "ctsim_plan_create")
+            else:
+                _lib.check(L.ctsim_plan_create_async(C.byref(g), self._betas.ctypes.data, self._couch.ctypes.data,
+                                                     self._map.ctypes.data, stream.cuda_stream, C.byref(h)),
+                           "ctsim_plan_create_async")
         self._h = h
         self._L = L
 

@@ -89,14 +89,14 @@ class PwlsSolver:
     """
 
     def __init__(self, y, w, geom: CTGeometry, beta: float, pfun: str = "huber", delta: float = 0.001,
-                 numos: int = 1, img0=None, method: str = "tf", storage=None):
+                 numos: int = 1, img0=None, method: str = "tf", storage=None, plan=None):
         torch = _torch()
         if pfun.lower() not in PENALTIES:
             raise ValueError("unknow penalty function")
         self.geom, self.beta, self.delta, self.M = geom, float(beta), float(delta), int(numos)
         self.kind = PENALTIES[pfun.lower()]
         self.method = method
-        self.plan = plan_for(geom, y.device)
+        self.plan = plan if plan is not None else plan_for(geom, y.device)
         self.dev = self.plan.device
         self.L = _lib.load()
         # the measured data (y, w: the largest arrays) may be stored in bfloat16 or float16;
@@ -140,29 +140,43 @@ class PwlsSolver:
         self.nx, self.ny, self.nz = geom.nx, geom.ny, geom.nz
         self.itn = 0
 
-    def step(self):
-        torch = _torch()
+    def subset_step(self, i: int):
+        """Sub-iteration i (0-based) of the current outer iteration, asynchronous on the
+        current stream (reconPwlsSeSqs.m:57-66)."""
         st = _stream(self.dev)
-        self.xold.copy_(self.x)
-        self.acc.zero_()
+        if i == 0:
+            self.xold.copy_(self.x)
+            self.acc.zero_()
         acc = self.acc.data_ptr()
         stride = 1 if self.M == 1 else self.M
-        for start, count, ys, ws in self.subsets:
-            ax = self.ax[:count]
-            wd = self.wd[:count]
-            self.plan.project(self.x, self.method, start, stride, count, out=ax)
-            _lib.check(self.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), self.sdt,
-                                                     self.w_scale, wd.data_ptr(), ax.numel(), acc, st),
-                       "ctsim_pwls_residual")
-            self.plan.backproject(wd, self.method, start, stride, count, scale=float(self.M), out=self.num)
-            _lib.check(self.L.ctsim_sqs_update(self.kind, self.beta, self.delta, self.nx, self.ny, self.nz,
-                                               self.x.data_ptr(), self.xn.data_ptr(), self.num.data_ptr(),
-                                               self.precom.data_ptr(), st), "ctsim_sqs_update")
-            self.x, self.xn = self.xn, self.x
+        start, count, ys, ws = self.subsets[i]
+        ax = self.ax[:count]
+        wd = self.wd[:count]
+        self.plan.project(self.x, self.method, start, stride, count, out=ax)
+        _lib.check(self.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), self.sdt,
+                                                 self.w_scale, wd.data_ptr(), ax.numel(), acc, st),
+                   "ctsim_pwls_residual")
+        self.plan.backproject(wd, self.method, start, stride, count, scale=float(self.M), out=self.num)
+        _lib.check(self.L.ctsim_sqs_update(self.kind, self.beta, self.delta, self.nx, self.ny, self.nz,
+                                           self.x.data_ptr(), self.xn.data_ptr(), self.num.data_ptr(),
+                                           self.precom.data_ptr(), st), "ctsim_sqs_update")
+        self.x, self.xn = self.xn, self.x
+
+    def end_iteration(self):
+        """Penalty value and squared change of the iteration into the FP64 accumulators
+        (asynchronous; ``step`` reads them)."""
+        st = _stream(self.dev)
+        acc = self.acc.data_ptr()
         _lib.check(self.L.ctsim_penalty(self.kind, 0, self.delta, self.nx, self.ny, self.nz, self.x.data_ptr(),
                                         None, acc + 16, st), "ctsim_penalty")
         _lib.check(self.L.ctsim_sqdiff(self.x.data_ptr(), self.xold.data_ptr(), self.x.numel(), acc + 8, st),
                    "ctsim_sqdiff")
+
+    def step(self):
+        """One outer iteration; returns (phi, rmsd) (synchronises)."""
+        for i in range(len(self.subsets)):
+            self.subset_step(i)
+        self.end_iteration()
         a = self.acc.cpu().numpy()
         self.itn += 1
         phi = a[0] / 2 + self.beta * a[2]

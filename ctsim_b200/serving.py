@@ -1,0 +1,385 @@
+"""Served reconstruction: a device-resident request loop with continuous batching.
+
+Requests are FDK (fbp/reconFDK.m) or OS-PWLS (statsrecon/pwls/reconPwlsSeSqs.m,
+initialised by reconFDK as the reference's scripts do) reconstructions, each with
+its own geometry.  The server
+
+* admits a request only when its HBM footprint fits the remaining budget and a
+  slot is free (``hbm_budget`` bytes, ``max_active`` slots), in arrival order;
+* gives each slot a persistent CUDA stream, and each admitted request its own
+  stream-ordered projector plan (tables and scratch from the library pool,
+  ctsim_plan_create_async), sinogram, weights and image, so requests never share
+  mutable device memory and a result does not depend on what else runs;
+* stores sinogram-sized data in float32, bfloat16 or float16 (FP32 arithmetic);
+* issues work per request in units -- one FDK pass, or one OS-PWLS outer
+  iteration (all subsets and the objective terms) -- with at most ``depth`` units
+  in flight per request, so kernels of different requests overlap on the device
+  and requests that arrive meanwhile are admitted as soon as slots and memory
+  free up.  From the second iteration on, an OS-PWLS iteration is one replay of
+  a CUDA graph captured from the first;
+* records per-request latency (completion - arrival) for p50/p99.
+
+OS-PWLS requests run a fixed number of iterations (the reference's stopping test
+on the RMS change needs a host read per iteration).
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass
+from typing import Callable, Optional
+
+import numpy as np
+
+from .geometry import CTGeometry, circular_betas
+
+
+@dataclass
+class ReconRequest:
+    kind: str                      # "fdk" or "pwls"
+    geom: CTGeometry
+    sino: "object"                 # log sinogram, host numpy or device tensor [views, nu, nv]
+    weights: "object" = None       # PWLS weights (reconPwlsSeSqs.m's w), same shape
+    window: str = "hamming"        # FDK window (reconFDK.m default)
+    beta: float = 1e3              # PWLS penalty weight
+    delta: float = 0.01            # Huber parameter
+    pfun: str = "huber"
+    iterations: int = 10
+    subsets: int = 12
+    storage: str = "float32"       # storage type of the sinogram and weights on the device
+    arrival: float = 0.0           # seconds, relative to the start of the run
+    rid: int = 0
+    # filled by the server
+    result: "object" = None
+    t_admit: float = float("nan")
+    t_done: float = float("nan")
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.arrival
+
+
+STORAGE = ("float32", "bfloat16", "float16")
+
+
+def _dtype(name):
+    import torch
+    return {"float32": torch.float32, "bfloat16": torch.bfloat16, "float16": torch.float16}[name]
+
+
+def hbm_footprint(req: ReconRequest) -> int:
+    """Upper bound of the device bytes a request holds while active: plan tables and
+    scratch, FDK buffers, the stored sinogram/weights and the FP32 solver state."""
+    g = req.geom
+    vox = g.nx * g.ny * g.nz
+    pix = g.nu * g.nv * g.noViews
+    s = 4 if req.storage == "float32" else 2
+    L = 64
+    while L < 2 * g.nu - 1:
+        L *= 2
+    plan = 4 * g.nx * g.ny * (g.nz + 1) + 4 * pix + 4 * g.nu * g.nv + g.nx * g.ny + 64 * g.noViews + 4096
+    fdk = 4 * pix + 4 * g.nu * g.nv + 12 * L + 4 * g.nu * g.noViews + 4096
+    image = 4 * vox
+    if req.kind == "fdk":
+        return plan + fdk + s * pix + image
+    # y, w in storage and their per-subset copies; while the solver is set up: the
+    # FP32 y and w, A(1) and the temporaries of w .* A(1); x, x_new, x_old, precom,
+    # num (FP32); the per-subset ax and wd
+    sub = 2 * 4 * g.nu * g.nv * math.ceil(g.noViews / req.subsets)
+    return plan + fdk + 4 * s * pix + 6 * 4 * pix + 5 * image + sub + 4096
+
+
+class _Active:
+    """Device state and work of one admitted request (runs on its slot's stream)."""
+
+    def __init__(self, req: ReconRequest, stream, device, graphs: bool = True):
+        import torch
+        from .fdk import FDK
+        from .projector import Plan
+        self.req = req
+        self.stream = stream
+        self.device = device
+        self.graphs = graphs
+        self.events = deque()
+        self.issued = 0
+        self.solver = None
+        self._graph = {}
+        dt = _dtype(req.storage)
+        with torch.cuda.device(device), torch.cuda.stream(stream):
+            self.plan = Plan(req.geom, device, stream=stream)
+            self.fdk = FDK(req.geom, req.window, 1.0, device, plan=self.plan)
+            sino = _to_device(req.sino, device)
+            if req.kind == "fdk":
+                self.sino = sino.to(dt).contiguous()
+                self.units = 1
+            else:
+                from .pwls import PwlsSolver
+                w = _to_device(req.weights, device)
+                x0 = self.fdk(sino.float().contiguous())  # reconFDK start image
+                self.solver = PwlsSolver(sino, w, req.geom, req.beta, req.pfun, req.delta, req.subsets, x0,
+                                         storage=dt, plan=self.plan)
+                self.fdk.close()
+                self.fdk = None
+                self.units = req.iterations
+
+    def in_flight(self) -> int:
+        while self.events and self.events[0].query():
+            self.events.popleft()
+        return len(self.events)
+
+    def _iteration(self):
+        s = self.solver
+        key = s.x.data_ptr()
+        if self.issued == 0 or not self.graphs:
+            for i in range(len(s.subsets)):
+                s.subset_step(i)
+            s.end_iteration()
+            return
+        g = self._graph.get(key)
+        if g is None:
+            import torch
+            # record (nothing runs during capture), then replay; the swaps of x and
+            # x_new done while recording leave the host-side pointers as after the run
+            g = torch.cuda.CUDAGraph()
+            g.capture_begin(capture_error_mode="thread_local")
+            for i in range(len(s.subsets)):
+                s.subset_step(i)
+            s.end_iteration()
+            g.capture_end()
+            self._graph[key] = g
+        else:
+            for _ in range(len(s.subsets)):  # the pointer swaps of the replayed iteration
+                s.x, s.xn = s.xn, s.x
+        g.replay()
+
+    def issue(self):
+        """Enqueue the next unit on this request's stream (asynchronous)."""
+        import torch
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            if self.req.kind == "fdk":
+                self.req.result = self.fdk(self.sino)
+            else:
+                self._iteration()
+                if self.issued + 1 == self.units:
+                    self.req.result = self.solver.x
+            self.issued += 1
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+            self.events.append(ev)
+
+    def complete(self) -> bool:
+        return self.issued == self.units and self.in_flight() == 0
+
+    def release(self):
+        """Free the request's device state (stream-ordered, no synchronisation)."""
+        import torch
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            self._graph.clear()
+            if self.fdk is not None:
+                self.fdk.close()
+            self.solver = None
+            self.sino = None
+            self.plan.close()
+
+
+def _to_device(a, device):
+    import torch
+    if isinstance(a, torch.Tensor):
+        return a.to(device, non_blocking=True)
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if torch.cuda.is_available():
+        t = t.pin_memory()
+    return t.to(device, non_blocking=True)
+
+
+class ReconServer:
+    """Admission by HBM budget into ``max_active`` slots (one stream each); every tick
+    issues one unit per active request with fewer than ``depth`` units in flight."""
+
+    def __init__(self, hbm_budget: int = 150 * 2 ** 30, max_active: int = 8, depth: int = 2, device=None,
+                 graphs: bool = True, activate: Optional[Callable] = None, clock: Optional[Callable] = None):
+        self.budget = int(hbm_budget)
+        self.max_active = int(max_active)
+        self.depth = int(depth)
+        self.graphs = graphs
+        self.pending = deque()
+        self.active = []
+        self.used = 0
+        self.peak_used = 0
+        self.done = []
+        self.t0 = 0.0
+        self._clock = clock or time.perf_counter
+        if activate is None:
+            import torch
+            self.device = torch.device("cuda", torch.cuda.current_device() if device is None else
+                                       (torch.device(device).index or 0))
+            self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.max_active)]
+            activate = lambda req, slot: _Active(req, self.streams[slot], self.device, self.graphs)
+        else:
+            self.streams = [None] * self.max_active
+        self._activate = activate
+        self._free_slots = list(range(self.max_active))[::-1]
+        self._slot_of = {}
+
+    def now(self) -> float:
+        return self._clock() - self.t0
+
+    def submit(self, req: ReconRequest):
+        if req.kind not in ("fdk", "pwls"):
+            raise ValueError(f"unknown request kind {req.kind!r}")
+        if req.storage not in STORAGE:
+            raise ValueError(f"unknown storage type {req.storage!r}")
+        if hbm_footprint(req) > self.budget:
+            raise ValueError(f"request {req.rid} needs more than the whole HBM budget")
+        self.pending.append(req)
+
+    def _admit(self):
+        while self.pending and self._free_slots:
+            req = self.pending[0]
+            if req.arrival > self.now():
+                break
+            need = hbm_footprint(req)
+            if self.used + need > self.budget:
+                break
+            self.pending.popleft()
+            req.t_admit = self.now()
+            slot = self._free_slots.pop()
+            a = self._activate(req, slot)
+            self._slot_of[id(a)] = slot
+            self.used += need
+            self.peak_used = max(self.peak_used, self.used)
+            self.active.append(a)
+
+    def _retire(self):
+        keep = []
+        for a in self.active:
+            if a.complete():
+                a.req.t_done = self.now()
+                a.release()
+                self.used -= hbm_footprint(a.req)
+                self._free_slots.append(self._slot_of.pop(id(a)))
+                self.done.append(a.req)
+            else:
+                keep.append(a)
+        self.active = keep
+
+    def tick(self):
+        self._admit()
+        for a in self.active:
+            if a.issued < a.units and a.in_flight() < self.depth:
+                a.issue()
+        self._retire()
+
+    def run(self, requests, time_limit: Optional[float] = None, idle_sleep: float = 2e-4):
+        """Serve requests (by arrival time) until all are done; returns the finished ones
+        in completion order."""
+        for r in sorted(requests, key=lambda r: r.arrival):
+            self.submit(r)
+        self.t0 = self._clock()
+        while self.pending or self.active:
+            self.tick()
+            if self.active or (self.pending and self.pending[0].arrival > self.now()):
+                time.sleep(idle_sleep)
+            if time_limit is not None and self.now() > time_limit:
+                break
+        return self.done
+
+
+def serve_sequential(requests, device=None):
+    """The plain single-instance path: one request at a time through the public FP32
+    API (reconFDK, reconFDK + reconPwlsSeSqs), host arrays in and out.  Sets result,
+    t_done (seconds from the start) and returns the requests."""
+    from .fdk import reconFDK
+    from .pwls import reconPwlsSeSqs
+    t0 = time.perf_counter()
+    for r in requests:
+        now = time.perf_counter() - t0
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        r.t_admit = time.perf_counter() - t0
+        y = np.asarray(r.sino, dtype=np.float32)
+        if r.kind == "fdk":
+            r.result = reconFDK(y, r.geom, r.window)
+        else:
+            import torch
+            x0 = reconFDK(y, r.geom, r.window)
+            x, _, _ = reconPwlsSeSqs(torch.from_numpy(y).cuda(), torch.from_numpy(np.asarray(r.weights)).cuda(),
+                                     r.geom, r.beta, r.pfun, r.iterations, r.delta, r.subsets,
+                                     torch.from_numpy(x0).cuda(), stopCrt=-1.0)
+            r.result = x.cpu().numpy()
+        r.t_done = time.perf_counter() - t0
+        # the plans and FDK objects the public API cached on the geometry
+        for f in r.geom.__dict__.pop("_fdk", {}).values():
+            f.close()
+        for p in r.geom.__dict__.pop("_plans", {}).values():
+            p.close()
+    return requests
+
+
+def latency_stats(done, t_total: float):
+    lat = np.array([r.latency for r in done])
+    if lat.size == 0:
+        return {"requests": 0}
+    return {"requests": int(lat.size), "req_per_s": float(lat.size / t_total),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_ms": float(lat.mean() * 1e3)}
+
+
+# ---------------------------------------------------------------------------
+# Seeded synthetic request stream
+# ---------------------------------------------------------------------------
+def random_geometry(rng, scale: float = 1.0) -> CTGeometry:
+    """Uneven instance geometry: volumes 128^2x64 .. 384^2x160 (voxel 0.5-1.0 mm), 180-720
+    views, detectors 256x64 .. 768x256 (0.8-1.6 mm); ~20% short scan, ~20% offset
+    detector.  ``scale`` shrinks every size."""
+    n = max(16, int(rng.integers(128, 385) * scale) // 16 * 16)
+    nz = max(8, int(rng.integers(64, 161) * scale) // 8 * 8)
+    vox = float(rng.uniform(0.5, 1.0))
+    nu = max(32, int(rng.integers(256, 769) * scale) // 16 * 16)
+    nv = max(16, int(rng.integers(64, 257) * scale) // 8 * 8)
+    # detector pitch covering the volume at magnification 1.5
+    du = max(0.8, min(1.6, 1.5 * n * vox * 1.5 / nu))
+    dv = max(0.8, min(1.6, 1.5 * nz * vox * 1.6 / nv))
+    views = max(8, int(rng.integers(180, 721) * scale) // 4 * 4)
+    short = bool(rng.random() < 0.2)
+    offset = (not short) and bool(rng.random() < 0.25)
+    if short:
+        fan = 2 * math.atan(nu * du / 2 / 1500.0)
+        betas = np.linspace(0.0, math.pi + fan, views)
+    else:
+        betas = circular_betas(views)
+    return CTGeometry((n, n, nz), (vox, vox, vox), (0, 0, 0), (nu, nv), (du, dv), (nu / 4.0 if offset else 0.0, 0),
+                      1000.0, 500.0, 1500.0, betas, shortScan=short)
+
+
+def make_requests(n: int, seed: int = 0, fdk_fraction: float = 0.7, storage: str = "bfloat16", scale: float = 1.0,
+                  iterations: int = 10, subsets: int = 12, rate: Optional[float] = None, i0: float = 1e5):
+    """``n`` requests (FDK with probability ``fdk_fraction``, else OS-PWLS) over
+    random_geometry, with Poisson arrivals at ``rate`` req/s (all at 0 if None).
+    The data: a random ellipsoid phantom projected with the SF projector, Poisson
+    counts at ``i0`` photons, y = log(i0 / max(counts, 10)) and w = counts
+    (computeWeightsPwls with r = v = 0 on counts)."""
+    import torch
+    from .phantom import ellipsoid_phantom, to_projector_units
+    from .projector import Plan
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    t, reqs = 0.0, []
+    for rid in range(n):
+        if rate is not None:
+            t += float(rng.exponential(1.0 / rate))
+        g = random_geometry(rng, scale)
+        r_xy = 0.4 * g.nx * g.reconSpacing[0]
+        x = to_projector_units(ellipsoid_phantom(g, 6, (0.015, 0.035), 0.02, r_xy, 0.6 * r_xy,
+                                                 0.3 * g.nz * g.reconSpacing[2], (2.0, 8.0),
+                                                 int(rng.integers(1 << 30))))
+        p = Plan(g)
+        line = p.project(torch.from_numpy(x).cuda(), "tf")
+        p.close()
+        counts = torch.poisson(i0 * torch.exp(-line), generator=gen)
+        y = torch.log(i0 / torch.clamp(counts, min=10.0)).cpu().numpy()
+        kind = "fdk" if rng.random() < fdk_fraction else "pwls"
+        reqs.append(ReconRequest(kind, g, y, counts.cpu().numpy() if kind == "pwls" else None, storage=storage,
+                                 arrival=t, rid=rid, iterations=iterations, subsets=subsets))
+    return reqs

@@ -144,6 +144,18 @@ ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *betas, cons
                                const bool *map, ctsim_plan **plan);
 ctsim_status ctsim_plan_destroy(ctsim_plan *plan);
 
+/* Stream-ordered plan (no reference counterpart; served reconstruction): its device
+ * memory comes from a library-owned pool of the current device, allocated, uploaded
+ * and -- at ctsim_plan_destroy, and ctsim_fdk_destroy for FDK objects built on it --
+ * freed on `stream` without a device-wide synchronisation.  All work on the plan must
+ * be ordered before its destruction on that stream, and the stream must outlive it. */
+ctsim_status ctsim_plan_create_async(const ctsim_geom *geom, const double *betas, const float *couchz,
+                                     const bool *map, void *stream, ctsim_plan **plan);
+
+/* Return unused memory of the current device's library pool to the driver, keeping
+ * at least keep_bytes. */
+ctsim_status ctsim_pool_trim(size_t keep_bytes);
+
 /* Bytes of device memory the plan holds (tables + scratch). */
 size_t ctsim_plan_device_bytes(const ctsim_plan *plan);
 
@@ -192,6 +204,10 @@ ctsim_status ctsim_fdk_filter(ctsim_fdk *fdk, const float *d_sino, float *d_filt
 
 /* Full FDK: filter, back,hpd, times dbeta, times 10 (reconFDK.m:84).  Image overwritten. */
 ctsim_status ctsim_fdk_run(ctsim_fdk *fdk, const float *d_sino, float *d_image, void *stream);
+
+/* The same with the sinogram stored as sino_dtype (ctsim_dtype; widened to FP32 on load). */
+ctsim_status ctsim_fdk_filter_ex(ctsim_fdk *fdk, const void *d_sino, int sino_dtype, float *d_filtered, void *stream);
+ctsim_status ctsim_fdk_run_ex(ctsim_fdk *fdk, const void *d_sino, int sino_dtype, float *d_image, void *stream);
 
 /* The dbeta the FDK scaling uses. */
 float ctsim_fdk_dbeta(const ctsim_fdk *fdk);
