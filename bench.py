@@ -396,7 +396,7 @@ def run_serving(args):
         return out
 
     def served(reqs, **kw):
-        srv = ReconServer(max_active=args.slots, **kw)
+        srv = ReconServer(max_active=args.slots, to_host=True, admit_workers=2, **kw)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         done = srv.run(reqs)

@@ -246,9 +246,10 @@ __device__ __forceinline__ float column_integral(const float *__restrict__ x, fl
 }
 
 // Dynamic shared-memory layout of proj_kernel.
+// groups: candidate-parallel thread groups, each with its own accumulator copy.
 struct ProjSmem {
-    int nq, nt, nlines;
-    __host__ __device__ size_t acc_bytes() const { return (size_t)kTU * nq * 16; }
+    int nq, nt, nlines, groups;
+    __host__ __device__ size_t acc_bytes() const { return (size_t)groups * kTU * nq * 16; }
     __host__ __device__ size_t bytes() const {
         return acc_bytes() + (size_t)nt * (6 + kTU) * 4 + (size_t)(2 * nlines + 1 + 32) * 4;
     }
@@ -262,19 +263,24 @@ struct ProjSmem {
 //     w_u(iu) * ampu * zinc * (X(iv+1) - X(iv))
 // -- the integral form of the distance-driven axial weights
 // (geom/cbct/cbct_proj.c:382-420) -- into float4 shared-memory accumulators that only
-// it touches: no atomics, deterministic.
-template <int METHOD>
+// it touches: no atomics, deterministic.  A block of NT threads holds NT / R groups
+// of R row threads (R a multiple of 32, passed by the launcher): group g takes candidates
+// g, g + groups, ... into its own accumulators, summed in group order at the store,
+// so short detectors (few rows) still keep 8 warps busy per block.
+template <int METHOD, int GROUPS>
 __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const View *__restrict__ views,
                                                                const float *__restrict__ xs,
                                                                const float *__restrict__ ampv,
                                                                const uint8_t *__restrict__ map,
                                                                void *__restrict__ proj, int out_dtype,
                                                                int view_begin, int view_stride, float margin) {
-    extern __shared__ float4 acc4[];  // [kTU][nq] row quads, then the arrays below
+    extern __shared__ float4 acc4[];  // [GROUPS][kTU][nq] row quads, then the arrays below
     const int NT = blockDim.x;
+    constexpr int groups = GROUPS;
+    const int R = NT / GROUPS;
     const int nq0 = (g.nv + 3) >> 2;
     const int nlines0 = max(g.nx, g.ny);
-    int *s_col = reinterpret_cast<int *>(acc4 + kTU * nq0);
+    int *s_col = reinterpret_cast<int *>(acc4 + groups * kTU * nq0);
     float *s_b0 = reinterpret_cast<float *>(s_col + NT);
     float *s_iz = s_b0 + NT;
     int *s_rlo = reinterpret_cast<int *>(s_iz + NT);
@@ -286,12 +292,15 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
     int *s_warp_tot = line_off + nlines0 + 1;
 
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int grp = GROUPS == 1 ? 0 : t / R;  // candidate group
+    const int gwarp = GROUPS == 1 ? warp : (t - grp * R) >> 5;  // warp within the group
     const int iu0 = blockIdx.x * kTU;
     const int k = blockIdx.y;
     const View v = views[view_begin + k * view_stride];
     const int nv = g.nv;
     const int nq = (nv + 3) >> 2;
-    for (int i = t; i < kTU * nq; i += NT) acc4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = t; i < groups * kTU * nq; i += NT) acc4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 *gacc = acc4 + grp * kTU * nq;
 
     // lines of constant iy when the rays run mostly along y, else lines of constant ix
     const bool rows = fabsf(v.cos_a) >= fabsf(v.sin_a);
@@ -359,7 +368,7 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
     const float fnz = (float)g.nz;
     const int nzm1 = g.nz - 1;
     const float fnzm1 = (float)nzm1;
-    const int rows_per_pass = 4 * NT;
+    const int rows_per_pass = 4 * R;
 
     for (int c0 = 0; c0 < ncand; c0 += NT) {
         // 3. exact footprints of this chunk of candidates
@@ -408,7 +417,7 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
         __syncthreads();
         // 4. row quads: R(iv) = X(iv+1) - X(iv) from the column's prefix pairs
         const int nslot = min(NT, ncand - c0);
-        for (int s = 0; s < nslot; s++) {
+        for (int s = grp; s < nslot; s += groups) {
             const int jj = s_j[s];
             if (jj < 0) continue;
             const int rlo = s_rlo[s], rhi = s_rhi[s];
@@ -416,7 +425,7 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
             const float *x = xs + (size_t)s_col[s] * (g.nz + 1);
             const int jlo = jj & 0xff, jhi = jj >> 8;
             for (int pbase = 0; pbase < nv; pbase += rows_per_pass) {
-                const int wrow = pbase + 128 * warp;  // first row of this warp's 128
+                const int wrow = pbase + 128 * gwarp;  // first row of this warp's 128
                 if (wrow > rhi || wrow + 127 < rlo) continue;  // warp-uniform
                 const int iv0 = wrow + 4 * lane;
                 const float f0 = small_int_to_float(iv0) - b0;
@@ -429,7 +438,7 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
                 if (lane == 31) X4 = column_integral(x, fminf(fmaxf((f0 + 4.0f) * izc, 0.0f), fnz), nzm1, fnzm1);
                 if (iv0 <= rhi && iv0 + 3 >= rlo && iv0 < nv) {
                     const float R0 = X1 - X0, R1 = X2 - X1, R2 = X3 - X2, R3 = X4 - X3;
-                    float4 *a = acc4 + (iv0 >> 2);
+                    float4 *a = gacc + (iv0 >> 2);
                     for (int j = jlo; j <= jhi; j++) {
                         const float w = s_wf[s * kTU + j];
                         float4 r = a[j * nq];
@@ -442,15 +451,19 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
         }
         __syncthreads();
     }
-    // 5. axial amplitude and store
+    // 5. sum of the groups (in group order), axial amplitude and store
     const size_t obase = (size_t)k * g.nu * nv;
     const float *accf = reinterpret_cast<const float *>(acc4);
+    const int gstride = kTU * 4 * nq;
     for (int j = 0; j < kTU; j++) {
         const int iu = iu0 + j;
         if (iu >= g.nu) break;
-        for (int iv = t; iv < nv; iv += NT)
-            store_from_float(proj, obase + (size_t)iu * nv + iv, accf[j * 4 * nq + iv] * ampv[(size_t)iu * nv + iv],
-                             out_dtype);
+        for (int iv = t; iv < nv; iv += NT) {
+            float a = accf[j * 4 * nq + iv];
+#pragma unroll
+            for (int q = 1; q < groups; q++) a += accf[q * gstride + j * 4 * nq + iv];
+            store_from_float(proj, obase + (size_t)iu * nv + iv, a * ampv[(size_t)iu * nv + iv], out_dtype);
+        }
     }
 }
 
@@ -628,9 +641,20 @@ cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, i
     return cudaGetLastError();
 }
 
-static int proj_threads(int nv) { return std::min(kProjMaxThreads, std::max(32, ((nv + 3) / 4 + 31) / 32 * 32)); }
+// Row threads R (one per 4 detector rows, whole warps, at most kProjMaxThreads) and
+// candidate groups: short detectors (R <= 64, up to 256 rows) fill the block with
+// groups; taller ones keep one group (measured: two groups of 3 warps at 384 rows are
+// slower than one).
+static int proj_row_threads(int nv) {
+    return std::min(kProjMaxThreads, std::max(32, ((nv + 3) / 4 + 31) / 32 * 32));
+}
+static int proj_groups(int nv) {
+    const int R = proj_row_threads(nv);
+    return R <= 64 ? kProjMaxThreads / R : 1;
+}
 size_t proj_smem_bytes(int nv, int nx, int ny) {
-    ProjSmem L{(nv + 3) / 4, proj_threads(nv), std::max(nx, ny)};
+    const int R = proj_row_threads(nv), G = proj_groups(nv);
+    ProjSmem L{(nv + 3) / 4, R * G, std::max(nx, ny), G};
     return L.bytes();
 }
 int proj_group_width() { return kTU; }
@@ -641,18 +665,21 @@ cudaError_t launch_proj(int method, const Geom &g, const View *views, const floa
                         cudaStream_t st) {
     const size_t sm = proj_smem_bytes(g.nv, g.nx, g.ny);
     dim3 grid((g.nu + kTU - 1) / kTU, vc);
-    // one thread per 4 detector rows (up to 256 threads per block, more rows loop)
-    const int nt = proj_threads(g.nv);
-    if (method == kDD) {
-        cudaError_t e = allow_dynamic_smem((const void *)proj_kernel<kDD>, sm);
-        if (e != cudaSuccess) return e;
-        proj_kernel<kDD><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin);
-    } else {
-        cudaError_t e = allow_dynamic_smem((const void *)proj_kernel<kTF>, sm);
-        if (e != cudaSuccess) return e;
-        proj_kernel<kTF><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin);
+    // one thread per 4 detector rows (up to 256 threads per group, more rows loop),
+    // groups of those threads share the candidates
+    const int G = proj_groups(g.nv);
+    const int nt = proj_row_threads(g.nv) * G;
+#define CTSIM_PROJ_CASE(M, GR)                                                                        \
+    if (method == M && G == GR) {                                                                     \
+        cudaError_t e = allow_dynamic_smem((const void *)proj_kernel<M, GR>, sm);                     \
+        if (e != cudaSuccess) return e;                                                               \
+        proj_kernel<M, GR><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin); \
+        return cudaGetLastError();                                                                    \
     }
-    return cudaGetLastError();
+    CTSIM_PROJ_CASE(kDD, 1) CTSIM_PROJ_CASE(kDD, 4) CTSIM_PROJ_CASE(kDD, 8)
+    CTSIM_PROJ_CASE(kTF, 1) CTSIM_PROJ_CASE(kTF, 4) CTSIM_PROJ_CASE(kTF, 8)
+#undef CTSIM_PROJ_CASE
+    return cudaErrorInvalidValue;
 }
 
 template <bool OFF, int MZ>

@@ -153,16 +153,22 @@ class _Active:
                 s.x, s.xn = s.xn, s.x
         g.replay()
 
-    def issue(self):
-        """Enqueue the next unit on this request's stream (asynchronous)."""
+    def issue(self, to_host: bool = False):
+        """Enqueue the next unit on this request's stream (asynchronous); after the last
+        one, with ``to_host``, the copy of the image into pinned host memory."""
         import torch
         with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
             if self.req.kind == "fdk":
-                self.req.result = self.fdk(self.sino)
+                img = self.fdk(self.sino)
             else:
                 self._iteration()
-                if self.issued + 1 == self.units:
-                    self.req.result = self.solver.x
+                img = self.solver.x
+            if self.issued + 1 == self.units:
+                if to_host:
+                    host = torch.empty(img.shape, dtype=img.dtype, pin_memory=True)
+                    host.copy_(img, non_blocking=True)
+                    img = host
+                self.req.result = img
             self.issued += 1
             ev = torch.cuda.Event()
             ev.record(self.stream)
@@ -198,13 +204,20 @@ class ReconServer:
     issues one unit per active request with fewer than ``depth`` units in flight."""
 
     def __init__(self, hbm_budget: int = 150 * 2 ** 30, max_active: int = 8, depth: int = 2, device=None,
-                 graphs: bool = True, activate: Optional[Callable] = None, clock: Optional[Callable] = None):
+                 graphs: bool = True, activate: Optional[Callable] = None, clock: Optional[Callable] = None,
+                 to_host: bool = False, admit_workers: int = 0):
         self.budget = int(hbm_budget)
         self.max_active = int(max_active)
         self.depth = int(depth)
         self.graphs = graphs
+        self.to_host = to_host
         self.pending = deque()
         self.active = []
+        self.starting = []   # (future, request, slot): requests set up by the admission workers
+        self._pool = None
+        if admit_workers > 0:
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(admit_workers, thread_name_prefix="ctsim-admit")
         self.used = 0
         self.peak_used = 0
         self.done = []
@@ -245,11 +258,30 @@ class ReconServer:
             self.pending.popleft()
             req.t_admit = self.now()
             slot = self._free_slots.pop()
-            a = self._activate(req, slot)
-            self._slot_of[id(a)] = slot
             self.used += need
             self.peak_used = max(self.peak_used, self.used)
-            self.active.append(a)
+            if self._pool is None:
+                self._start(self._activate(req, slot), slot)
+            else:
+                self.starting.append((self._pool.submit(self._activate_in_worker, req, slot), req, slot))
+
+    def _activate_in_worker(self, req, slot):
+        # the set-up work is ordered on the slot's stream, ahead of the units the main
+        # thread issues there later
+        return self._activate(req, slot)
+
+    def _start(self, a, slot):
+        self._slot_of[id(a)] = slot
+        self.active.append(a)
+
+    def _collect_started(self):
+        keep = []
+        for fut, req, slot in self.starting:
+            if fut.done():
+                self._start(fut.result(), slot)  # re-raises a set-up error here
+            else:
+                keep.append((fut, req, slot))
+        self.starting = keep
 
     def _retire(self):
         keep = []
@@ -266,10 +298,17 @@ class ReconServer:
 
     def tick(self):
         self._admit()
+        if self.starting:
+            self._collect_started()
         for a in self.active:
             if a.issued < a.units and a.in_flight() < self.depth:
-                a.issue()
+                a.issue(self.to_host)
         self._retire()
+
+    def close(self):
+        if self._pool is not None:
+            self._pool.shutdown(wait=True)
+            self._pool = None
 
     def run(self, requests, time_limit: Optional[float] = None, idle_sleep: float = 2e-4):
         """Serve requests (by arrival time) until all are done; returns the finished ones
@@ -277,12 +316,15 @@ class ReconServer:
         for r in sorted(requests, key=lambda r: r.arrival):
             self.submit(r)
         self.t0 = self._clock()
-        while self.pending or self.active:
-            self.tick()
-            if self.active or (self.pending and self.pending[0].arrival > self.now()):
-                time.sleep(idle_sleep)
-            if time_limit is not None and self.now() > time_limit:
-                break
+        try:
+            while self.pending or self.active or self.starting:
+                self.tick()
+                if self.active or self.starting or (self.pending and self.pending[0].arrival > self.now()):
+                    time.sleep(idle_sleep)
+                if time_limit is not None and self.now() > time_limit:
+                    break
+        finally:
+            self.close()
         return self.done
 
 

@@ -28,7 +28,7 @@ class _FakeActive:
         self.pending = [t - 1 for t in self.pending if t > 1]
         return len(self.pending)
 
-    def issue(self):
+    def issue(self, to_host=False):
         self.issued += 1
         self.pending.append(self.lag)
         self.log.append(("issue", self.req.rid, self.slot))
@@ -137,7 +137,8 @@ def _result(r):
 @pytest.mark.gpu
 def test_served_results_do_not_depend_on_the_mix():
     """Bit-identical images whether a request is served alone, in a mix of seven on four
-    slots, without CUDA graphs, or through the plain single-instance FP32 API."""
+    slots, without CUDA graphs, with set-up on admission threads and delivery to host
+    memory, or through the plain single-instance FP32 API."""
     from ctsim_b200.serving import serve_sequential
     reqs = _device_requests()
     mixed = copy.deepcopy(reqs)
@@ -145,6 +146,8 @@ def test_served_results_do_not_depend_on_the_mix():
     assert len(done) == len(reqs)
     eager = copy.deepcopy(reqs)
     ReconServer(max_active=4, graphs=False).run(eager)
+    threaded = copy.deepcopy(reqs)
+    ReconServer(max_active=3, to_host=True, admit_workers=2).run(threaded)
     plain = serve_sequential(copy.deepcopy(reqs))
     for i, r in enumerate(reqs):
         alone = copy.deepcopy(r)
@@ -153,6 +156,7 @@ def test_served_results_do_not_depend_on_the_mix():
         assert a.shape == r.geom.image_shape and np.isfinite(a).all() and np.abs(a).max() > 0
         assert np.array_equal(_result(mixed[i]), a), (i, r.kind)
         assert np.array_equal(_result(eager[i]), a), (i, r.kind)
+        assert not threaded[i].result.is_cuda and np.array_equal(_result(threaded[i]), a), (i, r.kind)
         assert np.array_equal(_result(plain[i]), a), (i, r.kind)
 
 
