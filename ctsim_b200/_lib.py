@@ -26,7 +26,8 @@ EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd
             "ctsim_fdk_design_filter", "ctsim_pwls_weights", "ctsim_pwls_residual", "ctsim_sqdiff",
             "ctsim_penalty", "ctsim_sqs_update", "ctsim_plan_project_ex", "ctsim_plan_backproject_ex",
             "ctsim_pwls_residual_ex", "ctsim_fdk_filter_ex", "ctsim_fdk_run_ex",
-            "ctsim_plan_create_async", "ctsim_pool_trim"]
+            "ctsim_plan_create_async", "ctsim_pool_trim", "ctsim_nesterov_update",
+            "ctsim_simulate_counts", "ctsim_log_attenuation"]
 
 
 class CtsimGeom(C.Structure):
@@ -78,6 +79,13 @@ def load():
     L.ctsim_plan_create.restype = _i
     L.ctsim_plan_create_async.argtypes = [C.POINTER(CtsimGeom), _p, _p, _p, _p, C.POINTER(_p)]
     L.ctsim_plan_create_async.restype = _i
+    L.ctsim_nesterov_update.argtypes = [_i, _f, _f, _i, _i, _i, _p, _p, _p, _p, _p, C.c_double, C.c_double, _p,
+                                        _p, _p]
+    L.ctsim_nesterov_update.restype = _i
+    L.ctsim_simulate_counts.argtypes = [_p, C.c_size_t, _f, _f, C.c_uint64, _i, _p, _p, _p]
+    L.ctsim_simulate_counts.restype = _i
+    L.ctsim_log_attenuation.argtypes = [_p, C.c_size_t, _f, _p, C.c_size_t, _p, _p]
+    L.ctsim_log_attenuation.restype = _i
     L.ctsim_pool_trim.argtypes = [C.c_size_t]
     L.ctsim_pool_trim.restype = _i
     L.ctsim_plan_destroy.argtypes = [_p]

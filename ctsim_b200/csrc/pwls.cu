@@ -6,6 +6,7 @@
 //   sqs_update       x <- max(0, x - (At_s(w d) + beta S(x)) / (precom + beta T(x)))
 //                    with S, T gathered inline; NaN/Inf -> 0  reconPwlsSeSqs.m:59-66
 //   sqdiff           sum((a - b)^2) for the iteration's rmsd      reconPwlsSeSqs.m:81
+//   nesterov_update  the Nesterov step of reconPwlsSeNesterovSqs.m:65-87
 // Image layout [nz][ny][nx] (MATLAB x(i,j,k) = img[k][j][i]).  Reductions in FP64.
 #include <cmath>
 
@@ -176,6 +177,39 @@ __global__ void sqs_update_kernel(const float *__restrict__ x, float *__restrict
     xn[c] = v;
 }
 
+// One subset step of statsrecon/pwls/reconPwlsSeNesterovSqs.m:65-87 at a voxel:
+//   du = (num + beta S(z)) / (precom + beta T(x))        (FP64, like sqs_update)
+//   x' = z - du;  s' = s - t du;  z' = (1 - 1/t') x' + (1/t') s'
+// with z' formed from the unclamped x' and s' (as the MATLAB code orders it), then
+// x', s', z' < 0, NaN, Inf -> 0.  s is updated in place (only its own voxel is read).
+__global__ void nesterov_update_kernel(const float *__restrict__ z, const float *__restrict__ x,
+                                       float *__restrict__ s, const float *__restrict__ num,
+                                       const float *__restrict__ precom, float *__restrict__ xn,
+                                       float *__restrict__ zn, int kind, float beta, float delta, float axy,
+                                       float az, float cquad, double t, double tn, int nx, int ny, int nz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const int k = blockIdx.z;
+    if (i >= nx) return;
+    const size_t c = (size_t)k * nx * ny + (size_t)j * nx + i;
+    float Sz = 0.f, Tx = 0.f;
+    if (beta != 0.0f) {
+        float unused;
+        grad_curv(gather_diffs(z, i, j, k, nx, ny, nz), kind, delta, axy, az, cquad, &Sz, &unused);
+        grad_curv(gather_diffs(x, i, j, k, nx, ny, nz), kind, delta, axy, az, cquad, &unused, &Tx);
+    }
+    const double grad = (double)num[c] + (double)beta * (double)Sz;
+    const double denom = (double)precom[c] + (double)beta * (double)Tx;
+    const double du = grad / denom;
+    const float xv = (float)((double)z[c] - du);
+    const float sv = (float)((double)s[c] - t * du);
+    const float zv = (float)((1.0 - 1.0 / tn) * (double)xv + (1.0 / tn) * (double)sv);
+    auto clean = [](float v) { return (!(v >= 0.0f) || isinf(v)) ? 0.0f : v; };
+    xn[c] = clean(xv);
+    s[c] = clean(sv);
+    zn[c] = clean(zv);
+}
+
 int grid_for(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
 }  // namespace
@@ -243,6 +277,31 @@ extern "C" ctsim_status ctsim_sqs_update(int kind, float beta, float delta, int 
     dim3 grid((nx + 127) / 128, ny, nz);
     sqs_update_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(d_x, d_xnew, d_num, d_precom, kind, beta, delta, axy,
                                                              az, cq, nx, ny, nz);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CTSIM_OK : ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
+}
+
+extern "C" ctsim_status ctsim_nesterov_update(int kind, float beta, float delta, int nx, int ny, int nz,
+                                              const float *d_z, const float *d_x, float *d_s, const float *d_num,
+                                              const float *d_precom, double t, double t_next, float *d_xnew,
+                                              float *d_znew, void *stream) {
+    if (!d_z || !d_x || !d_s || !d_num || !d_precom || !d_xnew || !d_znew)
+        return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    // x_new and z_new must not alias the arrays whose neighbours are read (z, x) or s
+    const void *in[3] = {d_z, d_x, d_s};
+    for (const void *q : in)
+        if (q == d_xnew || q == d_znew)
+            return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "x_new and z_new must differ from z, x and s");
+    if (d_xnew == d_znew) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "x_new and z_new must differ");
+    if (kind < 0 || kind > 1) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "unknown penalty");
+    if (nx < 1 || ny < 1 || nz < 1) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "sizes must be positive");
+    if (!(t >= 1.0) || !(t_next >= 1.0)) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "momentum t must be >= 1");
+    float axy, az, cq;
+    penalty_consts(&axy, &az, &cq);
+    dim3 grid((nx + 127) / 128, ny, nz);
+    nesterov_update_kernel<<<grid, 128, 0, (cudaStream_t)stream>>>(d_z, d_x, d_s, d_num, d_precom, d_xnew, d_znew,
+                                                                  kind, beta, delta, axy, az, cq, t, t_next, nx, ny,
+                                                                  nz);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? CTSIM_OK : ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
 }

@@ -8,6 +8,8 @@ Mirrors the reference's MATLAB entry points with torch CUDA tensors:
 * ``loadPenaltyOperator(pfun, delta)``          penalty/loadPenaltyOperator.m ('huber', 'quad')
 * ``reconPwlsSeSqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0)``
                                                 statsrecon/pwls/reconPwlsSeSqs.m
+* ``reconPwlsSeNesterovSqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0, imgOpt)``
+                                                statsrecon/pwls/reconPwlsSeNesterovSqs.m
 
 The projectors are the separable-footprint pair the reference's PWLS loads
 (geom/shell/loadPojectors.m:8-11); all per-voxel and per-ray arithmetic runs in
@@ -195,4 +197,97 @@ def reconPwlsSeSqs(y, w, geom: CTGeometry, beta: float, pfun: str = "huber", itn
         phis[itn - 1], rmsds[itn - 1] = phi, rmsd
         if itn > 5 and rmsd < stopCrt:  # reconPwlsSeSqs.m:106
             break
+    return solver.x, phis, rmsds
+
+
+class PwlsNesterovSolver(PwlsSolver):
+    """OS-SQS with Nesterov's momentum (statsrecon/pwls/reconPwlsSeNesterovSqs.m:41-136):
+    the subsets project the extrapolated image z, the step is taken from z, and the
+    momentum state s and scalar t follow Kim, Ramani and Fessler (2013) as the reference
+    writes them.  ``img_opt`` (the converged image) switches the rmsd to the distance of the
+    middle slice from it (reconPwlsSeNesterovSqs.m:102-113)."""
+
+    def __init__(self, *args, img_opt=None, **kw):
+        super().__init__(*args, **kw)
+        torch = _torch()
+        self.z = self.x.clone()
+        self.s = self.x.clone()
+        self.zn = torch.empty_like(self.x)
+        self.t = 1.0
+        self.img_opt = None
+        if img_opt is not None:
+            if self.nz % 2:
+                raise ValueError("the rmsd against imgOpt compares slice end/2, which needs an even nz")
+            k = self.nz // 2 - 1  # x(:,:,end/2), 0-based
+            self._slice = k
+            self.img_opt = img_opt.to(self.dev, torch.float32)[k].contiguous()
+
+    def subset_step(self, i: int):
+        st = _stream(self.dev)
+        if i == 0:
+            self.xold.copy_(self.x)
+            self.acc.zero_()
+        acc = self.acc.data_ptr()
+        stride = 1 if self.M == 1 else self.M
+        start, count, ys, ws = self.subsets[i]
+        ax = self.ax[:count]
+        wd = self.wd[:count]
+        self.plan.project(self.z, self.method, start, stride, count, out=ax)        # Aos(z, isub)
+        _lib.check(self.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), self.sdt,
+                                                 self.w_scale, wd.data_ptr(), ax.numel(), acc, st),
+                   "ctsim_pwls_residual")
+        self.plan.backproject(wd, self.method, start, stride, count, scale=float(self.M), out=self.num)
+        t_next = (1.0 + math.sqrt(1.0 + 4.0 * self.t * self.t)) / 2.0
+        _lib.check(self.L.ctsim_nesterov_update(self.kind, self.beta, self.delta, self.nx, self.ny, self.nz,
+                                                self.z.data_ptr(), self.x.data_ptr(), self.s.data_ptr(),
+                                                self.num.data_ptr(), self.precom.data_ptr(), self.t, t_next,
+                                                self.xn.data_ptr(), self.zn.data_ptr(), st),
+                   "ctsim_nesterov_update")
+        self.x, self.xn = self.xn, self.x
+        self.z, self.zn = self.zn, self.z
+        self.t = t_next
+
+    def end_iteration(self):
+        if self.img_opt is None:
+            return super().end_iteration()
+        st = _stream(self.dev)
+        acc = self.acc.data_ptr()
+        _lib.check(self.L.ctsim_penalty(self.kind, 0, self.delta, self.nx, self.ny, self.nz, self.x.data_ptr(),
+                                        None, acc + 16, st), "ctsim_penalty")
+        xs = self.x[self._slice]
+        _lib.check(self.L.ctsim_sqdiff(xs.data_ptr(), self.img_opt.data_ptr(), xs.numel(), acc + 8, st),
+                   "ctsim_sqdiff")
+
+    def step(self):
+        for i in range(len(self.subsets)):
+            self.subset_step(i)
+        self.end_iteration()
+        a = self.acc.cpu().numpy()
+        self.itn += 1
+        phi = a[0] / 2 + self.beta * a[2]
+        n = self.x.numel() if self.img_opt is None else self.img_opt.numel()
+        return phi, math.sqrt(a[1] / n)
+
+    def restart(self):
+        """t = 1, z = x, s = x (reconPwlsSeNesterovSqs.m:132-136)."""
+        self.t = 1.0
+        self.z.copy_(self.x)
+        self.s.copy_(self.x)
+
+
+def reconPwlsSeNesterovSqs(y, w, geom: CTGeometry, beta: float, pfun: str = "huber", itnlim: int = 10,
+                           delta: float = 0.001, numos: int = 1, img0=None, imgOpt=None, storage=None):
+    """statsrecon/pwls/reconPwlsSeNesterovSqs.m: returns (x, phis, rmsds).  Stops after
+    iteration 5 once rmsd < 1e-10; restarts the momentum every round(2 itnlim) iterations."""
+    solver = PwlsNesterovSolver(y, w, geom, beta, pfun, delta, numos, img0, storage=storage, img_opt=imgOpt)
+    stop_crt = 1e-10
+    nrestart = int(round(itnlim * 2))
+    phis, rmsds = np.zeros(itnlim), np.zeros(itnlim)
+    for itn in range(1, itnlim + 1):
+        phi, rmsd = solver.step()
+        phis[itn - 1], rmsds[itn - 1] = phi, rmsd
+        if itn > 5 and rmsd < stop_crt:
+            break
+        if itn % nrestart == 0:
+            solver.restart()
     return solver.x, phis, rmsds

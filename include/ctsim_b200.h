@@ -32,6 +32,7 @@
 
 #include <stdbool.h>
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -252,6 +253,36 @@ ctsim_status ctsim_penalty(int kind, int mode, float delta, int nx, int ny, int 
  * formed in FP64.  d_x and d_xnew must differ. */
 ctsim_status ctsim_sqs_update(int kind, float beta, float delta, int nx, int ny, int nz, const float *d_x,
                               float *d_xnew, const float *d_num, const float *d_precom, void *stream);
+
+/* One Nesterov subset step of statsrecon/pwls/reconPwlsSeNesterovSqs.m:65-87:
+ * du = (num + beta S(z)) / (precom + beta T(x)) (FP64); x_new = z - du; s = s - t du (in
+ * place); z_new = (1 - 1/t_next) x_new + (1/t_next) s, from the unclamped x_new and s; then
+ * negatives, NaN and Inf of x_new, s and z_new set to 0.  t is the momentum of this step,
+ * t_next = (1 + sqrt(1 + 4 t^2)) / 2 the one after it.  d_xnew and d_znew must differ from
+ * d_z, d_x, d_s and from each other. */
+ctsim_status ctsim_nesterov_update(int kind, float beta, float delta, int nx, int ny, int nz, const float *d_z,
+                                   const float *d_x, float *d_s, const float *d_num, const float *d_precom,
+                                   double t, double t_next, float *d_xnew, float *d_znew, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Sinogram pre-processing (the data step in front of the projectors).
+ * ------------------------------------------------------------------------- */
+
+/* sinogram/sim/simulateSimplePoissonData.m:161-190, monochromatic spectrum:
+ * counts = Poisson(photons * exp(-line)) + sqrt(electronic_noise) * N(0, 1) per element, or,
+ * with add_noise = 0, round(photons * exp(-line)).  photons = DQE * photonsTotal.  The draws
+ * come from a Philox4x32-10 stream per element keyed by seed, so they depend only on
+ * (seed, element index).  d_fallbacks (may be NULL) counts elements whose bounded
+ * rejection loop gave up and returned round(lambda) (not expected in practice). */
+ctsim_status ctsim_simulate_counts(const float *d_line, size_t n, float photons, float electronic_noise,
+                                   uint64_t seed, int add_noise, float *d_counts, unsigned int *d_fallbacks,
+                                   void *stream);
+
+/* sinogram/log/computeSimplePoissonSinogramAttunation.m:14-54:
+ * sino = -log(max(counts, 10) / source_intensity [./ flat]), d_flat (may be NULL) holding the
+ * bowtie flat-field ratio of one view (nuv = nu * nv elements, sinogram layout). */
+ctsim_status ctsim_log_attenuation(const float *d_counts, size_t n, float source_intensity, const float *d_flat,
+                                   size_t nuv, float *d_sino, void *stream);
 
 /* Matched distance-driven backprojection (same result as CTSIM_BACK_DD, within float
  * rounding) that allocates no device memory.  No counterpart in the reference: its MEX

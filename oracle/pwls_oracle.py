@@ -5,6 +5,7 @@ the reference's MATLAB in single precision, with the projectors of the C oracle.
     huber_penalty          penalty/huberPenalty.m:101-217 (3-D), :222-238
     quad_penalty           penalty/quadPenalty.m:296-352 (3-D), with dQuad(d) = d
     recon_pwls_se_sqs      statsrecon/pwls/reconPwlsSeSqs.m:36-110
+    recon_pwls_nesterov_sqs statsrecon/pwls/reconPwlsSeNesterovSqs.m:35-136
 
 Arrays follow the package layout [nz, ny, nx]; the MATLAB code indexes x(i,j,k)
 with i along x, so the slicing below is written on the transposed view.
@@ -187,4 +188,74 @@ def _recon_pwls_fp64(y, w, geom, beta, pfun, itnlim, delta, M, img0, history):
             history.append(x.copy())
         if itn > 5 and rmsds[-1] < 1e-5:
             break
+    return x, np.array(phis), np.array(rmsds)
+
+
+def _matlab_round(v):
+    return int(np.floor(abs(v) + 0.5)) * (1 if v >= 0 else -1)
+
+
+def recon_pwls_nesterov_sqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0, img_opt=None):
+    """reconPwlsSeNesterovSqs.m in single precision (MATLAB: a double scalar times a single
+    array is computed in single); returns (x, phis, rmsds)."""
+    if pfun == "huber":
+        R = lambda x: huber_penalty(x, 0, delta)
+        S = lambda x: huber_penalty(x, 1, delta)
+        T = lambda x: huber_penalty(x, 2, delta)
+    else:
+        R = lambda x: quad_penalty(x, 0)
+        S = lambda x: quad_penalty(x, 1)
+        T = lambda x: quad_penalty(x, 2)
+    M = numos
+    stop_crt = 1e-10
+    nrestart = _matlab_round(itnlim * 2)
+    x = np.asarray(img0, dtype=F32).copy()
+    a = oracle_cbct("proj,tf", geom, np.ones_like(x))
+    precom = oracle_cbct("back,tf", geom, (w * a).astype(F32))
+    t = 1.0
+    z = x.copy()
+    s = x.copy()
+    phis, rmsds = [], []
+
+    def clean(v):
+        v = v.copy()
+        v[v < 0] = 0
+        v[np.isnan(v)] = 0
+        v[np.isinf(v)] = 0
+        return v
+
+    for itn in range(1, itnlim + 1):
+        xold = x.copy()
+        phi = 0.0
+        for isub in range(1, M + 1):
+            g = geom.subset(M, isub)
+            start = isub % M if M > 1 else 0
+            ys = y[start::M] if M > 1 else y
+            ws = w[start::M] if M > 1 else w
+            d = (oracle_cbct("proj,tf", g, z) - ys).astype(F32)
+            grad = oracle_cbct("back,tf", g, (ws * d).astype(F32))
+            if M != 1:
+                grad = (F32(M) * grad).astype(F32)
+            grad = (grad + F32(beta) * S(z)).astype(F32)
+            du = (grad / (precom + F32(beta) * T(x)).astype(F32)).astype(F32)
+            x = (z - du).astype(F32)
+            s = (s - F32(t) * du).astype(F32)
+            t = (1 + np.sqrt(1 + 4 * t * t)) / 2
+            z = (F32(1 - 1 / t) * x + F32(1 / t) * s).astype(F32)
+            x, s, z = clean(x), clean(s), clean(z)
+            phi += float((ws.astype(np.float64) * d.astype(np.float64) ** 2).sum()) / 2
+        phi += beta * R(x)
+        if img_opt is None:
+            rmsd = float(np.sqrt(np.mean((x.astype(np.float64) - xold) ** 2)))
+        else:
+            k = x.shape[0] // 2 - 1  # x(:,:,end/2) in the [nz, ny, nx] layout
+            rmsd = float(np.sqrt(np.mean((x[k].astype(np.float64) - np.asarray(img_opt, np.float64)[k]) ** 2)))
+        phis.append(phi)
+        rmsds.append(rmsd)
+        if itn > 5 and rmsd < stop_crt:
+            break
+        if itn % nrestart == 0:
+            t = 1.0
+            z = x.copy()
+            s = x.copy()
     return x, np.array(phis), np.array(rmsds)

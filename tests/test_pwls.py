@@ -82,3 +82,43 @@ def test_device_os_sqs_matches_oracle(pfun):
     assert np.allclose(phis, phio, rtol=1e-4)
     assert np.allclose(rmsds, rmsdo, rtol=1e-3)
     assert phis[-1] < phis[0]  # the cost decreases
+
+
+def test_oracle_nesterov_first_step_is_the_sqs_step():
+    """With t = 1 the first Nesterov step from z = x is the plain SQS step, so one
+    iteration with one subset gives the reconPwlsSeSqs image exactly."""
+    g, y, w, counts, x0 = pwls_case()
+    xs, ps, _ = pwls_oracle.recon_pwls_se_sqs(y, w, g, 2.0, "huber", 1, 0.01, 1, x0)
+    xn, pn, _ = pwls_oracle.recon_pwls_nesterov_sqs(y, w, g, 2.0, "huber", 1, 0.01, 1, x0)
+    assert np.array_equal(xs, xn) and np.allclose(ps, pn, rtol=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pfun", ["huber", "quad"])
+def test_device_nesterov_sqs_matches_oracle(pfun):
+    import torch
+    from ctsim_b200.pwls import reconPwlsSeNesterovSqs
+    g, y, w, counts, x0 = pwls_case()
+    beta, delta, M, its = 2.0, 0.01, 3, 4
+    x, phis, rmsds = reconPwlsSeNesterovSqs(torch.from_numpy(y).cuda(), torch.from_numpy(w).cuda(), g, beta, pfun,
+                                            its, delta, M, torch.from_numpy(x0).cuda())
+    xo, phio, rmsdo = pwls_oracle.recon_pwls_nesterov_sqs(y, w, g, beta, pfun, its, delta, M, x0)
+    got = x.cpu().numpy()
+    err = np.linalg.norm(got - xo) / np.linalg.norm(xo)
+    assert err <= 1e-4, err
+    assert np.allclose(phis, phio, rtol=1e-4)
+    assert np.allclose(rmsds, rmsdo, rtol=1e-3)
+
+
+@pytest.mark.gpu
+def test_device_nesterov_rmsd_against_converged_image():
+    """imgOpt switches the rmsd to the middle slice's distance from the converged image."""
+    import torch
+    from ctsim_b200.pwls import reconPwlsSeNesterovSqs
+    g, y, w, counts, x0 = pwls_case()
+    x_opt, _, _ = pwls_oracle.recon_pwls_se_sqs(y, w, g, 2.0, "huber", 8, 0.01, 3, x0)
+    x, phis, rmsds = reconPwlsSeNesterovSqs(torch.from_numpy(y).cuda(), torch.from_numpy(w).cuda(), g, 2.0, "huber",
+                                            4, 0.01, 3, torch.from_numpy(x0).cuda(), torch.from_numpy(x_opt).cuda())
+    xo, _, rmsdo = pwls_oracle.recon_pwls_nesterov_sqs(y, w, g, 2.0, "huber", 4, 0.01, 3, x0, img_opt=x_opt)
+    assert np.allclose(rmsds, rmsdo, rtol=1e-3)
+    assert rmsds[-1] < rmsds[0]  # approaching the converged image
