@@ -204,6 +204,7 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
     g.dz_dv = G.dz / G.dv;
     g.wz_pd = centre(G.nz, G.offset_z);
     g.roff = G.offset_u * G.du * G.sad / G.sdd;
+    g.roff_var = G.offset_u * G.sad / G.sdd;
     g.u_lo = float_at_or_above(1e-6);
     g.u_hi = float_at_or_below((double)G.nu - 1.0 - 1e-6);
     g.v_lo = float_at_or_above(1e-6);
@@ -390,15 +391,17 @@ extern "C" ctsim_status ctsim_plan_backproject_ex(ctsim_plan *p, int method, con
         break;
     }
     case CTSIM_BACK_PD:
-    case CTSIM_BACK_HPD: {
+    case CTSIM_BACK_HPD:
+    case CTSIM_BACK_VAR: {
         const float *src = static_cast<const float *>(d_proj);
         if (proj_dtype != CTSIM_F32) {  // FP32 copy of the views in scratch
             e = launch_prescale(d_proj, proj_dtype, nullptr, p->d_ps, nuv, nuv * view_count, st);
             if (e != cudaSuccess) return cuda_fail(e, "conversion kernel");
             src = p->d_ps;
         }
-        e = launch_pd(method == CTSIM_BACK_PD, p->pd_mz, p->g, p->d_views, src, p->d_map, d_image, image_dtype,
-                      view_begin, view_stride, view_count, scale, st);
+        const int mode = method == CTSIM_BACK_PD ? kPdOff : method == CTSIM_BACK_HPD ? kPdClamp : kPdVar;
+        e = launch_pd(mode, p->pd_mz, p->g, p->d_views, src, p->d_map, d_image, image_dtype, view_begin, view_stride,
+                      view_count, scale, st);
         break;
     }
     default:
@@ -528,6 +531,7 @@ extern "C" bool ctsim_cbct_geom(const char *type, CTSIM_GEOM_PARAMS, const float
     else if (!std::strcmp(type, "back,tf")) method = CTSIM_BACK_TF;
     else if (!std::strcmp(type, "back,pd")) method = CTSIM_BACK_PD;
     else if (!std::strcmp(type, "back,hpd")) method = CTSIM_BACK_HPD;
+    else if (!std::strcmp(type, "back,var")) method = CTSIM_BACK_VAR;
     if (method < 0) {
         fail(CTSIM_ERR_ARGUMENT, "Error: unknown geom type.");
         return false;

@@ -45,6 +45,7 @@ struct Geom {
     float dz_dv;                  // dz / dv (first factor of zinc, :361)
     float wz_pd;                  // -(nz-1)/2 + offset_z, geom/cbct/cbct_back.c:47
     float roff;                   // curved FDK: offset_u*du*sad/sdd, cbct_back.c:80
+    float roff_var;               // curved back,var: offset_u*sad/sdd, cbct_back_var.c:70
     // FDK boundary tests "u < 1E-6 || u > nu - 1 - 1E-6" are done in double in the
     // reference (cbct_back.c:90, :105-111); these are the exact float thresholds:
     // u < 1e-6 (double) <=> u < u_lo ; u > nu-1-1e-6 (double) <=> u > u_hi (floats).

@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
 // by lane j for view k0+j and broadcast; every voxel accumulates the views in the
 // reference's order with its exact float operations.
 // ---------------------------------------------------------------------------
-template <bool OFF, int MZ>
+template <int MODE, int MZ>
 __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict__ views,
                                                  const float *__restrict__ proj, const uint8_t *__restrict__ map,
                                                  void *__restrict__ image, int out_dtype, int view_begin,
@@ -499,6 +499,7 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
         }
         if (on) {
             for (int k0 = 0; k0 < view_count; k0 += 32) {
+                constexpr bool OFF = MODE != kPdClamp, VAR = MODE == kPdVar;
                 float u = -1.0f, w2 = 0.0f, w2s = 0.0f, couch = 0.0f;
                 const int kl = k0 + lane;
                 if (kl < view_count) {
@@ -510,14 +511,14 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
                         w2 = fdiv(g.sdd, den);
                         w2s = fmul(w2, w2);
                         u = fsub(fdiv(fmul(xr, w2), g.du), g.wu);
-                    } else {           // cbct_back.c:78-88
-                        const float xo = fsub(xr, g.roff);
+                    } else {           // cbct_back.c:78-88, cbct_back_var.c:68-77
+                        const float xo = fsub(xr, VAR ? g.roff_var : g.roff);
                         const double at = atan((double)fdiv(xo, den));
                         u = (float)__dsub_rn(__ddiv_rn(__dmul_rn(at, (double)g.sdd), (double)g.du), (double)g.wu);
                         w2s = fdiv(fmul(g.sdd, g.sdd), fadd(fmul(den, den), fmul(xo, xo)));
                         w2 = fdiv(g.sdd, den);
                     }
-                    couch = v.couch_pd;
+                    couch = VAR ? v.wz : v.couch_pd;  // back,var: the couch shift is in wz
                 }
                 const int nk = min(32, view_count - k0);
                 for (int j = 0; j < nk; j++) {
@@ -534,7 +535,10 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
 #pragma unroll
                     for (int m = 0; m < MZ; m++) {
                         if (lane + 32 * m < izn) {
-                            const float zc = fadd(zc0[m], cj);
+                            // (iz + wz) * dz + couch (cbct_back.c:100); back,var: (iz + wz) * dz with
+                            // the view's wz (cbct_back_var.c:41, :89)
+                            const float zc = VAR ? fmul(fadd((float)(iz0 + lane + 32 * m), cj), g.dz)
+                                                 : fadd(zc0[m], cj);
                             float vv = fsub(div_by(fmul(zc, w2j), g.dv, g.rdv), g.wv);  // cbct_back.c:102
                             bool use = true;
                             if (OFF) {
@@ -552,7 +556,8 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
                                 const float s0 = fadd(fmul(omv, __ldg(p)), fmul(wvl, __ldg(p + 1)));
                                 const float s1 = fadd(fmul(omv, __ldg(p + g.nv)), fmul(wvl, __ldg(p + g.nv + 1)));
                                 const float val = fadd(fmul(omu, s0), fmul(wul, s1));
-                                acc[m] = fadd(acc[m], fmul(w2sj, val));
+                                // w2s * (...) (cbct_back.c:120); w2s * w2s * (...) (cbct_back_var.c:116)
+                                acc[m] = fadd(acc[m], fmul(VAR ? fmul(w2sj, w2sj) : w2sj, val));
                             }
                         }
                     }
@@ -682,20 +687,21 @@ cudaError_t launch_proj(int method, const Geom &g, const View *views, const floa
     return cudaErrorInvalidValue;
 }
 
-template <bool OFF, int MZ>
+template <int MODE, int MZ>
 static cudaError_t launch_pd_mz(const Geom &g, const View *views, const float *proj, const uint8_t *map,
                                 void *image, int out_dtype, int vb, int vs, int vc, float scale, cudaStream_t st) {
     const int blocks = g.ny * ((g.nx + 7) / 8);
-    pd_kernel<OFF, MZ><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale);
+    pd_kernel<MODE, MZ><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale);
     return cudaGetLastError();
 }
 
-cudaError_t launch_pd(bool off, int mz, const Geom &g, const View *views, const float *proj, const uint8_t *map,
+cudaError_t launch_pd(int mode, int mz, const Geom &g, const View *views, const float *proj, const uint8_t *map,
                       void *image, int out_dtype, int vb, int vs, int vc, float scale, cudaStream_t st) {
 #define CTSIM_PD_CASE(O, Z) \
-    if (off == O && mz == Z) return launch_pd_mz<O, Z>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale, st);
-    CTSIM_PD_CASE(true, 1) CTSIM_PD_CASE(true, 2) CTSIM_PD_CASE(true, 4) CTSIM_PD_CASE(true, 8)
-    CTSIM_PD_CASE(false, 1) CTSIM_PD_CASE(false, 2) CTSIM_PD_CASE(false, 4) CTSIM_PD_CASE(false, 8)
+    if (mode == O && mz == Z) return launch_pd_mz<O, Z>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale, st);
+    CTSIM_PD_CASE(kPdOff, 1) CTSIM_PD_CASE(kPdOff, 2) CTSIM_PD_CASE(kPdOff, 4) CTSIM_PD_CASE(kPdOff, 8)
+    CTSIM_PD_CASE(kPdClamp, 1) CTSIM_PD_CASE(kPdClamp, 2) CTSIM_PD_CASE(kPdClamp, 4) CTSIM_PD_CASE(kPdClamp, 8)
+    CTSIM_PD_CASE(kPdVar, 1) CTSIM_PD_CASE(kPdVar, 2) CTSIM_PD_CASE(kPdVar, 4) CTSIM_PD_CASE(kPdVar, 8)
 #undef CTSIM_PD_CASE
     return cudaErrorInvalidValue;
 }

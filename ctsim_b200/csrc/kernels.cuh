@@ -28,7 +28,10 @@ cudaError_t launch_proj(int method, const Geom &g, const View *views, const floa
                         const uint8_t *map, void *proj, int out_dtype, int view_begin, int view_stride,
                         int view_count, float margin, cudaStream_t st);
 
-cudaError_t launch_pd(bool off_boundary, int mz, const Geom &g, const View *views, const float *proj,
+// voxel-driven bilinear modes: back,pd (v outside the detector skipped), back,hpd (v
+// clamped), back,var (geom/cbct/cbct_back_var.c)
+enum PdMode { kPdOff = 0, kPdClamp = 1, kPdVar = 2 };
+cudaError_t launch_pd(int mode, int mz, const Geom &g, const View *views, const float *proj,
                       const uint8_t *map, void *image, int out_dtype, int view_begin, int view_stride,
                       int view_count, float scale, cudaStream_t st);
 

@@ -22,7 +22,7 @@
 #include "mex.h"
 #include "ctsim_b200.h"
 
-static const char *ARG_TYPES[] = {"proj,dd", "proj,tf", "back,dd", "back,tf", "back,pd", "back,hpd"};
+static const char *ARG_TYPES[] = {"proj,dd", "proj,tf", "back,dd", "back,tf", "back,pd", "back,hpd", "back,var"};
 
 static int known_type(const char *t)
 {

@@ -45,7 +45,7 @@ class _DTypeMap(dict):
 
 
 _DTYPES = _DTypeMap()
-BACK_TYPES = ("back,dd", "back,tf", "back,pd", "back,hpd")
+BACK_TYPES = ("back,dd", "back,tf", "back,pd", "back,hpd", "back,var")
 
 
 def _torch():
@@ -210,7 +210,7 @@ class Plan:
 
     def backproject(self, sino, method: str = "dd", view_begin: int = 0, view_stride: int = 1, view_count=None,
                     scale: float = 1.0, out=None, out_dtype=None):
-        """scale * A^T y (or the FDK pd/hpd backprojection) -> [nz, ny, nx] of ``out_dtype``
+        """scale * A^T y (or the FDK pd/hpd, or the variance backprojection) -> [nz, ny, nx] of ``out_dtype``
         (default: the sinogram's storage type)."""
         torch = _torch()
         vb, vs, vc = self._views(view_begin, view_stride, view_count)
@@ -219,7 +219,8 @@ class Plan:
             out = torch.empty(self.geom.image_shape, dtype=out_dtype or sino.dtype, device=self.device)
         else:
             out = self._check_tensor(out, self.geom.image_shape, "out")
-        m = {"dd": 2, "tf": 3, "pd": 4, "hpd": 5, "back,dd": 2, "back,tf": 3, "back,pd": 4, "back,hpd": 5}[method]
+        m = {"dd": 2, "tf": 3, "pd": 4, "hpd": 5, "var": 6, "back,dd": 2, "back,tf": 3, "back,pd": 4, "back,hpd": 5,
+             "back,var": 6}[method]
         st = torch.cuda.current_stream(self.device).cuda_stream
         _lib.check(self._L.ctsim_plan_backproject_ex(self._h, m, sino.data_ptr(), _DTYPES[sino.dtype],
                                                      out.data_ptr(), _DTYPES[out.dtype], vb, vs, vc, float(scale),

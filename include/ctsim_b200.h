@@ -54,7 +54,8 @@ typedef enum {
     CTSIM_BACK_DD = 2,  /* "back,dd"  */
     CTSIM_BACK_TF = 3,  /* "back,tf"  */
     CTSIM_BACK_PD = 4,  /* "back,pd"  */
-    CTSIM_BACK_HPD = 5  /* "back,hpd" */
+    CTSIM_BACK_HPD = 5, /* "back,hpd" */
+    CTSIM_BACK_VAR = 6  /* "back,var": variance backprojection, geom/cbct/cbct_back_var.c:1 */
 } ctsim_method;
 
 /* Storage types of volumes and sinograms in the plan API (arithmetic is always FP32). */
@@ -112,7 +113,7 @@ bool ctsim_back_pd(int nx, int ny, int nz, float dx, float dy, float dz, float o
                    float *image, const float *proj, const bool *map, bool offBoundary);
 
 /* String dispatch of the reference gateway (geom/cbct/cbct_geom_mex.c:253-312): type is one of
- * "proj,dd" "proj,tf" "back,dd" "back,tf" "back,pd" "back,hpd"; data is the image for "proj,*"
+ * "proj,dd" "proj,tf" "back,dd" "back,tf" "back,pd" "back,hpd" "back,var"; data is the image for "proj,*"
  * and the sinogram for "back,*"; out is the sinogram or image. */
 bool ctsim_cbct_geom(const char *type, int nx, int ny, int nz, float dx, float dy, float dz, float offset_x,
                      float offset_y, float offset_z, int nu, int nv, float du, float dv, float offset_u,
@@ -168,7 +169,7 @@ ctsim_status ctsim_plan_project(ctsim_plan *plan, int method, const float *d_ima
 
 /* Backprojection of view_count views read contiguously from d_proj (same view selection
  * as ctsim_plan_project).  The image is overwritten with (scale * A^T y); map-off columns are 0.
- * method: CTSIM_BACK_DD / CTSIM_BACK_TF / CTSIM_BACK_PD / CTSIM_BACK_HPD. */
+ * method: CTSIM_BACK_DD / CTSIM_BACK_TF / CTSIM_BACK_PD / CTSIM_BACK_HPD / CTSIM_BACK_VAR. */
 ctsim_status ctsim_plan_backproject(ctsim_plan *plan, int method, const float *d_proj, float *d_image,
                                     int view_begin, int view_stride, int view_count, float scale, void *stream);
 

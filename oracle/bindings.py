@@ -47,7 +47,8 @@ def _load(path):
             lib.orc_proj.argtypes = [_i] + _GEOM_ARGS
             lib.orc_back.argtypes = [_i] + _GEOM_ARGS
             lib.orc_back_pd.argtypes = _GEOM_ARGS + [_i]
-            for fn in (lib.orc_proj, lib.orc_back, lib.orc_back_pd):
+            lib.orc_back_var.argtypes = _GEOM_ARGS
+            for fn in (lib.orc_proj, lib.orc_back, lib.orc_back_pd, lib.orc_back_var):
                 fn.restype = _i
         else:
             lib.ref_cbct_call.argtypes = [_i] + _GEOM_ARGS
@@ -94,6 +95,8 @@ def oracle_cbct(kind: str, geom, data, fp64: bool = False) -> np.ndarray:
         ok = lib.orc_back(KINDS[kind] - 2, *args)
     elif kind in ("back,pd", "back,hpd"):
         ok = lib.orc_back_pd(*args, 1 if kind == "back,pd" else 0)
+    elif kind == "back,var":
+        ok = lib.orc_back_var(*args)
     else:
         raise NotImplementedError(kind)
     if not ok:

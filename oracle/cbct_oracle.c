@@ -399,3 +399,61 @@ int orc_back_pd(int nx, int ny, int nz, float dx, float dy, float dz, float ox, 
     }
     return 1;
 }
+
+/* Variance backprojection, back,var: geom/cbct/cbct_back_var.c:1-129 as the MEX calls it
+ * (offBoundary = true, geom/cbct/cbct_geom_mex.c:242).  Against back,pd: the couch shift
+ * enters wz in voxels (:41) instead of zc in mm, the curved-detector offset is
+ * offset_u * sad / sdd (:70, without du), and the weight is w2s^2 (:116). */
+int orc_back_var(int nx, int ny, int nz, float dx, float dy, float dz, float ox, float oy, float oz, int nu, int nv,
+                 float du, float dv, float ou, float ov, float sad, float add, float sdd, int noviews,
+                 const double *betas, const float *couchz, int detector_type, const real *proj, real *image,
+                 const bool *map)
+{
+    (void)add;
+    orc_geom g = orc_make_geom(nx, ny, nz, dx, dy, dz, ox, oy, oz, nu, nv, du, dv, ou, ov, sad, sdd, detector_type);
+    long nxy = (long)nx * ny, nuv = (long)nu * nv;
+    memset(image, 0, sizeof(real) * nxy * nz);
+    for (int ib = 0; ib < noviews; ib++) {
+        real wz = (real)(-((double)nz - 1.0) / 2.0 + (double)oz + (double)(couchz[ib] / dz));
+        real sin_a = (real)sin(betas[ib]);
+        real cos_a = (real)cos(betas[ib]);
+        const real *pv = proj + nuv * ib;
+        for (int iy = 0; iy < ny; iy++) {
+            for (int ix = 0; ix < nx; ix++) {
+                if (!map[iy * nx + ix]) continue;
+                real xc = ((real)ix + g.wx) * dx;
+                real yc = ((real)iy + g.wy) * dy;
+                real xr = xc * cos_a - yc * sin_a;
+                real yr = xc * sin_a + yc * cos_a;
+                real w2, w2s, u;
+                if (detector_type == 1) {
+                    w2 = sdd / (sad + yr);
+                    w2s = w2 * w2;
+                    u = xr * w2 / du - g.wu;
+                } else {
+                    real roff = ou * sad / sdd;
+                    u = (real)(atan((double)((xr - roff) / (sad + yr))) * (double)sdd / (double)du - (double)g.wu);
+                    w2s = sdd * sdd / ((sad + yr) * (sad + yr) + (xr - roff) * (xr - roff));
+                    w2 = sdd / (sad + yr);
+                }
+                if ((double)u < 1e-6 || (double)u > (double)nu - 1.0 - 1e-6) continue;
+                int iu = (int)floor(u);
+                real wul = u - (real)iu;
+                for (int iz = 0; iz < nz; iz++) {
+                    real zc = ((real)iz + wz) * dz;
+                    real vv = zc * w2 / dv - g.wv;
+                    if ((double)vv < 1e-6) continue;
+                    if ((double)vv > (double)nv - 1.0 - 1e-6) break;
+                    int iv = (int)floor(vv);
+                    real wvl = vv - (real)iv;
+                    const real *p = pv + (long)iu * nv + iv;
+                    real s0 = ((real)1.0 - wvl) * p[0] + wvl * p[1];
+                    real s1 = ((real)1.0 - wvl) * p[nv] + wvl * p[nv + 1];
+                    long idx = iz * nxy + (long)iy * nx + ix;
+                    image[idx] = image[idx] + w2s * w2s * (((real)1.0 - wul) * s0 + wul * s1);
+                }
+            }
+        }
+    }
+    return 1;
+}

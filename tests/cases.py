@@ -50,4 +50,4 @@ def case_inputs(geom, seed=0):
     return x, y
 
 
-KINDS = ("proj,dd", "proj,tf", "back,dd", "back,tf", "back,pd", "back,hpd")
+KINDS = ("proj,dd", "proj,tf", "back,dd", "back,tf", "back,pd", "back,hpd", "back,var")
