@@ -174,8 +174,10 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
         return fail(CTSIM_ERR_ARGUMENT, "sizes must be positive (nu, nv >= 2)");
     if (!(G.dx > 0 && G.dy > 0 && G.dz > 0 && G.du > 0 && G.dv > 0 && G.sad > 0 && G.sdd > 0))
         return fail(CTSIM_ERR_ARGUMENT, "spacings and distances must be positive");
-    if (G.detector_type != 0 && G.detector_type != 1)
-        return fail(CTSIM_ERR_ARGUMENT, "detector_type must be 1 (flat) or 0 (curved)");
+    if (G.detector_type != 0 && G.detector_type != 1 && G.detector_type != 2)
+        return fail(CTSIM_ERR_ARGUMENT, "detector_type must be 1 (flat), 0 (curved) or 2 (arc)");
+    if (G.detector_type == 2 && !(G.add > 0))
+        return fail(CTSIM_ERR_ARGUMENT, "the arc detector needs ADD > 0");
     const long long nxy = (long long)G.nx * G.ny;
     if (nxy * G.nz > (1LL << 31) - 1 || (long long)G.nu * G.nv * G.noviews > (1LL << 40))
         return fail(CTSIM_ERR_ARGUMENT, "volume too large");
@@ -205,6 +207,8 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
     g.wz_pd = centre(G.nz, G.offset_z);
     g.roff = G.offset_u * G.du * G.sad / G.sdd;
     g.roff_var = G.offset_u * G.sad / G.sdd;
+    g.add = G.add;
+    g.sad_add = G.detector_type == 2 ? G.sad / G.add : 0.0f;
     g.u_lo = float_at_or_above(1e-6);
     g.u_hi = float_at_or_below((double)G.nu - 1.0 - 1e-6);
     g.v_lo = float_at_or_above(1e-6);
@@ -242,8 +246,16 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
         for (int iv = 0; iv < G.nv; iv++) {
             const float v = ((float)iv + g.wv) * G.dv;
             float a;
-            if (G.detector_type == 1) a = (float)std::sqrt((double)((uu + v * v) / uu));
-            else a = (float)(std::sqrt((double)(G.sdd * G.sdd + v * v)) / (double)G.sdd);
+            if (G.detector_type == 1) {
+                a = (float)std::sqrt((double)((uu + v * v) / uu));
+            } else if (G.detector_type == 0) {
+                a = (float)(std::sqrt((double)(G.sdd * G.sdd + v * v)) / (double)G.sdd);
+            } else {  // arc: squared source-to-cell distance in double, stored in float (cbct_proj3.c:480-482)
+                const double ca = std::cos((double)(u / G.add)), sa = std::sin((double)(u / G.add));
+                const float s2 = (float)(((double)G.sad + (double)G.add * ca) * ((double)G.sad + (double)G.add * ca) +
+                                         ((double)G.add * sa) * ((double)G.add * sa));
+                a = (float)std::sqrt((double)((s2 + v * v) / s2));
+            }
             ampv[(size_t)iu * G.nv + iv] = a;
         }
     }
@@ -268,7 +280,21 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
     }
     p->zinc_max = (float)((double)G.dz / G.dv * G.sdd / ((double)G.sad - rmax) * 1.0001 + 1e-6);
     const double umm = std::max(std::fabs((double)g.wu * G.du), std::fabs(((double)G.nu - 1 + g.wu) * G.du)) + G.du;
-    const double stretch = G.detector_type == 1 ? 1.0 + (umm / G.sdd) * (umm / G.sdd) : 1.0;
+    double stretch = G.detector_type == 1 ? 1.0 + (umm / G.sdd) * (umm / G.sdd) : 1.0;
+    if (G.detector_type == 2) {
+        // arc: du/dgamma = add (1 + k cos g / sqrt(1 - k^2 sin^2 g)), k = sad/add, grows with
+        // the fan angle; sdd = sad + add is its value at g = 0
+        const double k = (double)G.sad / G.add;
+        const double sg = std::min(1.0, (rmax + diag) / G.sad);  // largest |sin(fan angle)| of a voxel edge
+        if (k * sg >= 0.999) {
+            free_plan(p);
+            return fail(CTSIM_ERR_UNSUPPORTED,
+                        "arc detector: the volume's fan angle leaves the arc (sad/add * sin(gamma) >= 1)");
+        }
+        const double cg = std::sqrt(1.0 - sg * sg);
+        stretch = (1.0 + k * cg / std::sqrt(1.0 - k * k * sg * sg)) / (1.0 + k) * ((double)G.sad + G.add) / G.sdd;
+        stretch = std::max(stretch, 1.0);
+    }
     p->margin = (float)std::ceil(0.5 * diag * G.sdd / dmin / G.du * stretch) + 2.0f;
     if (p->zinc_max > 9.0f) {
         // the kernels integrate the axial footprint exactly; the reference truncates
@@ -345,11 +371,15 @@ static ctsim_status check_views(const ctsim_plan *p, int vb, int vs, int vc) {
 
 static bool dtype_ok(int d) { return d == CTSIM_F32 || d == CTSIM_BF16 || d == CTSIM_F16; }
 
+static const char *kArcOnlyDD =
+    "the arc detector (detector_type 2) is defined for the distance-driven pair only (geom/cbct/cbct_proj3.c)";
+
 extern "C" ctsim_status ctsim_plan_project_ex(ctsim_plan *p, int method, const void *d_image, int image_dtype,
                                               void *d_proj, int proj_dtype, int view_begin, int view_stride,
                                               int view_count, void *stream) {
     if (!p || !d_image || !d_proj) return fail(CTSIM_ERR_ARGUMENT, "null argument");
     if (method != CTSIM_PROJ_DD && method != CTSIM_PROJ_TF) return fail(CTSIM_ERR_ARGUMENT, "unknown forward method");
+    if (p->g.det == 2 && method != CTSIM_PROJ_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
     if (!dtype_ok(image_dtype) || !dtype_ok(proj_dtype)) return fail(CTSIM_ERR_ARGUMENT, "unknown storage type");
     ctsim_status s = check_views(p, view_begin, view_stride, view_count);
     if (s != CTSIM_OK) return s;
@@ -375,6 +405,7 @@ extern "C" ctsim_status ctsim_plan_backproject_ex(ctsim_plan *p, int method, con
                                                   int view_count, float scale, void *stream) {
     if (!p || !d_image || !d_proj) return fail(CTSIM_ERR_ARGUMENT, "null argument");
     if (!dtype_ok(image_dtype) || !dtype_ok(proj_dtype)) return fail(CTSIM_ERR_ARGUMENT, "unknown storage type");
+    if (p->g.det == 2 && method != CTSIM_BACK_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
     ctsim_status s = check_views(p, view_begin, view_stride, view_count);
     if (s != CTSIM_OK) return s;
     cudaStream_t st = (cudaStream_t)stream;

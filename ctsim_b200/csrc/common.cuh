@@ -38,7 +38,7 @@ constexpr int kMaxRowsV = 10;   // ivmax <= ivmin + 9 (10)    geom/cbct/cbct_pro
 
 // Scalars shared by every kernel (passed by value).
 struct Geom {
-    int nx, ny, nz, nu, nv, det;  // det: 1 flat, 0 curved
+    int nx, ny, nz, nu, nv, det;  // det: 1 flat, 0 curved, 2 arc about the axis (DD pair only)
     float dx, dy, dz, sad, sdd, du, dv;
     float wx, wy, wu, wv;         // centre offsets, geom/cbct/cbct_proj.c:244-247
     float sdd_du;                 // sdd / du                  :248
@@ -52,6 +52,7 @@ struct Geom {
     float u_lo, u_hi, v_lo, v_hi;
     float v_clamp_lo, v_clamp_hi; // hpd clamps 0.5 and nv - 1.5 as floats (cbct_back.c:110-111)
     float rdv;                    // RN(1/dv) for the correctly rounded division by dv, 0 = use IEEE division
+    float add, sad_add;           // arc detector: radius ADD, sad / add (geom/cbct/cbct_proj3.c:337-355)
 };
 
 // Per-view constants, geom/cbct/cbct_proj.c:256-265 and cbct_back.c:50-52.
@@ -106,6 +107,13 @@ struct ColumnFP {
 // (geom/cbct/cbct_proj.c:301 flat, :316 curved).
 __device__ __forceinline__ float u_of(const Geom &g, float num, float den) {
     if (g.det == 1) return fsub(fdiv(fmul(g.sdd_du, num), den), g.wu);
+    if (g.det == 2) {
+        // arc: fan angle gam, arc angle xi = gam + asin(sad/add sin gam) where the ray meets
+        // the arc, u = xi * add / du - wu (geom/cbct/cbct_proj3.c:337-343)
+        const float gam = (float)atan((double)fdiv(num, den));
+        const float xi = (float)__dadd_rn((double)gam, asin(__dmul_rn((double)g.sad_add, sin((double)gam))));
+        return fsub(fdiv(fmul(xi, g.add), g.du), g.wu);
+    }
     double r = (double)fdiv(num, den);
     return (float)__dsub_rn(__dmul_rn((double)g.sdd_du, atan(r)), (double)g.wu);
 }
@@ -135,7 +143,9 @@ __device__ __forceinline__ ColumnFP column_footprint(const Geom &g, const View &
         } else {
             c.ampu = fdiv(fdiv(g.dx, sin_phi), 10.0f);
             umin = u_of(g, fadd(tproj0, v.dy_sin_2), fadd(dsxy0, v.n_dy_cos_2));
-            umax = u_of(g, fsub(tproj0, v.dy_sin_2), fsub(dsxy0, v.n_dy_cos_2));
+            // the arc code takes this edge from the x offsets (cbct_proj3.c:351, cbct_back3.c:300)
+            umax = g.det == 2 ? u_of(g, fsub(tproj0, v.dx_cos_2), fsub(dsxy0, v.dx_sin_2))
+                              : u_of(g, fsub(tproj0, v.dy_sin_2), fsub(dsxy0, v.n_dy_cos_2));
         }
         if (umin >= umax) { float t = umax; umax = umin; umin = t; }
         maxbins = kMaxBinsDD;

@@ -244,6 +244,8 @@ extern "C" ctsim_status ctsim_fdk_create(ctsim_plan *plan, const char *window, f
     if (!plan || !out) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
     if (!window || !window_known(window)) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "Invalid window selected.");
     const ctsim_geom &G = *ctsim_plan_geom(plan);
+    if (G.detector_type != 0 && G.detector_type != 1)
+        return ctsim_set_last_error(CTSIM_ERR_UNSUPPORTED, "FDK needs a flat (1) or curved (0) detector");
     const double *betas = ctsim_plan_betas(plan);
     const bool flat = G.detector_type == 1;
     ctsim_fdk *f = new ctsim_fdk();

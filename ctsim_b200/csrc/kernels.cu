@@ -314,7 +314,16 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
         const float tp = xcf * v.cos_a - ycf * v.sin_a;
         const float ds = g.sad + xcf * v.sin_a + ycf * v.cos_a;
         const float r = __fdividef(tp, ds);
-        return (g.det == 1 ? g.sdd_du * r : g.sdd_du * atanf(r)) - g.wu + 0.5f;
+        float u;
+        if (g.det == 1) {
+            u = g.sdd_du * r;
+        } else if (g.det == 0) {
+            u = g.sdd_du * atanf(r);
+        } else {  // arc (candidate search only; the footprints are exact)
+            const float gam = atanf(r);
+            u = (gam + asinf(g.sad_add * sinf(gam))) * g.add / g.du;
+        }
+        return u - g.wu + 0.5f;
     };
 
     // 1. candidate interval of every line (binary search on the monotone centre projection)

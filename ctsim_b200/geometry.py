@@ -105,3 +105,27 @@ class CTGeometry:
 def circular_betas(n_views: int, arc: float = 2 * np.pi) -> np.ndarray:
     """Evenly spaced view angles ``(0:N-1) * arc / N`` (geom/test_projectors_3d.m:59)."""
     return np.arange(n_views, dtype=np.float64) * (arc / n_views)
+
+
+def helical_geometry(reconSize, reconSpacing, reconOffset, detSize, detSpacing, detOffset, SAD: float, ADD: float,
+                     noViewsTurn: int, noTurns: int, pitch: float, flatPanel: int = 1) -> CTGeometry:
+    """Helical scan (parameters/loadProjectionGeometryHelicalCT.m:16-57): noViewsTurn *
+    noTurns + 1 views centred on beta = pi, the couch advancing pitch * (detector height)
+    per turn (couchZ in mm, centred on 0), and the FOV map of the fan."""
+    SDD = SAD + ADD
+    n_views = int(noViewsTurn) * int(noTurns) + 1
+    k = np.arange(1, n_views + 1, dtype=np.float64) - (n_views + 1) / 2.0
+    couch_spacing = pitch * detSize[1] * detSpacing[1] / noViewsTurn
+    betas = k * 2.0 * np.pi / noViewsTurn + np.pi
+    couch = (k * couch_spacing).astype(np.float32)
+    half_fan = detSize[0] * detSpacing[0] / 2.0 / SDD
+    if flatPanel:
+        half_fan = np.arctan(half_fan)
+    fov = 2.0 * np.sin(half_fan) * SAD
+    nx, ny = int(reconSize[0]), int(reconSize[1])
+    x = np.arange(nx) - (nx - 1) / 2.0
+    y = np.arange(ny) - (ny - 1) / 2.0
+    radius = max(max(reconSize), fov / reconSpacing[0]) / 2.0
+    mask = np.sqrt(x[None, :] ** 2 + y[:, None] ** 2) < radius      # [ny, nx]
+    return CTGeometry(reconSize, reconSpacing, reconOffset, detSize, detSpacing, detOffset, SAD, ADD, SDD, betas,
+                      couchZ=couch, flatPanel=flatPanel, map=mask, shortScan=True)

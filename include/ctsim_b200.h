@@ -15,7 +15,9 @@
  *      proj    float[noviews][nu][nv]   (MATLAB single [nv nu noviews], v fastest)
  *      map     bool[ny][nx]             (MATLAB logical [nx ny])
  *      betas   double[noviews] (radians), couchz float[noviews] (mm)
- *      detector_type: 1 flat panel, 0 curved (equiangular)
+ *      detector_type: 1 flat panel, 0 curved (equiangular), 2 arc of radius ADD about the
+ *      rotation axis (geom/cbct/cbct_proj3.c, cbct_back3.c: the distance-driven pair only;
+ *      other methods return CTSIM_ERR_UNSUPPORTED)
  *
  *    Outputs are overwritten (the reference MEX allocates them zero-filled and
  *    accumulates; the result is the same).

@@ -3,6 +3,8 @@
 * ``oracle_cbct``  -> this project's CPU restatement, ``_build/libcbct_oracle.so``
 * ``ref_cbct``     -> the reference's own geom/cbct C, ``_ref/libcbct_ref.so``
                       (single-threaded, or over view chunks with ``nthreads``)
+* ``ref3_cbct``    -> the reference's arc-detector DD pair (geom/cbct/cbct_proj3.c,
+                      cbct_back3.c), ``_ref/libcbct_ref3.so``
 
 Both take and return numpy arrays in the package conventions
 (image ``[nz, ny, nx]``, sino ``[noViews, nu, nv]``, float32).
@@ -19,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libcbct_oracle.so")
 ORACLE64_SO = os.path.join(HERE, "_build", "libcbct_oracle64.so")
 REF_SO = os.path.join(HERE, "_ref", "libcbct_ref.so")
+REF3_SO = os.path.join(HERE, "_ref", "libcbct_ref3.so")
 
 KINDS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3,
          "back,pd": 4, "back,hpd": 5, "back,var": 6}
@@ -50,6 +53,9 @@ def _load(path):
             lib.orc_back_var.argtypes = _GEOM_ARGS
             for fn in (lib.orc_proj, lib.orc_back, lib.orc_back_pd, lib.orc_back_var):
                 fn.restype = _i
+        elif path == REF3_SO:
+            lib.ref3_cbct_call.argtypes = [_i] + _GEOM_ARGS
+            lib.ref3_cbct_call.restype = _i
         else:
             lib.ref_cbct_call.argtypes = [_i] + _GEOM_ARGS
             lib.ref_cbct_call.restype = _i
@@ -113,5 +119,16 @@ def ref_cbct(kind: str, geom, data, nthreads: int = 1) -> np.ndarray:
     else:
         ok = lib.ref_cbct_call_mt(int(nthreads), KINDS[kind], *args)
     if not ok:
+        raise RuntimeError("reference call failed")
+    return out
+
+
+def ref3_cbct(kind: str, geom, data) -> np.ndarray:
+    """The reference's arc-detector variants of proj,dd / back,dd (needs _ref/libcbct_ref3.so)."""
+    if kind not in ("proj,dd", "back,dd"):
+        raise ValueError("the reference's arc-detector code covers proj,dd and back,dd")
+    lib = _load(REF3_SO)
+    data, out, args, keep = _prep(kind, geom, data)
+    if not lib.ref3_cbct_call(KINDS[kind], *args):
         raise RuntimeError("reference call failed")
     return out

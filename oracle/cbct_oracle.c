@@ -52,6 +52,7 @@ typedef struct {
     real dx, dy, dz, sad, sdd, du, dv;
     real wx, wy, wu, wv, sdd_du;
     real oz;
+    real add, sad_add; /* arc detector (detector_type 2): radius ADD about the axis, sad/add */
 } orc_geom;
 
 /* Per-view constants (geom/cbct/cbct_proj.c:256-265). */
@@ -77,6 +78,19 @@ static orc_geom orc_make_geom(int nx, int ny, int nz, real dx, real dy, real dz,
     g.wv = orc_centre(nv, ov);
     g.sdd_du = sdd / du;
     g.oz = oz;
+    g.add = 0;
+    g.sad_add = 0;
+    return g;
+}
+
+/* The arc detector needs ADD (geom/cbct/cbct_proj3.c:337-355). */
+static orc_geom orc_make_geom_add(int nx, int ny, int nz, real dx, real dy, real dz, real ox, real oy, real oz,
+                                  int nu, int nv, real du, real dv, real ou, real ov, real sad, real add, real sdd,
+                                  int detector_type)
+{
+    orc_geom g = orc_make_geom(nx, ny, nz, dx, dy, dz, ox, oy, oz, nu, nv, du, dv, ou, ov, sad, sdd, detector_type);
+    g.add = add;
+    g.sad_add = sad / add;
     return g;
 }
 
@@ -128,6 +142,13 @@ static void orc_column_centre(const orc_geom *g, const orc_view *v, int ix, int 
 static real orc_u_of(const orc_geom *g, real num, real den)
 {
     if (g->detector_type == 1) return g->sdd_du * num / den - g->wu;
+    if (g->detector_type == 2) {
+        /* arc: fan angle gam of the ray, arc angle xi = gam + asin(sad/add sin gam) where it
+         * meets the arc, u = xi * add / du - wu (geom/cbct/cbct_proj3.c:337-343) */
+        real gam = (real)atan((double)(num / den));
+        real xi = (real)((double)gam + asin((double)g->sad_add * sin((double)gam)));
+        return xi * g->add / g->du - g->wu;
+    }
     /* curved: sdd_du * atan(ratio) - wu in double, geom/cbct/cbct_proj.c:316 */
     return (real)((double)g->sdd_du * atan((double)(num / den)) - (double)g->wu);
 }
@@ -159,7 +180,10 @@ static void orc_column_dd(const orc_geom *g, const orc_view *v, int ix, int iy, 
     } else {
         c->ampu = (real)((double)(g->dx / sin_phi) / 10.0);
         umin = orc_u_of(g, tproj0 + v->dy_sin_2, dsxy0 + v->n_dy_cos_2);
-        umax = orc_u_of(g, tproj0 - v->dy_sin_2, dsxy0 - v->n_dy_cos_2);
+        if (g->detector_type == 2) /* the arc code takes this edge from the x offsets, cbct_proj3.c:351 */
+            umax = orc_u_of(g, tproj0 - v->dx_cos_2, dsxy0 - v->dx_sin_2);
+        else
+            umax = orc_u_of(g, tproj0 - v->dy_sin_2, dsxy0 - v->n_dy_cos_2);
     }
     if (umin >= umax) { real t = umax; umax = umin; umin = t; }
     umin = umin + (real)0.5; if (!(umin > (real)0.0)) umin = (real)0.0;
@@ -250,6 +274,14 @@ static real orc_ampv(const orc_geom *g, int iu, int iv)
     real uu = g->sdd * g->sdd + u * u;
     real v = ((real)iv + g->wv) * g->dv;
     if (g->detector_type == 1) return (real)sqrt((double)((uu + v * v) / uu));
+    if (g->detector_type == 2) {
+        /* source-to-arc-cell distance squared in double, stored in float (cbct_proj3.c:480-482) */
+        double ca = cos((double)(u / g->add)), sa = sin((double)(u / g->add));
+        double a = ((double)g->sad + (double)g->add * ca) * ((double)g->sad + (double)g->add * ca) +
+                   ((double)g->add * sa) * ((double)g->add * sa);
+        real s2 = (real)a;
+        return (real)sqrt((double)((s2 + v * v) / s2));
+    }
     return (real)(sqrt((double)(g->sdd * g->sdd + v * v)) / (double)g->sdd);
 }
 
@@ -265,8 +297,10 @@ int orc_proj(int kind, int nx, int ny, int nz, float dx, float dy, float dz, flo
              const double *betas, const float *couchz, int detector_type, const real *image, real *proj,
              const bool *map)
 {
-    (void)add;
-    orc_geom g = orc_make_geom(nx, ny, nz, dx, dy, dz, ox, oy, oz, nu, nv, du, dv, ou, ov, sad, sdd, detector_type);
+    /* the arc detector is defined for the distance-driven pair only (cbct_proj3.c, cbct_back3.c) */
+    if (detector_type == 2 && kind != ORC_DD) return 0;
+    orc_geom g = orc_make_geom_add(nx, ny, nz, dx, dy, dz, ox, oy, oz, nu, nv, du, dv, ou, ov, sad, add, sdd,
+                                   detector_type);
     long nxy = (long)nx * ny, nuv = (long)nu * nv;
     memset(proj, 0, sizeof(real) * nuv * noviews);
     for (int ib = 0; ib < noviews; ib++) {
@@ -303,8 +337,10 @@ int orc_back(int kind, int nx, int ny, int nz, float dx, float dy, float dz, flo
              const double *betas, const float *couchz, int detector_type, const real *proj, real *image,
              const bool *map)
 {
-    (void)add;
-    orc_geom g = orc_make_geom(nx, ny, nz, dx, dy, dz, ox, oy, oz, nu, nv, du, dv, ou, ov, sad, sdd, detector_type);
+    /* the arc detector is defined for the distance-driven pair only (cbct_proj3.c, cbct_back3.c) */
+    if (detector_type == 2 && kind != ORC_DD) return 0;
+    orc_geom g = orc_make_geom_add(nx, ny, nz, dx, dy, dz, ox, oy, oz, nu, nv, du, dv, ou, ov, sad, add, sdd,
+                                   detector_type);
     long nxy = (long)nx * ny, nuv = (long)nu * nv;
     real *scaled = (real *)malloc(sizeof(real) * (nuv > 0 ? nuv : 1));
     if (!scaled) return 0;

@@ -41,6 +41,22 @@ def make_cases():
     return cases
 
 
+def make_arc_cases():
+    """Arc-detector geometries (detector_type 2: an arc of radius ADD about the rotation
+    axis, geom/cbct/cbct_proj3.c), for the distance-driven pair only."""
+    rng = np.random.default_rng(20261204)
+    cases = {}
+    cases["arc_basic"] = _geom((24, 20, 10), (1.0, 1.0, 1.0), (0, 0, 0), (48, 16), (1.2, 1.6), (0, 0), 11, flat=2)
+    cases["arc_offsets_couch"] = _geom((20, 22, 9), (1.0, 1.0, 1.0), (0.3, -0.2, 0.7), (44, 14), (1.3, 1.6),
+                                       (1.5, -0.5), 13, flat=2, betas=np.sort(rng.uniform(0, 2 * np.pi, 13)),
+                                       couch=np.linspace(-4.0, 4.0, 13).astype(np.float32),
+                                       mask=rng.random((22, 20)) > 0.2)
+    return cases
+
+
+ARC_KINDS = ("proj,dd", "back,dd")
+
+
 def case_inputs(geom, seed=0):
     """Seeded non-negative image (with exact zeros) and sinogram for a case."""
     rng = np.random.default_rng(seed)

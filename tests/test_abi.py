@@ -85,3 +85,20 @@ def test_subset_selection_matches_reference_indexing():
             assert np.array_equal(s.betas, want)
     y = np.arange(11 * 2 * 3).reshape(11, 2, 3)
     assert np.array_equal(ctsim_b200.orderedSubset(y, 4, 5), y[1::4])
+
+
+def test_helical_geometry_follows_the_loader():
+    """parameters/loadProjectionGeometryHelicalCT.m:26-57 restated by hand for a small scan."""
+    from ctsim_b200.geometry import helical_geometry
+    g = helical_geometry((8, 6, 4), (0.5, 0.5, 1.0), (0, 0, 0), (30, 10), (1.2, 2.0), (0, 0), 900.0, 600.0, 10, 2,
+                         1.5, flatPanel=0)
+    n = 10 * 2 + 1
+    k = np.arange(1, n + 1) - (n + 1) / 2
+    assert g.noViews == n and g.SDD == 1500.0 and g.shortScan
+    assert np.allclose(g.betas, k * 2 * np.pi / 10 + np.pi)
+    assert np.allclose(g.couchZ, k * (1.5 * 10 * 2.0 / 10), atol=1e-5)
+    fov = 2 * np.sin(30 * 1.2 / 2 / 1500) * 900
+    r = max(8, fov / 0.5) / 2
+    xx = np.arange(8) - 3.5
+    yy = np.arange(6) - 2.5
+    assert np.array_equal(g.map, np.hypot(xx[None, :], yy[:, None]) < r)

@@ -12,10 +12,12 @@ import os
 import numpy as np
 import pytest
 
-from cases import KINDS, case_inputs, make_cases
+from cases import ARC_KINDS, KINDS, case_inputs, make_arc_cases, make_cases
 from oracle.bindings import oracle_cbct, ref_available, ref_cbct
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN_DIR = os.path.join(os.path.dirname(__file__), "golden")
+# the arc-detector fixtures (DD only) are checked on their own below
+GOLDEN = sorted(p for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")) if not os.path.basename(p).startswith("arc_"))
 CASES = make_cases()
 
 
@@ -76,3 +78,18 @@ def test_oracle_adjointness():
         lhs = float(np.sum(ax * y))
         rhs = float(np.sum(x.astype(np.float64) * aty))
         assert abs(lhs - rhs) / abs(lhs) < 1e-6
+
+
+@pytest.mark.parametrize("name", sorted(make_arc_cases()))
+def test_oracle_arc_detector_matches_reference(name):
+    """The arc-detector DD pair (detector_type 2) against the reference's cbct_proj3.c /
+    cbct_back3.c fixtures: bit-exact; and the pair is adjoint."""
+    g = make_arc_cases()[name]
+    d = np.load(os.path.join(GOLDEN_DIR, f"{name}.npz"))
+    for k in ARC_KINDS:
+        src = d["image_in"] if k.startswith("proj") else d["sino_in"]
+        assert np.array_equal(oracle_cbct(k, g, src), d[k.replace(",", "_")]), k
+    x, y = case_inputs(g, seed=3)
+    lhs = float(np.sum(oracle_cbct("proj,dd", g, x).astype(np.float64) * y))
+    rhs = float(np.sum(x.astype(np.float64) * oracle_cbct("back,dd", g, y)))
+    assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
