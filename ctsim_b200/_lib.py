@@ -27,7 +27,8 @@ EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd
             "ctsim_penalty", "ctsim_sqs_update", "ctsim_plan_project_ex", "ctsim_plan_backproject_ex",
             "ctsim_pwls_residual_ex", "ctsim_fdk_filter_ex", "ctsim_fdk_run_ex",
             "ctsim_plan_create_async", "ctsim_pool_trim", "ctsim_nesterov_update",
-            "ctsim_simulate_counts", "ctsim_log_attenuation"]
+            "ctsim_simulate_counts", "ctsim_log_attenuation", "ctsim_fbct_geom", "ctsim_fan_plan_create",
+            "ctsim_fan_plan_destroy", "ctsim_fan_project", "ctsim_fan_backproject"]
 
 
 class CtsimGeom(C.Structure):
@@ -35,6 +36,12 @@ class CtsimGeom(C.Structure):
                 ("offset_x", _f), ("offset_y", _f), ("offset_z", _f), ("nu", _i), ("nv", _i),
                 ("du", _f), ("dv", _f), ("offset_u", _f), ("offset_v", _f),
                 ("sad", _f), ("add", _f), ("sdd", _f), ("noviews", _i), ("detector_type", _i)]
+
+
+class CtsimFanGeom(C.Structure):
+    _fields_ = [("nx", _i), ("ny", _i), ("dx", _f), ("dy", _f), ("offset_x", _f), ("offset_y", _f), ("nu", _i),
+                ("du", _f), ("offset_u", _f), ("sad", _f), ("add", _f), ("sdd", _f), ("noviews", _i),
+                ("detector_type", _i)]
 
 
 class CtsimError(RuntimeError):
@@ -82,6 +89,16 @@ def load():
     L.ctsim_nesterov_update.argtypes = [_i, _f, _f, _i, _i, _i, _p, _p, _p, _p, _p, C.c_double, C.c_double, _p,
                                         _p, _p]
     L.ctsim_nesterov_update.restype = _i
+    L.ctsim_fbct_geom.argtypes = [C.c_char_p, _i, _i, _f, _f, _f, _f, _i, _f, _f, _f, _f, _f, _i, _p, _i, _p, _p]
+    L.ctsim_fbct_geom.restype = C.c_bool
+    L.ctsim_fan_plan_create.argtypes = [C.POINTER(CtsimFanGeom), _p, C.POINTER(_p)]
+    L.ctsim_fan_plan_create.restype = _i
+    L.ctsim_fan_plan_destroy.argtypes = [_p]
+    L.ctsim_fan_plan_destroy.restype = _i
+    L.ctsim_fan_project.argtypes = [_p, _i, _p, _p, _i, _i, _i, _p]
+    L.ctsim_fan_project.restype = _i
+    L.ctsim_fan_backproject.argtypes = [_p, _i, _p, _p, _i, _i, _i, _f, _p]
+    L.ctsim_fan_backproject.restype = _i
     L.ctsim_simulate_counts.argtypes = [_p, C.c_size_t, _f, _f, C.c_uint64, _i, _p, _p, _p]
     L.ctsim_simulate_counts.restype = _i
     L.ctsim_log_attenuation.argtypes = [_p, C.c_size_t, _f, _p, C.c_size_t, _p, _p]

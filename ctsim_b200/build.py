@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libctsim_b200.so")
-SOURCES = ["kernels.cu", "capi.cu", "noalloc.cu", "fdk.cu", "pwls.cu", "sino.cu"]
+SOURCES = ["kernels.cu", "capi.cu", "noalloc.cu", "fdk.cu", "pwls.cu", "sino.cu", "fan.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 FLAGS = [

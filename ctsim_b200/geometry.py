@@ -129,3 +129,47 @@ def helical_geometry(reconSize, reconSpacing, reconOffset, detSize, detSpacing, 
     mask = np.sqrt(x[None, :] ** 2 + y[:, None] ** 2) < radius      # [ny, nx]
     return CTGeometry(reconSize, reconSpacing, reconOffset, detSize, detSpacing, detOffset, SAD, ADD, SDD, betas,
                       couchZ=couch, flatPanel=flatPanel, map=mask, shortScan=True)
+
+
+@dataclass
+class FanGeometry:
+    """2-D fan-beam geometry, the arguments of geom/fbct/fbct_geom_mex.c:66-84:
+    image ``[ny, nx]`` (MATLAB ``[nx ny]``), sinogram ``[noViews, nu]`` (MATLAB ``[nu noViews]``)."""
+    reconSize: tuple            # (nx, ny)
+    reconSpacing: tuple         # (dx, dy) mm
+    reconOffset: tuple          # (ox, oy) voxels
+    nu: int
+    du: float
+    detOffset: float            # pixels
+    SAD: float
+    ADD: float
+    SDD: float
+    betas: np.ndarray
+    flatPanel: int = 1
+
+    def __post_init__(self):
+        self.reconSize = tuple(int(v) for v in self.reconSize)
+        self.reconSpacing = tuple(float(np.float32(v)) for v in self.reconSpacing)
+        self.reconOffset = tuple(float(np.float32(v)) for v in self.reconOffset)
+        self.nu = int(self.nu)
+        self.du = float(np.float32(self.du))
+        self.detOffset = float(np.float32(self.detOffset))
+        self.betas = np.ascontiguousarray(np.asarray(self.betas, dtype=np.float64).reshape(-1))
+
+    nx = property(lambda s: s.reconSize[0])
+    ny = property(lambda s: s.reconSize[1])
+    noViews = property(lambda s: int(s.betas.size))
+
+    @property
+    def image_shape(self):
+        return (self.ny, self.nx)
+
+    @property
+    def sino_shape(self):
+        return (self.noViews, self.nu)
+
+    def scalars(self):
+        """nx, ny, dx, dy, ox, oy, nu, du, ou, sad, add, sdd, noviews (fbct_geom_mex.c order)."""
+        return (self.nx, self.ny, self.reconSpacing[0], self.reconSpacing[1], self.reconOffset[0],
+                self.reconOffset[1], self.nu, self.du, self.detOffset, float(np.float32(self.SAD)),
+                float(np.float32(self.ADD)), float(np.float32(self.SDD)), self.noViews)

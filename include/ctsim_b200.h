@@ -268,6 +268,40 @@ ctsim_status ctsim_nesterov_update(int kind, float beta, float delta, int nx, in
                                    double t, double t_next, float *d_xnew, float *d_znew, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * 2-D fan-beam distance-driven and separable-footprint pair (geom/fbct).
+ * Image float[ny][nx] (MATLAB [nx ny]), sinogram float[noviews][nu] (MATLAB [nu noViews]).
+ * ------------------------------------------------------------------------- */
+
+/* Replaces fbct_geom_mex (geom/fbct/fbct_geom_mex.c:225-278) for type "proj,dd", "proj,tf",
+ * "back,dd", "back,tf" (fbct_proj.c:153,292; fbct_back.c:80,225): host pointers, out
+ * overwritten, synchronous; false (and ctsim_last_error) on any error. */
+bool ctsim_fbct_geom(const char *type, int nx, int ny, float dx, float dy, float offset_x, float offset_y, int nu,
+                     float du, float offset_u, float sad, float add, float sdd, int noviews, const double *betas,
+                     int detector_type, const float *data, float *out);
+
+typedef struct ctsim_fan_plan ctsim_fan_plan;
+typedef struct {
+    int nx, ny;
+    float dx, dy, offset_x, offset_y;
+    int nu;
+    float du, offset_u;
+    float sad, add, sdd;
+    int noviews;
+    int detector_type; /* 1 flat, 0 curved */
+} ctsim_fan_geom;
+
+/* Device plan of a fan-beam geometry (view table on the current device; betas on the host). */
+ctsim_status ctsim_fan_plan_create(const ctsim_fan_geom *geom, const double *betas, ctsim_fan_plan **plan);
+ctsim_status ctsim_fan_plan_destroy(ctsim_fan_plan *plan);
+/* A (CTSIM_PROJ_DD / CTSIM_PROJ_TF) of views view_begin + k * view_stride, k < view_count, into
+ * d_sino[view_count][nu] (overwritten). */
+ctsim_status ctsim_fan_project(ctsim_fan_plan *plan, int method, const float *d_image, float *d_sino, int view_begin,
+                               int view_stride, int view_count, void *stream);
+/* scale * A^T (CTSIM_BACK_DD / CTSIM_BACK_TF) of d_sino[view_count][nu] into d_image (overwritten). */
+ctsim_status ctsim_fan_backproject(ctsim_fan_plan *plan, int method, const float *d_sino, float *d_image,
+                                   int view_begin, int view_stride, int view_count, float scale, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Sinogram pre-processing (the data step in front of the projectors).
  * ------------------------------------------------------------------------- */
 

@@ -132,3 +132,49 @@ def ref3_cbct(kind: str, geom, data) -> np.ndarray:
     if not lib.ref3_cbct_call(KINDS[kind], *args):
         raise RuntimeError("reference call failed")
     return out
+
+
+FBCT_ORACLE_SO = os.path.join(HERE, "_build", "libfbct_oracle.so")
+FBCT_REF_SO = os.path.join(HERE, "_ref", "libfbct_ref.so")
+FAN_KINDS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3}
+_FAN_ARGS = [_i, _i, _f, _f, _f, _f, _i, _f, _f, _f, _f, _f, _i, _p, _i, _p, _p]
+
+
+def _fan_call(path, fn_name, kind, geom, data):
+    if kind not in FAN_KINDS:
+        raise ValueError(f"unknown fan-beam geom type {kind!r}")
+    if path not in _libs:
+        if not os.path.exists(path):
+            build()
+        lib = C.CDLL(path)
+        for n in ("fbo_proj", "fbo_back", "ref_fbct_call"):
+            if hasattr(lib, n):
+                getattr(lib, n).argtypes = [_i] + _FAN_ARGS
+                getattr(lib, n).restype = _i
+        _libs[path] = lib
+    lib = _libs[path]
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    proj = kind.startswith("proj")
+    if data.shape != (geom.image_shape if proj else geom.sino_shape):
+        raise ValueError("data has the wrong shape")
+    out = np.zeros(geom.sino_shape if proj else geom.image_shape, dtype=np.float32)
+    betas = np.ascontiguousarray(geom.betas, dtype=np.float64)
+    args = tuple(geom.scalars()) + (betas.ctypes.data, int(geom.flatPanel), data.ctypes.data, out.ctypes.data)
+    k = FAN_KINDS[kind]
+    if fn_name == "ref_fbct_call":
+        ok = lib.ref_fbct_call(k, *args)
+    else:
+        ok = (lib.fbo_proj if proj else lib.fbo_back)(k & 1, *args)
+    if not ok:
+        raise RuntimeError("fan-beam call failed")
+    return out
+
+
+def oracle_fbct(kind: str, geom, data) -> np.ndarray:
+    """This project's restatement of the geom/fbct DD/SF pair (bit-exact FP32)."""
+    return _fan_call(FBCT_ORACLE_SO, "fbo", kind, geom, data)
+
+
+def ref_fbct(kind: str, geom, data) -> np.ndarray:
+    """The reference's own geom/fbct C (needs _ref/libfbct_ref.so)."""
+    return _fan_call(FBCT_REF_SO, "ref_fbct_call", kind, geom, data)

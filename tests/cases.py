@@ -57,6 +57,26 @@ def make_arc_cases():
 ARC_KINDS = ("proj,dd", "back,dd")
 
 
+def make_fan_cases():
+    """2-D fan-beam geometries (geom/fbct): flat and curved detectors, offsets, a truncated
+    detector and footprints several bins wide (the 2-D code has no footprint-width limit)."""
+    from ctsim_b200.geometry import FanGeometry
+    rng = np.random.default_rng(20261205)
+    return {
+        "fan_basic": FanGeometry((32, 28), (1.0, 1.0), (0, 0), 64, 1.2, 0.0, 1000.0, 500.0, 1500.0,
+                                 circular_betas(17)),
+        "fan_offsets_curved": FanGeometry((30, 34), (0.7, 0.9), (0.4, -0.3), 50, 1.6, 2.5, 900.0, 600.0, 1500.0,
+                                          np.sort(rng.uniform(0, 2 * np.pi, 13)), 0),
+        "fan_wide": FanGeometry((16, 16), (2.0, 2.0), (0, 0), 90, 0.5, -3.0, 1000.0, 500.0, 1500.0,
+                                circular_betas(9)),
+        "fan_truncated": FanGeometry((40, 40), (1.0, 1.0), (0, 0), 24, 1.6, 4.0, 1000.0, 500.0, 1500.0,
+                                     circular_betas(10)),
+    }
+
+
+FAN_KINDS = ("proj,dd", "proj,tf", "back,dd", "back,tf")
+
+
 def case_inputs(geom, seed=0):
     """Seeded non-negative image (with exact zeros) and sinogram for a case."""
     rng = np.random.default_rng(seed)

@@ -20,8 +20,9 @@ ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
-from cases import ARC_KINDS, KINDS, case_inputs, make_arc_cases, make_cases  # noqa: E402
-from oracle.bindings import build, ref3_cbct, ref_available, ref_cbct  # noqa: E402
+from cases import (ARC_KINDS, FAN_KINDS, KINDS, case_inputs, make_arc_cases, make_cases,  # noqa: E402
+                   make_fan_cases)
+from oracle.bindings import build, ref3_cbct, ref_available, ref_cbct, ref_fbct  # noqa: E402
 
 
 def main():
@@ -47,5 +48,18 @@ def main():
         print(path, os.path.getsize(path))
 
 
+def fan_main():
+    """The 2-D fan-beam pair (geom/fbct/fbct_proj.c, fbct_back.c through ref_shim_fbct.c)."""
+    for name, g in make_fan_cases().items():
+        x, y = case_inputs(g)
+        out = {"image_in": x, "sino_in": y, "betas": g.betas}
+        for k in FAN_KINDS:
+            out[k.replace(",", "_")] = ref_fbct(k, g, x if k.startswith("proj") else y)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(path, os.path.getsize(path))
+
+
 if __name__ == "__main__":
     main()
+    fan_main()

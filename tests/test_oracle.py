@@ -12,12 +12,13 @@ import os
 import numpy as np
 import pytest
 
-from cases import ARC_KINDS, KINDS, case_inputs, make_arc_cases, make_cases
+from cases import ARC_KINDS, FAN_KINDS, KINDS, case_inputs, make_arc_cases, make_cases, make_fan_cases
 from oracle.bindings import oracle_cbct, ref_available, ref_cbct
 
 GOLDEN_DIR = os.path.join(os.path.dirname(__file__), "golden")
-# the arc-detector fixtures (DD only) are checked on their own below
-GOLDEN = sorted(p for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")) if not os.path.basename(p).startswith("arc_"))
+# the arc-detector (DD only) and fan-beam fixtures are checked on their own below
+GOLDEN = sorted(p for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))
+                if not os.path.basename(p).startswith(("arc_", "fan_")))
 CASES = make_cases()
 
 
@@ -93,3 +94,14 @@ def test_oracle_arc_detector_matches_reference(name):
     lhs = float(np.sum(oracle_cbct("proj,dd", g, x).astype(np.float64) * y))
     rhs = float(np.sum(x.astype(np.float64) * oracle_cbct("back,dd", g, y)))
     assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
+
+
+@pytest.mark.parametrize("name", sorted(make_fan_cases()))
+def test_oracle_fan_beam_matches_reference(name):
+    """The 2-D fan-beam DD/SF pair against the reference's geom/fbct fixtures: bit-exact."""
+    from oracle.bindings import oracle_fbct
+    g = make_fan_cases()[name]
+    d = np.load(os.path.join(GOLDEN_DIR, f"{name}.npz"))
+    for k in FAN_KINDS:
+        src = d["image_in"] if k.startswith("proj") else d["sino_in"]
+        assert np.array_equal(oracle_fbct(k, g, src), d[k.replace(",", "_")]), k
