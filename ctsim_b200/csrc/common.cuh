@@ -143,7 +143,7 @@ __device__ __forceinline__ ColumnFP column_footprint(const Geom &g, const View &
         } else {
             c.ampu = fdiv(fdiv(g.dx, sin_phi), 10.0f);
             umin = u_of(g, fadd(tproj0, v.dy_sin_2), fadd(dsxy0, v.n_dy_cos_2));
-            // the arc code takes this edge from the x offsets (cbct_proj3.c:351, cbct_back3.c:300)
+            // the arc code takes this edge from the x offsets (cbct_proj3.c:352, cbct_back3.c:299)
             umax = g.det == 2 ? u_of(g, fsub(tproj0, v.dx_cos_2), fsub(dsxy0, v.dx_sin_2))
                               : u_of(g, fsub(tproj0, v.dy_sin_2), fsub(dsxy0, v.n_dy_cos_2));
         }

@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(256) fan_back_kernel(FanGeom g, const FanView 
             }
             img = fadd(img, fmul(amp, temp));
         } else {
-            // iumin = max(floorf(t0 + 0.5), 0), iumax = min(ceilf(t3 + 0.5), nu - 1), fbct_back.c:348-349
+            // iumin = max(floorf(t0 + 0.5), 0), iumax = min(ceilf(t3 + 0.5), nu - 1), fbct_back.c:345-346
             const int lo = max((int)floorf((float)__dadd_rn((double)t[0], 0.5)), 0);
             const int hi = min((int)ceilf((float)__dadd_rn((double)t[3], 0.5)), g.nu - 1);
             if (lo > hi) continue;

@@ -180,7 +180,7 @@ static void orc_column_dd(const orc_geom *g, const orc_view *v, int ix, int iy, 
     } else {
         c->ampu = (real)((double)(g->dx / sin_phi) / 10.0);
         umin = orc_u_of(g, tproj0 + v->dy_sin_2, dsxy0 + v->n_dy_cos_2);
-        if (g->detector_type == 2) /* the arc code takes this edge from the x offsets, cbct_proj3.c:351 */
+        if (g->detector_type == 2) /* the arc code takes this edge from the x offsets, cbct_proj3.c:352 */
             umax = orc_u_of(g, tproj0 - v->dx_cos_2, dsxy0 - v->dx_sin_2);
         else
             umax = orc_u_of(g, tproj0 - v->dy_sin_2, dsxy0 - v->n_dy_cos_2);

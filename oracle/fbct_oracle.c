@@ -194,7 +194,7 @@ int fbo_back(int kind, int nx, int ny, float dx, float dy, float ox, float oy, i
                     }
                     image[iy * nx + ix] = image[iy * nx + ix] + amp * temp;
                 } else {
-                    /* iumin = max(floorf(t0 + 0.5), 0), iumax = min(ceilf(t3 + 0.5), nu - 1), fbct_back.c:348-349 */
+                    /* iumin = max(floorf(t0 + 0.5), 0), iumax = min(ceilf(t3 + 0.5), nu - 1), fbct_back.c:345-346 */
                     int lo = (int)floorf((float)((double)t[0] + 0.5));
                     if (lo < 0) lo = 0;
                     int hi = (int)ceilf((float)((double)t[3] + 0.5));
