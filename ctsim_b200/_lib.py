@@ -28,7 +28,8 @@ EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd
             "ctsim_pwls_residual_ex", "ctsim_fdk_filter_ex", "ctsim_fdk_run_ex",
             "ctsim_plan_create_async", "ctsim_pool_trim", "ctsim_nesterov_update",
             "ctsim_simulate_counts", "ctsim_log_attenuation", "ctsim_fbct_geom", "ctsim_fan_plan_create",
-            "ctsim_fan_plan_destroy", "ctsim_fan_project", "ctsim_fan_backproject"]
+            "ctsim_fan_plan_destroy", "ctsim_fan_project", "ctsim_fan_backproject",
+            "ctsim_plan_get_tuning", "ctsim_plan_set_tuning", "ctsim_plan_autotune", "ctsim_autotune_clear"]
 
 
 class CtsimGeom(C.Structure):
@@ -42,6 +43,10 @@ class CtsimFanGeom(C.Structure):
     _fields_ = [("nx", _i), ("ny", _i), ("dx", _f), ("dy", _f), ("offset_x", _f), ("offset_y", _f), ("nu", _i),
                 ("du", _f), ("offset_u", _f), ("sad", _f), ("add", _f), ("sdd", _f), ("noviews", _i),
                 ("detector_type", _i)]
+
+
+class CtsimTuning(C.Structure):
+    _fields_ = [("proj_groups", _i), ("back_mz", _i), ("pd_mz", _i), ("back_mz_tf", _i)]
 
 
 class CtsimError(RuntimeError):
@@ -89,6 +94,14 @@ def load():
     L.ctsim_nesterov_update.argtypes = [_i, _f, _f, _i, _i, _i, _p, _p, _p, _p, _p, C.c_double, C.c_double, _p,
                                         _p, _p]
     L.ctsim_nesterov_update.restype = _i
+    L.ctsim_plan_get_tuning.argtypes = [_p, C.POINTER(CtsimTuning)]
+    L.ctsim_plan_get_tuning.restype = _i
+    L.ctsim_plan_set_tuning.argtypes = [_p, C.POINTER(CtsimTuning)]
+    L.ctsim_plan_set_tuning.restype = _i
+    L.ctsim_plan_autotune.argtypes = [_p, _i, _i, _p, C.POINTER(CtsimTuning)]
+    L.ctsim_plan_autotune.restype = _i
+    L.ctsim_autotune_clear.argtypes = []
+    L.ctsim_autotune_clear.restype = _i
     L.ctsim_fbct_geom.argtypes = [C.c_char_p, _i, _i, _f, _f, _f, _f, _i, _f, _f, _f, _f, _f, _i, _p, _i, _p, _p]
     L.ctsim_fbct_geom.restype = C.c_bool
     L.ctsim_fan_plan_create.argtypes = [C.POINTER(CtsimFanGeom), _p, C.POINTER(_p)]

@@ -64,7 +64,9 @@ struct ctsim_plan {
     size_t bytes = 0;
     float margin = 0.f;      // candidate window margin of the forward projector (pixels)
     float zinc_max = 0.f;    // upper bound of a voxel's height in detector rows
-    int back_mz = 1, back_qcap = 0, pd_mz = 1;
+    int back_mz = 1, back_qcap = 0, pd_mz = 1;  // A^T (DD) and FDK z-pass depths (tunable)
+    int back_mz_tf = 1, back_qcap_tf = 0;       // A^T (SF) z-pass depth (tunable)
+    int fwd_groups = 1;      // candidate groups of the forward projector (tunable)
     bool fwd_ok = true;
     std::string fwd_reason;
     std::vector<double> betas;  // host copy of the view angles (FDK weights need them)
@@ -144,6 +146,14 @@ static void free_plan(ctsim_plan *p) {
 
 static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, const float *couchz, const bool *map,
                                 bool stream_ordered, cudaStream_t stream, ctsim_plan **out);
+
+// Rows of one A^T z pass of 32*mz voxels (+2 partial rows, +3 for the 4-row alignment),
+// rounded to the 128-row passes of the row buffer.
+static int back_qcap_for(const ctsim_plan *p, int mz) {
+    const int rows = std::min(p->geom.nv, (int)std::ceil(32.0 * mz * p->zinc_max) + 2) + 4;
+    return (rows + 127) / 128 * 128;
+}
+static bool back_mz_fits(const ctsim_plan *p, int mz) { return back_smem_bytes(back_qcap_for(p, mz)) <= 200 * 1024; }
 
 extern "C" ctsim_status ctsim_plan_create(const ctsim_geom *geom, const double *betas, const float *couchz,
                                           const bool *map, ctsim_plan **out) {
@@ -306,23 +316,20 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
         p->fwd_ok = false;
         p->fwd_reason = "forward projection supports nx, ny <= 2048";
     }
-    if (proj_smem_bytes(G.nv, G.nx, G.ny) > 200 * 1024) {
+    p->fwd_groups = proj_default_groups(G.nv);
+    if (proj_smem_bytes(G.nv, G.nx, G.ny, p->fwd_groups) > 200 * 1024) {
         p->fwd_ok = false;
         p->fwd_reason = "forward projection supports nv <= 6080";
     }
     // A^T: z pass of 32*MZ voxels and the per-warp row buffer that covers its shadow
     {
         int mz = std::min(8, pow2_at_least((G.nz + 31) / 32));
-        int qcap = 0;
-        for (;; mz >>= 1) {
-            // rows of one z pass (+2 partial rows, +3 for the 4-row alignment), in 128-row passes
-            const int rows = std::min(G.nv, (int)std::ceil(32.0 * mz * p->zinc_max) + 2) + 4;
-            qcap = (rows + 127) / 128 * 128;
-            if (back_smem_bytes(qcap) <= 200 * 1024 || mz == 1) break;
-        }
-        p->back_mz = mz;
-        p->back_qcap = qcap;
-        p->pd_mz = std::min(8, pow2_at_least((G.nz + 31) / 32));
+        while (mz > 1 && !back_mz_fits(p, mz)) mz >>= 1;
+        p->back_mz = p->back_mz_tf = mz;
+        p->back_qcap = p->back_qcap_tf = back_qcap_for(p, mz);
+        // FDK: one z block of 32 voxels per lane measured fastest on B200 (config 2:
+        // 124 ms against 179 ms for eight)
+        p->pd_mz = 1;
     }
 
     // device allocations
@@ -388,7 +395,7 @@ extern "C" ctsim_status ctsim_plan_project_ex(ctsim_plan *p, int method, const v
     const int nxy = p->g.nx * p->g.ny;
     cudaError_t e = launch_prefix(d_image, image_dtype, p->d_xs, nxy, p->g.nz, st);
     if (e != cudaSuccess) return cuda_fail(e, "prefix kernel");
-    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
+    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->fwd_groups, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
                     proj_dtype, view_begin, view_stride, view_count, p->margin, st);
     if (e != cudaSuccess) return cuda_fail(e, "forward projection kernel");
     return CTSIM_OK;
@@ -417,8 +424,10 @@ extern "C" ctsim_status ctsim_plan_backproject_ex(ctsim_plan *p, int method, con
         if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
         e = launch_prescale(d_proj, proj_dtype, p->d_ampv, p->d_ps, nuv, nuv * view_count, st);
         if (e != cudaSuccess) return cuda_fail(e, "prescale kernel");
-        e = launch_back(method == CTSIM_BACK_DD ? kDD : kTF, p->back_mz, p->g, p->d_views, p->d_ps, p->d_map,
-                        d_image, image_dtype, view_begin, view_stride, view_count, scale, p->back_qcap, p->d_err, st);
+        const bool dd = method == CTSIM_BACK_DD;
+        e = launch_back(dd ? kDD : kTF, dd ? p->back_mz : p->back_mz_tf, p->g, p->d_views, p->d_ps, p->d_map,
+                        d_image, image_dtype, view_begin, view_stride, view_count, scale,
+                        dd ? p->back_qcap : p->back_qcap_tf, p->d_err, st);
         break;
     }
     case CTSIM_BACK_PD:
@@ -568,4 +577,151 @@ extern "C" bool ctsim_cbct_geom(const char *type, CTSIM_GEOM_PARAMS, const float
         return false;
     }
     return run_host(method, CTSIM_GEOM_VALUES, betas, couchz, map, data, out);
+}
+
+// ---------------------------------------------------------------------------
+// Tuning: the forward projector's candidate groups, the A^T and FDK z-pass depths.
+// ---------------------------------------------------------------------------
+extern "C" ctsim_status ctsim_plan_get_tuning(const ctsim_plan *p, ctsim_tuning *t) {
+    if (!p || !t) return fail(CTSIM_ERR_ARGUMENT, "null argument");
+    t->proj_groups = p->fwd_groups;
+    t->back_mz = p->back_mz;
+    t->back_mz_tf = p->back_mz_tf;
+    t->pd_mz = p->pd_mz;
+    return CTSIM_OK;
+}
+
+static bool mz_valid(int mz) { return mz == 1 || mz == 2 || mz == 4 || mz == 8; }
+
+extern "C" ctsim_status ctsim_plan_set_tuning(ctsim_plan *p, const ctsim_tuning *t) {
+    if (!p || !t) return fail(CTSIM_ERR_ARGUMENT, "null argument");
+    if (t->proj_groups && (!proj_groups_valid(p->geom.nv, t->proj_groups) ||
+                           proj_smem_bytes(p->geom.nv, p->geom.nx, p->geom.ny, t->proj_groups) > 200 * 1024))
+        return fail(CTSIM_ERR_ARGUMENT, "proj_groups must be 1, 2, 4 or 8 with groups * row threads <= 256");
+    if ((t->back_mz && (!mz_valid(t->back_mz) || !back_mz_fits(p, t->back_mz))) ||
+        (t->back_mz_tf && (!mz_valid(t->back_mz_tf) || !back_mz_fits(p, t->back_mz_tf))))
+        return fail(CTSIM_ERR_ARGUMENT, "back_mz must be 1, 2, 4 or 8 and fit the row buffer");
+    if (t->pd_mz && !mz_valid(t->pd_mz)) return fail(CTSIM_ERR_ARGUMENT, "pd_mz must be 1, 2, 4 or 8");
+    if (t->proj_groups) p->fwd_groups = t->proj_groups;
+    if (t->back_mz) {
+        p->back_mz = t->back_mz;
+        p->back_qcap = back_qcap_for(p, t->back_mz);
+    }
+    if (t->back_mz_tf) {
+        p->back_mz_tf = t->back_mz_tf;
+        p->back_qcap_tf = back_qcap_for(p, t->back_mz_tf);
+    }
+    if (t->pd_mz) p->pd_mz = t->pd_mz;
+    return CTSIM_OK;
+}
+
+namespace {
+// Choices measured in this process, by shape class: method, the forward projector's row
+// threads (a function of nv), the z passes, the volume and detector sizes.
+std::mutex g_tune_mutex;
+std::map<std::vector<int>, int> g_tuned;
+}  // namespace
+
+// The tuning field a method's launch shape lives in.
+static int &tuning_field(ctsim_tuning &t, int method) {
+    switch (method) {
+    case CTSIM_PROJ_DD:
+    case CTSIM_PROJ_TF: return t.proj_groups;
+    case CTSIM_BACK_DD: return t.back_mz;
+    case CTSIM_BACK_TF: return t.back_mz_tf;
+    default: return t.pd_mz;
+    }
+}
+
+extern "C" ctsim_status ctsim_autotune_clear(void) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tuned.clear();
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sample_views, void *stream,
+                                            ctsim_tuning *chosen) {
+    if (!p) return fail(CTSIM_ERR_ARGUMENT, "null plan");
+    if (method < CTSIM_PROJ_DD || method > CTSIM_BACK_VAR) return fail(CTSIM_ERR_ARGUMENT, "unknown method");
+    const bool fwd = method == CTSIM_PROJ_DD || method == CTSIM_PROJ_TF;
+    const bool vox = method >= CTSIM_BACK_PD;
+    if ((fwd || !vox) && !p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
+    const ctsim_geom &G = p->geom;
+    const std::vector<int> key = {method, G.nx, G.ny, G.nz, G.nu, G.nv, G.detector_type};
+    int best = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) best = it->second;
+    }
+    if (!best) {
+        std::vector<int> cand;
+        for (int c : {1, 2, 4, 8}) {
+            if (fwd ? (proj_groups_valid(G.nv, c) && proj_smem_bytes(G.nv, G.nx, G.ny, c) <= 200 * 1024)
+                    : vox ? true : back_mz_fits(p, c))
+                cand.push_back(c);
+        }
+        // the launch shape that wins depends on the grid, so the sample should be the size
+        // of the real launches (an OS-PWLS subset, or all views); default: up to 64 views
+        if (sample_views < 1) sample_views = 64;
+        const int count = std::min(sample_views, G.noviews);
+        const int stride = std::max(1, G.noviews / count);
+        cudaStream_t st = (cudaStream_t)stream;
+        const size_t nimg = (size_t)G.nx * G.ny * G.nz, nsino = (size_t)count * G.nu * G.nv;
+        void *img = nullptr, *sino = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaError_t e;
+        // the plan's own allocation mode; the buffers are freed before returning
+        if ((e = ctsim_plan_alloc(p, &img, nimg * 4)) != cudaSuccess ||
+            (e = ctsim_plan_alloc(p, &sino, nsino * 4)) != cudaSuccess) {
+            ctsim_plan_release(p, img);
+            return fail(CTSIM_ERR_ALLOC, std::string("autotune buffers: ") + cudaGetErrorString(e));
+        }
+        const ctsim_tuning saved = {p->fwd_groups, p->back_mz, p->pd_mz, p->back_mz_tf};
+        float best_ms = 0.f;
+        ctsim_status s = CTSIM_OK;
+        if ((e = cudaMemsetAsync(img, 0, nimg * 4, st)) != cudaSuccess ||
+            (e = cudaMemsetAsync(sino, 0, nsino * 4, st)) != cudaSuccess || (e = cudaEventCreate(&e0)) != cudaSuccess ||
+            (e = cudaEventCreate(&e1)) != cudaSuccess) {
+            s = cuda_fail(e, "autotune set-up");
+        }
+        for (size_t i = 0; s == CTSIM_OK && i < cand.size(); i++) {
+            ctsim_tuning t = {0, 0, 0, 0};
+            tuning_field(t, method) = cand[i];
+            if ((s = ctsim_plan_set_tuning(p, &t)) != CTSIM_OK) break;
+            float ms = 0.f;
+            for (int rep = 0; rep < 3 && s == CTSIM_OK; rep++) {  // one warm-up, then the faster of two
+                cudaEventRecord(e0, st);
+                s = fwd ? ctsim_plan_project(p, method, (const float *)img, (float *)sino, 0, stride, count, stream)
+                        : ctsim_plan_backproject(p, method, (const float *)sino, (float *)img, 0, stride, count, 1.0f,
+                                                 stream);
+                cudaEventRecord(e1, st);
+                if (s != CTSIM_OK) break;
+                if ((e = cudaEventSynchronize(e1)) != cudaSuccess) {
+                    s = cuda_fail(e, "autotune timing");
+                    break;
+                }
+                float t_ms = 0.f;
+                cudaEventElapsedTime(&t_ms, e0, e1);
+                if (rep == 1 || (rep == 2 && t_ms < ms)) ms = t_ms;
+            }
+            if (s == CTSIM_OK && (best == 0 || ms < best_ms)) {
+                best = cand[i];
+                best_ms = ms;
+            }
+        }
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        ctsim_plan_release(p, img);
+        ctsim_plan_release(p, sino);
+        ctsim_plan_set_tuning(p, &saved);
+        if (s != CTSIM_OK) return s;
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tuned[key] = best;
+    }
+    ctsim_tuning t = {0, 0, 0, 0};
+    tuning_field(t, method) = best;
+    ctsim_status s = ctsim_plan_set_tuning(p, &t);
+    if (s == CTSIM_OK && chosen) ctsim_plan_get_tuning(p, chosen);
+    return s;
 }

@@ -656,42 +656,44 @@ cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, i
 }
 
 // Row threads R (one per 4 detector rows, whole warps, at most kProjMaxThreads) and
-// candidate groups: short detectors (R <= 64, up to 256 rows) fill the block with
-// groups; taller ones keep one group (measured: two groups of 3 warps at 384 rows are
-// slower than one).
+// candidate groups (1, 2, 4 or 8, with R * groups <= kProjMaxThreads).  Default: two
+// groups wherever they fit (R <= 128, up to 512 rows) -- the fastest count on every
+// shape measured on B200 (nv 72..384); one group above.  A plan's autotuner may pick
+// another valid count.
 static int proj_row_threads(int nv) {
     return std::min(kProjMaxThreads, std::max(32, ((nv + 3) / 4 + 31) / 32 * 32));
 }
-static int proj_groups(int nv) {
-    const int R = proj_row_threads(nv);
-    return R <= 64 ? kProjMaxThreads / R : 1;
+int proj_default_groups(int nv) { return proj_row_threads(nv) <= kProjMaxThreads / 2 ? 2 : 1; }
+bool proj_groups_valid(int nv, int groups) {
+    return (groups == 1 || groups == 2 || groups == 4 || groups == 8) &&
+           proj_row_threads(nv) * groups <= kProjMaxThreads;
 }
-size_t proj_smem_bytes(int nv, int nx, int ny) {
-    const int R = proj_row_threads(nv), G = proj_groups(nv);
-    ProjSmem L{(nv + 3) / 4, R * G, std::max(nx, ny), G};
+size_t proj_smem_bytes(int nv, int nx, int ny, int groups) {
+    const int R = proj_row_threads(nv);
+    ProjSmem L{(nv + 3) / 4, R * groups, std::max(nx, ny), groups};
     return L.bytes();
 }
 int proj_group_width() { return kTU; }
 int proj_max_lines() { return kMaxLines; }
 
-cudaError_t launch_proj(int method, const Geom &g, const View *views, const float *xc, const float *ampv,
-                        const uint8_t *map, void *proj, int out_dtype, int vb, int vs, int vc, float margin,
-                        cudaStream_t st) {
-    const size_t sm = proj_smem_bytes(g.nv, g.nx, g.ny);
+cudaError_t launch_proj(int method, int groups, const Geom &g, const View *views, const float *xc,
+                        const float *ampv, const uint8_t *map, void *proj, int out_dtype, int vb, int vs, int vc,
+                        float margin, cudaStream_t st) {
+    if (!proj_groups_valid(g.nv, groups)) return cudaErrorInvalidValue;
+    const size_t sm = proj_smem_bytes(g.nv, g.nx, g.ny, groups);
     dim3 grid((g.nu + kTU - 1) / kTU, vc);
     // one thread per 4 detector rows (up to 256 threads per group, more rows loop),
     // groups of those threads share the candidates
-    const int G = proj_groups(g.nv);
-    const int nt = proj_row_threads(g.nv) * G;
+    const int nt = proj_row_threads(g.nv) * groups;
 #define CTSIM_PROJ_CASE(M, GR)                                                                        \
-    if (method == M && G == GR) {                                                                     \
+    if (method == M && groups == GR) {                                                                \
         cudaError_t e = allow_dynamic_smem((const void *)proj_kernel<M, GR>, sm);                     \
         if (e != cudaSuccess) return e;                                                               \
         proj_kernel<M, GR><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin); \
         return cudaGetLastError();                                                                    \
     }
-    CTSIM_PROJ_CASE(kDD, 1) CTSIM_PROJ_CASE(kDD, 4) CTSIM_PROJ_CASE(kDD, 8)
-    CTSIM_PROJ_CASE(kTF, 1) CTSIM_PROJ_CASE(kTF, 4) CTSIM_PROJ_CASE(kTF, 8)
+    CTSIM_PROJ_CASE(kDD, 1) CTSIM_PROJ_CASE(kDD, 2) CTSIM_PROJ_CASE(kDD, 4) CTSIM_PROJ_CASE(kDD, 8)
+    CTSIM_PROJ_CASE(kTF, 1) CTSIM_PROJ_CASE(kTF, 2) CTSIM_PROJ_CASE(kTF, 4) CTSIM_PROJ_CASE(kTF, 8)
 #undef CTSIM_PROJ_CASE
     return cudaErrorInvalidValue;
 }

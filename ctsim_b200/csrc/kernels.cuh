@@ -24,9 +24,11 @@ cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const
 
 cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, cudaStream_t st);
 
-cudaError_t launch_proj(int method, const Geom &g, const View *views, const float *xs, const float *ampv,
-                        const uint8_t *map, void *proj, int out_dtype, int view_begin, int view_stride,
-                        int view_count, float margin, cudaStream_t st);
+cudaError_t launch_proj(int method, int groups, const Geom &g, const View *views, const float *xs,
+                        const float *ampv, const uint8_t *map, void *proj, int out_dtype, int view_begin,
+                        int view_stride, int view_count, float margin, cudaStream_t st);
+int proj_default_groups(int nv);
+bool proj_groups_valid(int nv, int groups);
 
 // voxel-driven bilinear modes: back,pd (v outside the detector skipped), back,hpd (v
 // clamped), back,var (geom/cbct/cbct_back_var.c)
@@ -40,7 +42,7 @@ cudaError_t launch_scale(float *y, size_t n, float s, cudaStream_t st);
 // Raises (never lowers) a kernel's dynamic shared-memory limit on the current device.
 cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes);
 
-size_t proj_smem_bytes(int nv, int nx, int ny);
+size_t proj_smem_bytes(int nv, int nx, int ny, int groups);
 int proj_group_width();
 int proj_max_lines();
 

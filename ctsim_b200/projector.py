@@ -162,6 +162,30 @@ class Plan:
         self._L = L
 
     @property
+    def tuning(self) -> dict:
+        """Launch shapes: forward candidate groups, A^T and FDK z-pass depths."""
+        t = _lib.CtsimTuning()
+        _lib.check(self._L.ctsim_plan_get_tuning(self._h, C.byref(t)), "ctsim_plan_get_tuning")
+        return {"proj_groups": t.proj_groups, "back_mz": t.back_mz, "back_mz_tf": t.back_mz_tf, "pd_mz": t.pd_mz}
+
+    def set_tuning(self, proj_groups: int = 0, back_mz: int = 0, pd_mz: int = 0, back_mz_tf: int = 0):
+        t = _lib.CtsimTuning(int(proj_groups), int(back_mz), int(pd_mz), int(back_mz_tf))
+        _lib.check(self._L.ctsim_plan_set_tuning(self._h, C.byref(t)), "ctsim_plan_set_tuning")
+
+    def autotune(self, method: str, sample_views: int = 0) -> dict:
+        """Time every valid launch shape of ``method`` on a sample of views and keep the
+        fastest (recorded per shape class for the process); synchronises the stream."""
+        torch = _torch()
+        m = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3, "back,pd": 4, "back,hpd": 5,
+             "back,var": 6}[method]
+        t = _lib.CtsimTuning()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        with torch.cuda.device(self.device):
+            _lib.check(self._L.ctsim_plan_autotune(self._h, m, int(sample_views), st, C.byref(t)),
+                       "ctsim_plan_autotune")
+        return {"proj_groups": t.proj_groups, "back_mz": t.back_mz, "back_mz_tf": t.back_mz_tf, "pd_mz": t.pd_mz}
+
+    @property
     def device_bytes(self) -> int:
         return int(self._L.ctsim_plan_device_bytes(self._h))
 

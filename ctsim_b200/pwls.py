@@ -91,7 +91,7 @@ class PwlsSolver:
     """
 
     def __init__(self, y, w, geom: CTGeometry, beta: float, pfun: str = "huber", delta: float = 0.001,
-                 numos: int = 1, img0=None, method: str = "tf", storage=None, plan=None):
+                 numos: int = 1, img0=None, method: str = "tf", storage=None, plan=None, autotune: bool = False):
         torch = _torch()
         if pfun.lower() not in PENALTIES:
             raise ValueError("unknow penalty function")
@@ -99,6 +99,10 @@ class PwlsSolver:
         self.kind = PENALTIES[pfun.lower()]
         self.method = method
         self.plan = plan if plan is not None else plan_for(geom, y.device)
+        if autotune:  # launch shapes timed on subset-sized launches (recorded per shape class)
+            sub = max(1, -(-geom.noViews // self.M))
+            self.plan.autotune(f"proj,{method}", sub)
+            self.plan.autotune(f"back,{method}", sub)
         self.dev = self.plan.device
         self.L = _lib.load()
         # the measured data (y, w: the largest arrays) may be stored in bfloat16 or float16;

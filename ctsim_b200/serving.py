@@ -93,7 +93,7 @@ def hbm_footprint(req: ReconRequest) -> int:
 class _Active:
     """Device state and work of one admitted request (runs on its slot's stream)."""
 
-    def __init__(self, req: ReconRequest, stream, device, graphs: bool = True):
+    def __init__(self, req: ReconRequest, stream, device, graphs: bool = True, autotune: bool = False):
         import torch
         from .fdk import FDK
         from .projector import Plan
@@ -118,7 +118,7 @@ class _Active:
                 w = _to_device(req.weights, device)
                 x0 = self.fdk(sino.float().contiguous())  # reconFDK start image
                 self.solver = PwlsSolver(sino, w, req.geom, req.beta, req.pfun, req.delta, req.subsets, x0,
-                                         storage=dt, plan=self.plan)
+                                         storage=dt, plan=self.plan, autotune=autotune)
                 self.fdk.close()
                 self.fdk = None
                 self.units = req.iterations
@@ -205,7 +205,7 @@ class ReconServer:
 
     def __init__(self, hbm_budget: int = 150 * 2 ** 30, max_active: int = 8, depth: int = 2, device=None,
                  graphs: bool = True, activate: Optional[Callable] = None, clock: Optional[Callable] = None,
-                 to_host: bool = False, admit_workers: int = 0):
+                 to_host: bool = False, admit_workers: int = 0, autotune: bool = False):
         self.budget = int(hbm_budget)
         self.max_active = int(max_active)
         self.depth = int(depth)
@@ -228,7 +228,7 @@ class ReconServer:
             self.device = torch.device("cuda", torch.cuda.current_device() if device is None else
                                        (torch.device(device).index or 0))
             self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.max_active)]
-            activate = lambda req, slot: _Active(req, self.streams[slot], self.device, self.graphs)
+            activate = lambda req, slot: _Active(req, self.streams[slot], self.device, self.graphs, autotune)
         else:
             self.streams = [None] * self.max_active
         self._activate = activate

@@ -160,6 +160,31 @@ ctsim_status ctsim_plan_create_async(const ctsim_geom *geom, const double *betas
  * at least keep_bytes. */
 ctsim_status ctsim_pool_trim(size_t keep_bytes);
 
+/* Launch shapes of a plan (no reference counterpart): the forward projector's
+ * candidate-parallel thread groups (1, 2, 4, 8) and the 32-voxel z blocks per lane of
+ * the A^T passes (back_mz for DD, back_mz_tf for SF) and of the FDK/var kernel (pd_mz),
+ * each 1, 2, 4 or 8.  Plans start with a size rule; set_tuning changes the non-zero
+ * fields (validated against the geometry).  The group count and the A^T z blocks change
+ * the floating-point rounding of A and A^T (the summation order and the start of the
+ * running row sums), never the footprints; the FDK/var z blocks change nothing. */
+typedef struct {
+    int proj_groups;
+    int back_mz;
+    int pd_mz;
+    int back_mz_tf;
+} ctsim_tuning;
+ctsim_status ctsim_plan_get_tuning(const ctsim_plan *plan, ctsim_tuning *tuning);
+ctsim_status ctsim_plan_set_tuning(ctsim_plan *plan, const ctsim_tuning *tuning);
+
+/* Autotuner: times every valid launch shape of `method` on sample_views evenly spaced
+ * views of the plan (<= 0: up to 64; the best shape depends on the grid, so pass the
+ * view count of the real launches) (zero data, the plan's allocation mode for two temporary buffers),
+ * keeps the fastest and records it for the shape class (method, volume and detector
+ * sizes, detector type) so later plans of the class reuse it without timing.
+ * Synchronises `stream`.  ctsim_autotune_clear forgets the recorded choices. */
+ctsim_status ctsim_plan_autotune(ctsim_plan *plan, int method, int sample_views, void *stream, ctsim_tuning *chosen);
+ctsim_status ctsim_autotune_clear(void);
+
 /* Bytes of device memory the plan holds (tables + scratch). */
 size_t ctsim_plan_device_bytes(const ctsim_plan *plan);
 

@@ -165,3 +165,37 @@ def test_helical_scan_matches_oracle():
         src = x if k.startswith("proj") else y
         err = rel_l2(mex(k, g, src), oracle_cbct(k, g, src))
         assert err <= REL_L2, f"{k}: rel L2 {err:.3e}"
+
+
+def test_launch_shapes_keep_parity_and_autotune():
+    """Every valid launch shape stays within the parity bar (the FDK kernel's z blocks are
+    bit-neutral); the autotuner picks a valid shape and records it for the shape class."""
+    import torch
+    from ctsim_b200._lib import CtsimError
+    g = CASES["ragged"]
+    x, y = case_inputs(g, seed=12)
+    xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    plan = Plan(g)
+    hpd0 = plan.backproject(yd, "hpd").cpu().numpy()
+    for G in (1, 2, 4, 8):
+        try:
+            plan.set_tuning(proj_groups=G)
+        except CtsimError:
+            continue
+        for m in ("dd", "tf"):
+            assert rel_l2(plan.project(xd, m).cpu().numpy(), oracle_cbct(f"proj,{m}", g, x)) <= REL_L2
+    for mz in (1, 2, 4, 8):
+        plan.set_tuning(pd_mz=mz)
+        assert np.array_equal(plan.backproject(yd, "hpd").cpu().numpy(), hpd0)
+        try:
+            plan.set_tuning(back_mz=mz, back_mz_tf=mz)
+        except CtsimError:
+            continue
+        for m in ("dd", "tf"):
+            assert rel_l2(plan.backproject(yd, m).cpu().numpy(), oracle_cbct(f"back,{m}", g, y)) <= REL_L2
+    with pytest.raises(CtsimError):
+        plan.set_tuning(proj_groups=3)
+    t = Plan(g).autotune("proj,tf", 4)
+    assert t["proj_groups"] in (1, 2, 4, 8)
+    t2 = Plan(g).autotune("back,tf", 4)
+    assert t2["back_mz_tf"] in (1, 2, 4, 8)
