@@ -450,6 +450,82 @@ def run_serving(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args):
+    """Batched uneven instances: OS-PWLS reconstructions of random_geometry instances
+    (volumes 128^2x64 .. 384^2x160, 180-720 views, ~20% short scan, ~20% offset detector),
+    10 iterations x 12 subsets each, Huber and quadratic penalties alternating, FP32.
+    Arms: every instance solved on its own, one after another (reconPwlsSeSqs's loop), and
+    all instances stepped together by BatchedPwls (one persistent A and one persistent A^T
+    launch per sub-iteration and launch-shape class, CUDA-graph iterations).  Both arms
+    start from the same FDK images and must end on identical images."""
+    import torch
+    from ctsim_b200.fdk import FDK
+    from ctsim_b200.projector import Plan
+    from ctsim_b200.pwls import BatchedPwls, PwlsSolver
+    from ctsim_b200.serving import make_requests
+    torch.cuda.set_device(0)
+    reqs = make_requests(args.instances, seed=args.seed, fdk_fraction=0.0, storage="float32", scale=args.scale)
+    solvers, starts = [], []
+    for k, r in enumerate(reqs):
+        plan = Plan(r.geom)
+        if args.autotune:
+            sub = -(-r.geom.noViews // 12)
+            plan.autotune("proj,tf", sub)
+            plan.autotune("back,tf", sub)
+        y = torch.from_numpy(r.sino).cuda()
+        w = torch.from_numpy(r.weights).cuda()
+        f = FDK(r.geom, "hamming", 1.0, plan=plan)
+        x0 = f(y)
+        f.close()
+        s = PwlsSolver(y, w, r.geom, 1e3 if k % 2 == 0 else 1e2, "huber" if k % 2 == 0 else "quad", 0.01, 12, x0,
+                       plan=plan)
+        solvers.append(s)
+        starts.append(x0)
+    its = 10
+
+    def reset():
+        for s, x0 in zip(solvers, starts):
+            s.x.copy_(x0)
+            s.itn = 0
+
+    vv = sum(2 * its * r.geom.nx * r.geom.ny * r.geom.nz * r.geom.noViews for r in reqs)
+    # warm-up of both arms (one iteration each)
+    for s in solvers:
+        s.step()
+    reset()
+    BatchedPwls(solvers).iteration()
+    reset()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in solvers:
+        for _ in range(its):
+            s.step()
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    seq_images = [s.x.clone() for s in solvers]
+    reset()
+    b = BatchedPwls(solvers)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(its):
+        b.iteration()
+    torch.cuda.synchronize()
+    t_bat = time.perf_counter() - t0
+    same = all(torch.equal(s.x, x) for s, x in zip(solvers, seq_images))
+    sizes = [(r.geom.nx, r.geom.nz, r.geom.noViews, r.geom.nu, r.geom.nv) for r in reqs]
+    line = {
+        "metric": "batched OS-PWLS reconstructions/s (uneven instances)", "value": len(reqs) / t_bat,
+        "unit": "instances/s", "impl": "batched", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded ellipsoid phantoms, Poisson counts)",
+        "config": {"workload": "random_geometry instances", "instances": len(reqs), "iterations": its,
+                   "subsets": 12, "scale": args.scale, "seed": args.seed, "autotune": bool(args.autotune)},
+        "sequential_instances_per_s": len(reqs) / t_seq, "speedup_vs_sequential": t_seq / t_bat,
+        "batched_s": t_bat, "sequential_s": t_seq, "gvoxel_views_per_s_batched": vv / t_bat / 1e9,
+        "identical_images": bool(same), "sizes_nx_nz_views_nu_nv": sizes,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -465,9 +541,13 @@ def main():
     ap.add_argument("--slots", type=int, default=8, help="concurrent requests of the serving run")
     ap.add_argument("--scale", type=float, default=1.0, help="size scale of the serving run's geometries")
     ap.add_argument("--seed", type=int, default=7)
-    ap.add_argument("--autotune", action="store_true", help="serving: autotune launch shapes per shape class")
+    ap.add_argument("--autotune", action="store_true", help="serving/batched: autotune launch shapes")
+    ap.add_argument("--batched", action="store_true", help="batched uneven OS-PWLS instances instead of A/A^T")
+    ap.add_argument("--instances", type=int, default=16, help="instances of the batched run")
     args = ap.parse_args()
-    if args.serving:
+    if args.batched:
+        run_batched(args)
+    elif args.serving:
         run_serving(args)
     elif args.impl == "reference":
         run_reference(args)

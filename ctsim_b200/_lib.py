@@ -29,7 +29,8 @@ EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd
             "ctsim_plan_create_async", "ctsim_pool_trim", "ctsim_nesterov_update",
             "ctsim_simulate_counts", "ctsim_log_attenuation", "ctsim_fbct_geom", "ctsim_fan_plan_create",
             "ctsim_fan_plan_destroy", "ctsim_fan_project", "ctsim_fan_backproject",
-            "ctsim_plan_get_tuning", "ctsim_plan_set_tuning", "ctsim_plan_autotune", "ctsim_autotune_clear"]
+            "ctsim_plan_get_tuning", "ctsim_plan_set_tuning", "ctsim_plan_autotune", "ctsim_autotune_clear",
+            "ctsim_batch_project", "ctsim_batch_backproject"]
 
 
 class CtsimGeom(C.Structure):
@@ -47,6 +48,11 @@ class CtsimFanGeom(C.Structure):
 
 class CtsimTuning(C.Structure):
     _fields_ = [("proj_groups", _i), ("back_mz", _i), ("pd_mz", _i), ("back_mz_tf", _i)]
+
+
+class CtsimBatchItem(C.Structure):
+    _fields_ = [("plan", _p), ("in_", _p), ("out", _p), ("view_begin", _i), ("view_stride", _i),
+                ("view_count", _i), ("scale", _f)]
 
 
 class CtsimError(RuntimeError):
@@ -102,6 +108,10 @@ def load():
     L.ctsim_plan_autotune.restype = _i
     L.ctsim_autotune_clear.argtypes = []
     L.ctsim_autotune_clear.restype = _i
+    L.ctsim_batch_project.argtypes = [_i, C.POINTER(CtsimBatchItem), _i, _p]
+    L.ctsim_batch_project.restype = _i
+    L.ctsim_batch_backproject.argtypes = [_i, C.POINTER(CtsimBatchItem), _i, _p]
+    L.ctsim_batch_backproject.restype = _i
     L.ctsim_fbct_geom.argtypes = [C.c_char_p, _i, _i, _f, _f, _f, _f, _i, _f, _f, _f, _f, _f, _i, _p, _i, _p, _p]
     L.ctsim_fbct_geom.restype = C.c_bool
     L.ctsim_fan_plan_create.argtypes = [C.POINTER(CtsimFanGeom), _p, C.POINTER(_p)]

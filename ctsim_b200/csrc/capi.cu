@@ -725,3 +725,130 @@ extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sampl
     if (s == CTSIM_OK && chosen) ctsim_plan_get_tuning(p, chosen);
     return s;
 }
+
+// ---------------------------------------------------------------------------
+// Batched launches over many plans (ctsim_batch_item).
+// ---------------------------------------------------------------------------
+static ctsim_status batch_check(int method, const ctsim_batch_item *items, int n, bool fwd) {
+    if (!items || n < 0) return fail(CTSIM_ERR_ARGUMENT, "null batch");
+    if (fwd ? (method != CTSIM_PROJ_DD && method != CTSIM_PROJ_TF) : (method != CTSIM_BACK_DD && method != CTSIM_BACK_TF))
+        return fail(CTSIM_ERR_ARGUMENT, "batched launches cover the DD and SF A / A^T");
+    int dev = -1;
+    for (int i = 0; i < n; i++) {
+        const ctsim_batch_item &it = items[i];
+        if (!it.plan || !it.in || !it.out) return fail(CTSIM_ERR_ARGUMENT, "null plan or buffer in the batch");
+        if (!it.plan->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, it.plan->fwd_reason);
+        if (it.plan->g.det == 2 && method != (fwd ? CTSIM_PROJ_DD : CTSIM_BACK_DD))
+            return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
+        if (dev >= 0 && it.plan->device != dev) return fail(CTSIM_ERR_ARGUMENT, "batch plans must share one device");
+        for (int j = 0; j < i; j++)  // each plan's scratch serves one item
+            if (items[j].plan == it.plan) return fail(CTSIM_ERR_ARGUMENT, "a plan may appear only once per batch");
+        dev = it.plan->device;
+        ctsim_status s = check_views(it.plan, it.view_begin, it.view_stride, it.view_count);
+        if (s != CTSIM_OK) return s;
+    }
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *items, int n, void *stream) {
+    ctsim_status s = batch_check(method, items, n, true);
+    if (s != CTSIM_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    // column prefix sums of every image (each plan's own scratch)
+    for (int i = 0; i < n; i++) {
+        const ctsim_plan *p = items[i].plan;
+        if ((e = launch_prefix(items[i].in, CTSIM_F32, p->d_xs, p->g.nx * p->g.ny, p->g.nz, st)) != cudaSuccess)
+            return cuda_fail(e, "prefix kernel");
+    }
+    // one persistent launch per launch-shape class (row threads, candidate groups)
+    std::map<std::pair<int, int>, std::vector<int>> classes;
+    for (int i = 0; i < n; i++) {
+        const ctsim_plan *p = items[i].plan;
+        classes[{proj_row_threads_of(p->g.nv), p->fwd_groups}].push_back(i);
+    }
+    for (auto &cl : classes) {
+        const std::vector<int> &idx = cl.second;
+        for (size_t c0 = 0; c0 < idx.size(); c0 += kBatchMax) {
+            ProjBatch b;
+            b.n = 0;
+            b.total = 0;
+            size_t smem = 0;
+            for (size_t c = c0; c < std::min(idx.size(), c0 + kBatchMax); c++) {
+                const ctsim_batch_item &it = items[idx[c]];
+                const ctsim_plan *p = it.plan;
+                ProjTask &T = b.t[b.n++];
+                T.g = p->g;
+                T.views = p->d_views;
+                T.xs = p->d_xs;
+                T.ampv = p->d_ampv;
+                T.map = p->d_map;
+                T.proj = static_cast<float *>(it.out);
+                T.vb = it.view_begin;
+                T.vs = it.view_stride;
+                T.gx = (p->g.nu + proj_group_width() - 1) / proj_group_width();
+                T.first = b.total;
+                T.margin = p->margin;
+                b.total += proj_task_blocks(p->g, it.view_count);
+                smem = std::max(smem, proj_smem_bytes(p->g.nv, p->g.nx, p->g.ny, p->fwd_groups));
+            }
+            if ((e = launch_proj_batch(method == CTSIM_PROJ_DD ? kDD : kTF, cl.first.second, cl.first.first, smem, b,
+                                       st)) != cudaSuccess)
+                return cuda_fail(e, "batched forward projection");
+        }
+    }
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_item *items, int n, void *stream) {
+    ctsim_status s = batch_check(method, items, n, false);
+    if (s != CTSIM_OK) return s;
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool dd = method == CTSIM_BACK_DD;
+    cudaError_t e;
+    for (int i = 0; i < n; i++) {  // sinograms times ampv into each plan's scratch
+        const ctsim_plan *p = items[i].plan;
+        const size_t nuv = (size_t)p->g.nu * p->g.nv;
+        if ((e = launch_prescale(items[i].in, CTSIM_F32, p->d_ampv, p->d_ps, nuv, nuv * items[i].view_count, st)) !=
+            cudaSuccess)
+            return cuda_fail(e, "prescale kernel");
+    }
+    std::map<std::pair<int, bool>, std::vector<int>> classes;  // (z blocks per lane, float4 rows)
+    for (int i = 0; i < n; i++) {
+        const ctsim_plan *p = items[i].plan;
+        const bool vec = (p->g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(p->d_ps) % 16) == 0;
+        classes[{dd ? p->back_mz : p->back_mz_tf, vec}].push_back(i);
+    }
+    for (auto &cl : classes) {
+        const std::vector<int> &idx = cl.second;
+        for (size_t c0 = 0; c0 < idx.size(); c0 += kBatchMax) {
+            BackBatch b;
+            b.n = 0;
+            b.total = 0;
+            int qcap = 0;
+            for (size_t c = c0; c < std::min(idx.size(), c0 + kBatchMax); c++) {
+                const ctsim_batch_item &it = items[idx[c]];
+                const ctsim_plan *p = it.plan;
+                BackTask &T = b.t[b.n++];
+                T.g = p->g;
+                T.views = p->d_views;
+                T.ps = p->d_ps;
+                T.map = p->d_map;
+                T.image = static_cast<float *>(it.out);
+                T.err = p->d_err;
+                T.vb = it.view_begin;
+                T.vs = it.view_stride;
+                T.vc = it.view_count;
+                T.qcap = dd ? p->back_qcap : p->back_qcap_tf;
+                T.first = b.total;
+                T.scale = it.scale;
+                b.total += back_task_blocks(p->g);
+                qcap = std::max(qcap, T.qcap);
+            }
+            if ((e = launch_back_batch(dd ? kDD : kTF, cl.first.first, cl.first.second, back_smem_bytes(qcap), b, st)) !=
+                cudaSuccess)
+                return cuda_fail(e, "batched backprojection");
+        }
+    }
+    return CTSIM_OK;
+}

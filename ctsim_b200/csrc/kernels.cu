@@ -29,20 +29,21 @@ constexpr unsigned kFull = 0xffffffffu;
 // Adjacent voxels share their common edge (warp shuffles), so each voxel costs one
 // edge evaluation.  Accumulation over views stays in registers; no atomics.
 // ---------------------------------------------------------------------------
-template <int METHOD, int MZ, bool VEC, bool PRESCALED = true>
-__global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restrict__ views,
-                                                   const float *__restrict__ ps, const uint8_t *__restrict__ map,
-                                                   void *__restrict__ image, int out_dtype, int view_begin,
-                                                   int view_stride, int view_count, float scale, int qcap,
-                                                   int *__restrict__ err, const float *__restrict__ ampv) {
-    extern __shared__ float smem[];
+// The work of one block (8 columns of one row iy), as a device function: the plain
+// kernel runs it for blockIdx.x, the batched kernel for each of its work items.
+template <int METHOD, int MZ, bool VEC, bool PRESCALED>
+__device__ __forceinline__ void back_block(const Geom g, const View *__restrict__ views, const float *__restrict__ ps,
+                                           const uint8_t *__restrict__ map, void *__restrict__ image, int out_dtype,
+                                           int view_begin, int view_stride, int view_count, float scale, int qcap,
+                                           int *__restrict__ err, const float *__restrict__ ampv, float *smem,
+                                           int block) {
     constexpr int kWS = 17;  // row stride of the per-warp weight table (conflict-free writes)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float *wtab = smem + warp * (32 * kWS + 2 * qcap);   // [32 views][17] u weights of the view chunk
     float2 *CQ = reinterpret_cast<float2 *>(wtab + 32 * kWS);  // [qcap] (running sum, q) per row
     const int tiles_x = (g.nx + 7) >> 3;
-    const int iy = blockIdx.x / tiles_x;
-    const int ix = (blockIdx.x % tiles_x) * 8 + warp;
+    const int iy = block / tiles_x;
+    const int ix = (block % tiles_x) * 8 + warp;
     if (ix >= g.nx || iy >= g.ny) return;
     const size_t nxy = (size_t)g.nx * g.ny;
     const size_t nuv = (size_t)g.nu * g.nv;
@@ -184,6 +185,17 @@ __global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restric
 
 // ps = proj * ampv (the axial amplitude the reference applies to the backprojected
 // view in place, geom/cbct/cbct_back.c:196-214), into scratch.
+template <int METHOD, int MZ, bool VEC, bool PRESCALED = true>
+__global__ void __launch_bounds__(256) back_kernel(Geom g, const View *__restrict__ views,
+                                                   const float *__restrict__ ps, const uint8_t *__restrict__ map,
+                                                   void *__restrict__ image, int out_dtype, int view_begin,
+                                                   int view_stride, int view_count, float scale, int qcap,
+                                                   int *__restrict__ err, const float *__restrict__ ampv) {
+    extern __shared__ float smem[];
+    back_block<METHOD, MZ, VEC, PRESCALED>(g, views, ps, map, image, out_dtype, view_begin, view_stride, view_count,
+                                           scale, qcap, err, ampv, smem, blockIdx.x);
+}
+
 __global__ void prescale_kernel(const void *__restrict__ proj, int in_dtype, const float *__restrict__ ampv,
                                 float *__restrict__ ps, size_t nuv, size_t n) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -268,13 +280,11 @@ struct ProjSmem {
 // g, g + groups, ... into its own accumulators, summed in group order at the store,
 // so short detectors (few rows) still keep 8 warps busy per block.
 template <int METHOD, int GROUPS>
-__global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const View *__restrict__ views,
-                                                               const float *__restrict__ xs,
-                                                               const float *__restrict__ ampv,
-                                                               const uint8_t *__restrict__ map,
-                                                               void *__restrict__ proj, int out_dtype,
-                                                               int view_begin, int view_stride, float margin) {
-    extern __shared__ float4 acc4[];  // [GROUPS][kTU][nq] row quads, then the arrays below
+__device__ __forceinline__ void proj_block(const Geom g, const View *__restrict__ views, const float *__restrict__ xs,
+                                           const float *__restrict__ ampv, const uint8_t *__restrict__ map,
+                                           void *__restrict__ proj, int out_dtype, int view_begin, int view_stride,
+                                           float margin, float4 *acc4, int bx, int by) {
+    // acc4: [GROUPS][kTU][nq] row quads, then the arrays below (dynamic shared memory)
     const int NT = blockDim.x;
     constexpr int groups = GROUPS;
     const int R = NT / GROUPS;
@@ -294,8 +304,8 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int grp = GROUPS == 1 ? 0 : t / R;  // candidate group
     const int gwarp = GROUPS == 1 ? warp : (t - grp * R) >> 5;  // warp within the group
-    const int iu0 = blockIdx.x * kTU;
-    const int k = blockIdx.y;
+    const int iu0 = bx * kTU;
+    const int k = by;
     const View v = views[view_begin + k * view_stride];
     const int nv = g.nv;
     const int nq = (nv + 3) >> 2;
@@ -474,6 +484,18 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
             store_from_float(proj, obase + (size_t)iu * nv + iv, a * ampv[(size_t)iu * nv + iv], out_dtype);
         }
     }
+}
+
+template <int METHOD, int GROUPS>
+__global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const View *__restrict__ views,
+                                                               const float *__restrict__ xs,
+                                                               const float *__restrict__ ampv,
+                                                               const uint8_t *__restrict__ map,
+                                                               void *__restrict__ proj, int out_dtype,
+                                                               int view_begin, int view_stride, float margin) {
+    extern __shared__ float4 acc4_smem[];
+    proj_block<METHOD, GROUPS>(g, views, xs, ampv, map, proj, out_dtype, view_begin, view_stride, margin, acc4_smem,
+                               blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -747,6 +769,96 @@ cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const
     case 4: return launch_back_unscaled_mz<kDD, 4>(g, views, proj, ampv, map, image, vc, qcap, err, st);
     case 8: return launch_back_unscaled_mz<kDD, 8>(g, views, proj, ampv, map, image, vc, qcap, err, st);
     }
+    return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// Batched launches.  One persistent grid (the resident blocks of the whole GPU) walks
+// the flat block list of up to kBatchMax tasks -- plans of different geometries -- and
+// runs each block's work with its task's tables; the task table is a __grid_constant__
+// kernel parameter, so a batch needs no device allocation and can be graph-captured.
+// ---------------------------------------------------------------------------
+template <int METHOD, int GROUPS>
+__global__ void __launch_bounds__(kProjMaxThreads) proj_batch_kernel(const __grid_constant__ ProjBatch b) {
+    extern __shared__ float4 acc4_batch[];
+    for (int blk = blockIdx.x; blk < b.total; blk += gridDim.x) {
+        int lo = 0, hi = b.n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (b.t[mid].first <= blk) lo = mid; else hi = mid - 1;
+        }
+        const ProjTask &T = b.t[lo];
+        const int local = blk - T.first;
+        proj_block<METHOD, GROUPS>(T.g, T.views, T.xs, T.ampv, T.map, T.proj, kF32, T.vb, T.vs, T.margin, acc4_batch,
+                                   local % T.gx, local / T.gx);
+        __syncthreads();  // the next block reuses the shared accumulators
+    }
+}
+
+template <int METHOD, int MZ, bool VEC>
+__global__ void __launch_bounds__(256) back_batch_kernel(const __grid_constant__ BackBatch b) {
+    extern __shared__ float smem_batch[];
+    for (int blk = blockIdx.x; blk < b.total; blk += gridDim.x) {
+        int lo = 0, hi = b.n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (b.t[mid].first <= blk) lo = mid; else hi = mid - 1;
+        }
+        const BackTask &T = b.t[lo];
+        back_block<METHOD, MZ, VEC, true>(T.g, T.views, T.ps, T.map, T.image, kF32, T.vb, T.vs, T.vc, T.scale, T.qcap,
+                                          T.err, nullptr, smem_batch, blk - T.first);
+        // the per-warp row buffers are laid out with the task's own stride, so a warp may
+        // not start the next item (possibly another task) while its neighbours still work
+        __syncthreads();
+    }
+}
+
+int proj_task_blocks(const Geom &g, int view_count) { return ((g.nu + kTU - 1) / kTU) * view_count; }
+int back_task_blocks(const Geom &g) { return g.ny * ((g.nx + 7) / 8); }
+int proj_row_threads_of(int nv) { return proj_row_threads(nv); }
+
+template <class K>
+static int persistent_grid(K kernel, int threads, size_t smem, int total) {
+    int dev = 0, sms = 148, per_sm = 1;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    return std::max(1, std::min(total, sms * per_sm));
+}
+
+cudaError_t launch_proj_batch(int method, int groups, int row_threads, size_t smem, const ProjBatch &b,
+                              cudaStream_t st) {
+    if (b.n < 1 || b.total < 1) return cudaSuccess;
+    const int nt = row_threads * groups;
+#define CTSIM_PB_CASE(M, GR)                                                                          \
+    if (method == M && groups == GR) {                                                                \
+        auto k = proj_batch_kernel<M, GR>;                                                            \
+        cudaError_t e = allow_dynamic_smem((const void *)k, smem);                                    \
+        if (e != cudaSuccess) return e;                                                               \
+        k<<<persistent_grid(k, nt, smem, b.total), nt, smem, st>>>(b);                                \
+        return cudaGetLastError();                                                                    \
+    }
+    CTSIM_PB_CASE(kDD, 1) CTSIM_PB_CASE(kDD, 2) CTSIM_PB_CASE(kDD, 4) CTSIM_PB_CASE(kDD, 8)
+    CTSIM_PB_CASE(kTF, 1) CTSIM_PB_CASE(kTF, 2) CTSIM_PB_CASE(kTF, 4) CTSIM_PB_CASE(kTF, 8)
+#undef CTSIM_PB_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_back_batch(int method, int mz, bool vec, size_t smem, const BackBatch &b, cudaStream_t st) {
+    if (b.n < 1 || b.total < 1) return cudaSuccess;
+#define CTSIM_BB_CASE(M, Z, V)                                                                        \
+    if (method == M && mz == Z && vec == V) {                                                         \
+        auto k = back_batch_kernel<M, Z, V>;                                                          \
+        cudaError_t e = allow_dynamic_smem((const void *)k, smem);                                    \
+        if (e != cudaSuccess) return e;                                                               \
+        k<<<persistent_grid(k, 256, smem, b.total), 256, smem, st>>>(b);                              \
+        return cudaGetLastError();                                                                    \
+    }
+    CTSIM_BB_CASE(kDD, 1, true) CTSIM_BB_CASE(kDD, 2, true) CTSIM_BB_CASE(kDD, 4, true) CTSIM_BB_CASE(kDD, 8, true)
+    CTSIM_BB_CASE(kDD, 1, false) CTSIM_BB_CASE(kDD, 2, false) CTSIM_BB_CASE(kDD, 4, false) CTSIM_BB_CASE(kDD, 8, false)
+    CTSIM_BB_CASE(kTF, 1, true) CTSIM_BB_CASE(kTF, 2, true) CTSIM_BB_CASE(kTF, 4, true) CTSIM_BB_CASE(kTF, 8, true)
+    CTSIM_BB_CASE(kTF, 1, false) CTSIM_BB_CASE(kTF, 2, false) CTSIM_BB_CASE(kTF, 4, false) CTSIM_BB_CASE(kTF, 8, false)
+#undef CTSIM_BB_CASE
     return cudaErrorInvalidValue;
 }
 

@@ -39,6 +39,49 @@ cudaError_t launch_pd(int mode, int mz, const Geom &g, const View *views, const 
 
 cudaError_t launch_scale(float *y, size_t n, float s, cudaStream_t st);
 
+// ---------------------------------------------------------------------------
+// Batched launches: the blocks of many plans' A (or A^T) in one persistent grid.
+// ---------------------------------------------------------------------------
+constexpr int kBatchMax = 64;  // tasks per launch (the task table travels as a kernel parameter)
+
+struct ProjTask {
+    Geom g;
+    const View *views;
+    const float *xs;
+    const float *ampv;
+    const uint8_t *map;
+    float *proj;
+    int vb, vs, gx, first;  // view selection, blocks along u, first flat block of the task
+    float margin;
+};
+struct ProjBatch {
+    int n, total;  // tasks, flat blocks of all tasks
+    ProjTask t[kBatchMax];
+};
+
+struct BackTask {
+    Geom g;
+    const View *views;
+    const float *ps;
+    const uint8_t *map;
+    float *image;
+    int *err;
+    int vb, vs, vc, qcap, first;
+    float scale;
+};
+struct BackBatch {
+    int n, total;
+    BackTask t[kBatchMax];
+};
+
+// The flat blocks of a task: A (u groups x views), A^T (rows x column tiles).
+int proj_task_blocks(const Geom &g, int view_count);
+int back_task_blocks(const Geom &g);
+int proj_row_threads_of(int nv);
+cudaError_t launch_proj_batch(int method, int groups, int row_threads, size_t smem, const ProjBatch &b,
+                              cudaStream_t st);
+cudaError_t launch_back_batch(int method, int mz, bool vec, size_t smem, const BackBatch &b, cudaStream_t st);
+
 // Raises (never lowers) a kernel's dynamic shared-memory limit on the current device.
 cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes);
 

@@ -328,3 +328,34 @@ def loadPojectors(geom: CTGeometry, numos: int = 1):
     At = lambda y: backProjectMex(y, geom, 1, 0, "back,tf")
     Os = lambda x, isub: orderedSubset(x, numos, isub)
     return A, At, Aos, Atos, Os
+
+
+def _batch(fn_name, method_id, entries):
+    """entries: (plan, in_tensor, out_tensor, view_begin, view_stride, view_count, scale)."""
+    torch = _torch()
+    L = _lib.load()
+    n = len(entries)
+    if n == 0:
+        return
+    arr = (_lib.CtsimBatchItem * n)()
+    keep = []
+    for k, (plan, x, y, vb, vs, vc, scale) in enumerate(entries):
+        for t in (x, y):
+            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+                raise TypeError("batched launches take contiguous float32 CUDA tensors")
+        arr[k] = _lib.CtsimBatchItem(plan._h, x.data_ptr(), y.data_ptr(), int(vb), int(vs), int(vc), float(scale))
+        keep.append(plan)
+    st = torch.cuda.current_stream(entries[0][0].device).cuda_stream
+    _lib.check(getattr(L, fn_name)(method_id, arr, n, st), fn_name)
+
+
+def batch_project(method: str, entries):
+    """A of many plans in one persistent launch per launch-shape class: entries are
+    (plan, image, out_sino, view_begin, view_stride, view_count) (ctsim_batch_project)."""
+    _batch("ctsim_batch_project", {"dd": 0, "tf": 1}[method], [e + (1.0,) if len(e) == 6 else e for e in entries])
+
+
+def batch_backproject(method: str, entries):
+    """scale * A^T of many plans: entries are (plan, sino, out_image, view_begin,
+    view_stride, view_count, scale) (ctsim_batch_backproject)."""
+    _batch("ctsim_batch_backproject", {"dd": 2, "tf": 3}[method], entries)

@@ -10,6 +10,7 @@ Mirrors the reference's MATLAB entry points with torch CUDA tensors:
                                                 statsrecon/pwls/reconPwlsSeSqs.m
 * ``reconPwlsSeNesterovSqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0, imgOpt)``
                                                 statsrecon/pwls/reconPwlsSeNesterovSqs.m
+* ``BatchedPwls(solvers)``                      many reconPwlsSeSqs instances in batched launches
 
 The projectors are the separable-footprint pair the reference's PWLS loads
 (geom/shell/loadPojectors.m:8-11); all per-voxel and per-ray arithmetic runs in
@@ -295,3 +296,104 @@ def reconPwlsSeNesterovSqs(y, w, geom: CTGeometry, beta: float, pfun: str = "hub
         if itn % nrestart == 0:
             solver.restart()
     return solver.x, phis, rmsds
+
+
+class BatchedPwls:
+    """Many OS-PWLS reconstructions (reconPwlsSeSqs.m:57-66 each) stepped together.
+
+    Every sub-iteration runs ONE persistent A launch over all instances' subset views
+    (ctsim_batch_project, per launch-shape class), the per-instance residuals, ONE
+    persistent A^T launch (ctsim_batch_backproject) and the per-instance SQS updates;
+    with ``graphs`` an outer iteration of all instances is one CUDA-graph replay after
+    the first.  The instances keep their own plans, data and state, so each result is
+    the one its own solver would compute.  All solvers use the same projector method
+    and number of subsets.
+    """
+
+    def __init__(self, solvers, graphs: bool = True):
+        if not solvers:
+            raise ValueError("no solvers")
+        self.solvers = list(solvers)
+        self.M = self.solvers[0].M
+        self.method = self.solvers[0].method
+        if any(s.M != self.M or s.method != self.method for s in self.solvers):
+            raise ValueError("batched solvers need the same method and number of subsets")
+        if len({id(s.plan) for s in self.solvers}) != len(self.solvers):
+            raise ValueError("each batched solver needs its own plan")
+        self.graphs = graphs
+        self._graph = {}
+        self.itn = 0
+
+    def subset_step(self, i: int):
+        from .projector import batch_backproject, batch_project
+        stride = 1 if self.M == 1 else self.M
+        fwd, back = [], []
+        for s in self.solvers:
+            if i == 0:
+                s.xold.copy_(s.x)
+                s.acc.zero_()
+            start, count, _, _ = s.subsets[i]
+            fwd.append((s.plan, s.x, s.ax[:count], start, stride, count))
+        batch_project(self.method, fwd)
+        for s in self.solvers:
+            start, count, ys, ws = s.subsets[i]
+            ax, wd = s.ax[:count], s.wd[:count]
+            _lib.check(s.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), s.sdt, s.w_scale,
+                                                  wd.data_ptr(), ax.numel(), s.acc.data_ptr(), _stream(s.dev)),
+                       "ctsim_pwls_residual")
+            back.append((s.plan, wd, s.num, start, stride, count, float(s.M)))
+        batch_backproject(self.method, back)
+        for s in self.solvers:
+            _lib.check(s.L.ctsim_sqs_update(s.kind, s.beta, s.delta, s.nx, s.ny, s.nz, s.x.data_ptr(),
+                                            s.xn.data_ptr(), s.num.data_ptr(), s.precom.data_ptr(), _stream(s.dev)),
+                       "ctsim_sqs_update")
+            s.x, s.xn = s.xn, s.x
+
+    def _eager_iteration(self):
+        for i in range(self.M):
+            self.subset_step(i)
+        for s in self.solvers:
+            s.end_iteration()
+
+    def iteration(self):
+        """One outer iteration of every instance (asynchronous, ordered after the work
+        already queued on the current stream; graphs are captured on a private stream)."""
+        torch = _torch()
+        cur = torch.cuda.current_stream(self.solvers[0].dev)
+        if not hasattr(self, "_stream"):
+            self._stream = torch.cuda.Stream(device=self.solvers[0].dev)
+        self._stream.wait_stream(cur)
+        with torch.cuda.stream(self._stream):
+            self._iteration_on_stream(torch)
+        cur.wait_stream(self._stream)
+        self.itn += 1
+        for s in self.solvers:
+            s.itn += 1
+
+    def _iteration_on_stream(self, torch):
+        if not self.graphs or self.itn == 0:
+            self._eager_iteration()
+        else:
+            key = tuple(s.x.data_ptr() for s in self.solvers)
+            g = self._graph.get(key)
+            if g is None:
+                # recorded, not run: the pointer swaps leave the host side as after the run
+                g = torch.cuda.CUDAGraph()
+                g.capture_begin(capture_error_mode="thread_local")
+                self._eager_iteration()
+                g.capture_end()
+                self._graph[key] = g
+            else:
+                for s in self.solvers:
+                    for _ in range(self.M):
+                        s.x, s.xn = s.xn, s.x
+            g.replay()
+
+    def step(self):
+        """One outer iteration; returns [(phi, rmsd)] per instance (synchronises)."""
+        self.iteration()
+        out = []
+        for s in self.solvers:
+            a = s.acc.cpu().numpy()
+            out.append((a[0] / 2 + s.beta * a[2], math.sqrt(a[1] / s.x.numel())))
+        return out

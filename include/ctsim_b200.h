@@ -185,6 +185,25 @@ ctsim_status ctsim_plan_set_tuning(ctsim_plan *plan, const ctsim_tuning *tuning)
 ctsim_status ctsim_plan_autotune(ctsim_plan *plan, int method, int sample_views, void *stream, ctsim_tuning *chosen);
 ctsim_status ctsim_autotune_clear(void);
 
+/* Batched launches (no reference counterpart): the distance-driven or separable-footprint
+ * A (CTSIM_PROJ_DD/TF) or A^T (CTSIM_BACK_DD/TF) of n plans -- different geometries, one
+ * device -- with FP32 device buffers: `in` is the image (A) or the selected views' sinogram
+ * (A^T), `out` the sinogram of the selected views or the image (overwritten; A^T times
+ * scale).  After the per-plan pre-passes (column prefix sums, or the ampv pre-scaling)
+ * the projector blocks of all plans run in ONE persistent grid per launch-shape class
+ * (forward: row threads and candidate groups; backward: z blocks and row vectorisation),
+ * at most 64 plans per grid.  Each plan's scratch is used, so a plan appears at most once
+ * per call.  Results equal the per-plan calls bit for bit. */
+typedef struct {
+    ctsim_plan *plan;
+    const float *in;
+    float *out;
+    int view_begin, view_stride, view_count;
+    float scale;
+} ctsim_batch_item;
+ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *items, int n, void *stream);
+ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_item *items, int n, void *stream);
+
 /* Bytes of device memory the plan holds (tables + scratch). */
 size_t ctsim_plan_device_bytes(const ctsim_plan *plan);
 
