@@ -396,14 +396,15 @@ def run_serving(args):
         return out
 
     def served(reqs, **kw):
-        srv = ReconServer(max_active=args.slots, to_host=True, admit_workers=2, **kw)
+        srv = ReconServer(max_active=args.slots, to_host=True, admit_workers=2, batch_pwls=args.batch_pwls, **kw)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         done = srv.run(reqs)
         torch.cuda.synchronize()
         return done, time.perf_counter() - t0, srv
 
-    reqs = make_requests(args.requests, seed=args.seed, scale=args.scale, iterations=10, subsets=12)
+    reqs = make_requests(args.requests, seed=args.seed, scale=args.scale, iterations=10, subsets=12,
+                         sizes=args.sizes)
     kinds = [r.kind for r in reqs]
     # untimed pass of every arm over the same requests: pinned host buffers, the memory
     # pools, graph instantiation and (with --autotune) the launch-shape records warm up
@@ -425,8 +426,11 @@ def run_serving(args):
     plain_rps = len(plain) / t_plain
     cap = len(done16) / t16
     sweep = []
-    for frac in (0.5, 0.8):
-        rate = frac * cap
+    # the configured arrival rates (2-50 req/s) that the measured capacity can carry, and
+    # 50% / 80% of the capacity
+    rates = sorted({r for r in (2.0, 5.0, 10.0, 20.0, 50.0) if r <= 0.9 * cap} | {0.5 * cap, 0.8 * cap})
+    for rate in rates:
+        frac = rate / cap
         arr = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
         d, t, _ = served(fresh(reqs, "bfloat16", arr), autotune=args.autotune)
         st = latency_stats(d, t)
@@ -440,7 +444,8 @@ def run_serving(args):
         "data": "synthetic (seeded ellipsoid phantoms, Poisson counts)",
         "config": {"workload": "random_geometry mix", "requests": len(reqs), "fdk": kinds.count("fdk"),
                    "pwls": kinds.count("pwls"), "pwls_iterations": 10, "pwls_subsets": 12, "slots": args.slots,
-                   "scale": args.scale, "seed": args.seed, "autotune": bool(args.autotune)},
+                   "scale": args.scale, "seed": args.seed, "autotune": bool(args.autotune), "sizes": args.sizes,
+                   "batch_pwls_per_tick": bool(args.batch_pwls)},
         "plain_fp32_single_instance_req_per_s": plain_rps,
         "served_fp32_req_per_s": len(done32) / t32,
         "speedup_vs_plain_fp32": cap / plain_rps,
@@ -543,6 +548,9 @@ def main():
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--autotune", action="store_true", help="serving/batched: autotune launch shapes")
     ap.add_argument("--batched", action="store_true", help="batched uneven OS-PWLS instances instead of A/A^T")
+    ap.add_argument("--sizes", choices=["config1", "uneven"], default="uneven", help="serving: request sizes")
+    ap.add_argument("--batch-pwls", dest="batch_pwls", action="store_true",
+                    help="serving: batch the OS-PWLS requests per scheduler tick")
     ap.add_argument("--instances", type=int, default=16, help="instances of the batched run")
     args = ap.parse_args()
     if args.batched:

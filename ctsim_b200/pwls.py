@@ -298,6 +298,40 @@ def reconPwlsSeNesterovSqs(y, w, geom: CTGeometry, beta: float, pfun: str = "hub
     return solver.x, phis, rmsds
 
 
+def batched_subset_steps(pairs):
+    """Sub-iteration i_k of solver k for every (solver_k, i_k) in ``pairs`` -- solvers of
+    different geometries and subset counts, each at its own place in its iteration --
+    with one batched A and one batched A^T (reconPwlsSeSqs.m:57-66 for each solver).
+    Asynchronous on the current stream; the solvers need distinct plans and one method."""
+    from .projector import batch_backproject, batch_project
+    if not pairs:
+        return
+    method = pairs[0][0].method
+    fwd, back = [], []
+    for s, i in pairs:
+        if s.method != method:
+            raise ValueError("batched solvers need the same projector method")
+        if i == 0:
+            s.xold.copy_(s.x)
+            s.acc.zero_()
+        start, count, _, _ = s.subsets[i]
+        fwd.append((s.plan, s.x, s.ax[:count], start, 1 if s.M == 1 else s.M, count))
+    batch_project(method, fwd)
+    for s, i in pairs:
+        start, count, ys, ws = s.subsets[i]
+        ax, wd = s.ax[:count], s.wd[:count]
+        _lib.check(s.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), s.sdt, s.w_scale,
+                                              wd.data_ptr(), ax.numel(), s.acc.data_ptr(), _stream(s.dev)),
+                   "ctsim_pwls_residual")
+        back.append((s.plan, wd, s.num, start, 1 if s.M == 1 else s.M, count, float(s.M)))
+    batch_backproject(method, back)
+    for s, i in pairs:
+        _lib.check(s.L.ctsim_sqs_update(s.kind, s.beta, s.delta, s.nx, s.ny, s.nz, s.x.data_ptr(),
+                                        s.xn.data_ptr(), s.num.data_ptr(), s.precom.data_ptr(), _stream(s.dev)),
+                   "ctsim_sqs_update")
+        s.x, s.xn = s.xn, s.x
+
+
 class BatchedPwls:
     """Many OS-PWLS reconstructions (reconPwlsSeSqs.m:57-66 each) stepped together.
 
@@ -325,29 +359,7 @@ class BatchedPwls:
         self.itn = 0
 
     def subset_step(self, i: int):
-        from .projector import batch_backproject, batch_project
-        stride = 1 if self.M == 1 else self.M
-        fwd, back = [], []
-        for s in self.solvers:
-            if i == 0:
-                s.xold.copy_(s.x)
-                s.acc.zero_()
-            start, count, _, _ = s.subsets[i]
-            fwd.append((s.plan, s.x, s.ax[:count], start, stride, count))
-        batch_project(self.method, fwd)
-        for s in self.solvers:
-            start, count, ys, ws = s.subsets[i]
-            ax, wd = s.ax[:count], s.wd[:count]
-            _lib.check(s.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), s.sdt, s.w_scale,
-                                                  wd.data_ptr(), ax.numel(), s.acc.data_ptr(), _stream(s.dev)),
-                       "ctsim_pwls_residual")
-            back.append((s.plan, wd, s.num, start, stride, count, float(s.M)))
-        batch_backproject(self.method, back)
-        for s in self.solvers:
-            _lib.check(s.L.ctsim_sqs_update(s.kind, s.beta, s.delta, s.nx, s.ny, s.nz, s.x.data_ptr(),
-                                            s.xn.data_ptr(), s.num.data_ptr(), s.precom.data_ptr(), _stream(s.dev)),
-                       "ctsim_sqs_update")
-            s.x, s.xn = s.xn, s.x
+        batched_subset_steps([(s, i) for s in self.solvers])
 
     def _eager_iteration(self):
         for i in range(self.M):

@@ -93,7 +93,8 @@ def hbm_footprint(req: ReconRequest) -> int:
 class _Active:
     """Device state and work of one admitted request (runs on its slot's stream)."""
 
-    def __init__(self, req: ReconRequest, stream, device, graphs: bool = True, autotune: bool = False):
+    def __init__(self, req: ReconRequest, stream, device, graphs: bool = True, autotune: bool = False,
+                 batched: bool = False):
         import torch
         from .fdk import FDK
         from .projector import Plan
@@ -122,6 +123,15 @@ class _Active:
                 self.fdk.close()
                 self.fdk = None
                 self.units = req.iterations
+        # batched OS-PWLS: the server steps the request's sub-iterations together with the
+        # other active requests' on its batch stream, after this set-up on the slot stream
+        self.batched = batched and req.kind == "pwls"
+        if self.batched:
+            self.units = req.iterations * req.subsets
+            self.sub = 0
+            self.joined = False
+            self.ready = torch.cuda.Event()
+            self.ready.record(stream)
 
     def in_flight(self) -> int:
         while self.events and self.events[0].query():
@@ -174,6 +184,30 @@ class _Active:
             ev.record(self.stream)
             self.events.append(ev)
 
+    def batch_pair(self):
+        """(solver, subset index) of the next batched sub-iteration."""
+        return self.solver, self.sub
+
+    def batch_advance(self, to_host: bool, stream):
+        """Book-keeping after a batched sub-iteration (on the batch stream): the
+        iteration's objective terms after its last subset, the result after the last."""
+        import torch
+        self.sub += 1
+        self.issued += 1
+        if self.sub == self.req.subsets:
+            self.sub = 0
+            self.solver.end_iteration()
+        if self.issued == self.units:
+            img = self.solver.x
+            if to_host:
+                host = torch.empty(img.shape, dtype=img.dtype, pin_memory=True)
+                host.copy_(img, non_blocking=True)
+                img = host
+            self.req.result = img
+            ev = torch.cuda.Event()
+            ev.record(stream)
+            self.events.append(ev)
+
     def complete(self) -> bool:
         return self.issued == self.units and self.in_flight() == 0
 
@@ -205,7 +239,7 @@ class ReconServer:
 
     def __init__(self, hbm_budget: int = 150 * 2 ** 30, max_active: int = 8, depth: int = 2, device=None,
                  graphs: bool = True, activate: Optional[Callable] = None, clock: Optional[Callable] = None,
-                 to_host: bool = False, admit_workers: int = 0, autotune: bool = False):
+                 to_host: bool = False, admit_workers: int = 0, autotune: bool = False, batch_pwls: bool = False):
         self.budget = int(hbm_budget)
         self.max_active = int(max_active)
         self.depth = int(depth)
@@ -228,10 +262,14 @@ class ReconServer:
             self.device = torch.device("cuda", torch.cuda.current_device() if device is None else
                                        (torch.device(device).index or 0))
             self.streams = [torch.cuda.Stream(device=self.device) for _ in range(self.max_active)]
-            activate = lambda req, slot: _Active(req, self.streams[slot], self.device, self.graphs, autotune)
+            self.batch_stream = torch.cuda.Stream(device=self.device) if batch_pwls else None
+            activate = lambda req, slot: _Active(req, self.streams[slot], self.device, self.graphs, autotune,
+                                                 batch_pwls)
         else:
             self.streams = [None] * self.max_active
         self._activate = activate
+        self.batch_pwls = batch_pwls
+        self._tick_events = deque()
         self._free_slots = list(range(self.max_active))[::-1]
         self._slot_of = {}
 
@@ -301,9 +339,36 @@ class ReconServer:
         if self.starting:
             self._collect_started()
         for a in self.active:
-            if a.issued < a.units and a.in_flight() < self.depth:
+            if not getattr(a, "batched", False) and a.issued < a.units and a.in_flight() < self.depth:
                 a.issue(self.to_host)
+        if self.batch_pwls:
+            self._batched_tick()
         self._retire()
+
+    def _batched_tick(self):
+        """One sub-iteration of every active OS-PWLS request in one batched A and one
+        batched A^T launch on the batch stream (at most ``depth`` ticks in flight)."""
+        import torch
+        from .pwls import batched_subset_steps
+        while self._tick_events and self._tick_events[0].query():
+            self._tick_events.popleft()
+        if len(self._tick_events) >= self.depth:
+            return
+        pw = [a for a in self.active if getattr(a, "batched", False) and a.issued < a.units]
+        if not pw:
+            return
+        bs = self.batch_stream
+        with torch.cuda.device(self.device), torch.cuda.stream(bs):
+            for a in pw:
+                if not a.joined:
+                    bs.wait_event(a.ready)
+                    a.joined = True
+            batched_subset_steps([a.batch_pair() for a in pw])
+            for a in pw:
+                a.batch_advance(self.to_host, bs)
+            ev = torch.cuda.Event()
+            ev.record(bs)
+            self._tick_events.append(ev)
 
     def close(self):
         if self._pool is not None:
@@ -395,10 +460,19 @@ def random_geometry(rng, scale: float = 1.0) -> CTGeometry:
                       1000.0, 500.0, 1500.0, betas, shortScan=short)
 
 
+def config1_geometry() -> CTGeometry:
+    """The plain small reconstruction: 128x128x64 at 1 mm, 360 views over 2 pi, flat
+    256x96 detector at 1.6 mm, SAD 1000 mm, SDD 1500 mm."""
+    return CTGeometry((128, 128, 64), (1.0, 1.0, 1.0), (0, 0, 0), (256, 96), (1.6, 1.6), (0, 0), 1000.0, 500.0,
+                      1500.0, circular_betas(360))
+
+
 def make_requests(n: int, seed: int = 0, fdk_fraction: float = 0.7, storage: str = "bfloat16", scale: float = 1.0,
-                  iterations: int = 10, subsets: int = 12, rate: Optional[float] = None, i0: float = 1e5):
+                  iterations: int = 10, subsets: int = 12, rate: Optional[float] = None, i0: float = 1e5,
+                  sizes: str = "uneven"):
     """``n`` requests (FDK with probability ``fdk_fraction``, else OS-PWLS) over
-    random_geometry, with Poisson arrivals at ``rate`` req/s (all at 0 if None).
+    random_geometry (``sizes="uneven"``) or the config-1 geometry (``sizes="config1"``),
+    with Poisson arrivals at ``rate`` req/s (all at 0 if None).
     The data: a random ellipsoid phantom projected with the SF projector, Poisson
     counts at ``i0`` photons, y = log(i0 / max(counts, 10)) and w = counts
     (computeWeightsPwls with r = v = 0 on counts)."""
@@ -411,7 +485,7 @@ def make_requests(n: int, seed: int = 0, fdk_fraction: float = 0.7, storage: str
     for rid in range(n):
         if rate is not None:
             t += float(rng.exponential(1.0 / rate))
-        g = random_geometry(rng, scale)
+        g = random_geometry(rng, scale) if sizes == "uneven" else config1_geometry()
         r_xy = 0.4 * g.nx * g.reconSpacing[0]
         x = to_projector_units(ellipsoid_phantom(g, 6, (0.015, 0.035), 0.02, r_xy, 0.6 * r_xy,
                                                  0.3 * g.nz * g.reconSpacing[2], (2.0, 8.0),

@@ -138,7 +138,8 @@ def _result(r):
 def test_served_results_do_not_depend_on_the_mix():
     """Bit-identical images whether a request is served alone, in a mix of seven on four
     slots, without CUDA graphs, with set-up on admission threads and delivery to host
-    memory, or through the plain single-instance FP32 API."""
+    memory, with the OS-PWLS requests batched per tick, or through the plain
+    single-instance FP32 API."""
     from ctsim_b200.serving import serve_sequential
     reqs = _device_requests()
     mixed = copy.deepcopy(reqs)
@@ -148,6 +149,8 @@ def test_served_results_do_not_depend_on_the_mix():
     ReconServer(max_active=4, graphs=False).run(eager)
     threaded = copy.deepcopy(reqs)
     ReconServer(max_active=3, to_host=True, admit_workers=2).run(threaded)
+    batched = copy.deepcopy(reqs)
+    ReconServer(max_active=5, to_host=True, admit_workers=2, batch_pwls=True).run(batched)
     plain = serve_sequential(copy.deepcopy(reqs))
     for i, r in enumerate(reqs):
         alone = copy.deepcopy(r)
@@ -157,6 +160,7 @@ def test_served_results_do_not_depend_on_the_mix():
         assert np.array_equal(_result(mixed[i]), a), (i, r.kind)
         assert np.array_equal(_result(eager[i]), a), (i, r.kind)
         assert not threaded[i].result.is_cuda and np.array_equal(_result(threaded[i]), a), (i, r.kind)
+        assert np.array_equal(_result(batched[i]), a), (i, r.kind)
         assert np.array_equal(_result(plain[i]), a), (i, r.kind)
 
 
