@@ -67,6 +67,7 @@ struct ctsim_plan {
     int back_mz = 1, back_qcap = 0, pd_mz = 1;  // A^T (DD) and FDK z-pass depths (tunable)
     int back_mz_tf = 1, back_qcap_tf = 0;       // A^T (SF) z-pass depth (tunable)
     int fwd_groups = 1;      // candidate groups of the forward projector (tunable)
+    int fwd_rows = 32;       // row threads per group of the forward projector (tunable)
     bool fwd_ok = true;
     std::string fwd_reason;
     std::vector<double> betas;  // host copy of the view angles (FDK weights need them)
@@ -317,6 +318,7 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
         p->fwd_reason = "forward projection supports nx, ny <= 2048";
     }
     p->fwd_groups = proj_default_groups(G.nv);
+    p->fwd_rows = proj_default_rows(G.nv);
     if (proj_smem_bytes(G.nv, G.nx, G.ny, p->fwd_groups) > 200 * 1024) {
         p->fwd_ok = false;
         p->fwd_reason = "forward projection supports nv <= 6080";
@@ -395,7 +397,7 @@ extern "C" ctsim_status ctsim_plan_project_ex(ctsim_plan *p, int method, const v
     const int nxy = p->g.nx * p->g.ny;
     cudaError_t e = launch_prefix(d_image, image_dtype, p->d_xs, nxy, p->g.nz, st);
     if (e != cudaSuccess) return cuda_fail(e, "prefix kernel");
-    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->fwd_groups, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
+    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->fwd_groups, p->fwd_rows, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
                     proj_dtype, view_begin, view_stride, view_count, p->margin, st);
     if (e != cudaSuccess) return cuda_fail(e, "forward projection kernel");
     return CTSIM_OK;
@@ -585,6 +587,7 @@ extern "C" bool ctsim_cbct_geom(const char *type, CTSIM_GEOM_PARAMS, const float
 extern "C" ctsim_status ctsim_plan_get_tuning(const ctsim_plan *p, ctsim_tuning *t) {
     if (!p || !t) return fail(CTSIM_ERR_ARGUMENT, "null argument");
     t->proj_groups = p->fwd_groups;
+    t->proj_rows = p->fwd_rows;
     t->back_mz = p->back_mz;
     t->back_mz_tf = p->back_mz_tf;
     t->pd_mz = p->pd_mz;
@@ -595,14 +598,20 @@ static bool mz_valid(int mz) { return mz == 1 || mz == 2 || mz == 4 || mz == 8; 
 
 extern "C" ctsim_status ctsim_plan_set_tuning(ctsim_plan *p, const ctsim_tuning *t) {
     if (!p || !t) return fail(CTSIM_ERR_ARGUMENT, "null argument");
-    if (t->proj_groups && (!proj_groups_valid(p->geom.nv, t->proj_groups) ||
-                           proj_smem_bytes(p->geom.nv, p->geom.nx, p->geom.ny, t->proj_groups) > 200 * 1024))
-        return fail(CTSIM_ERR_ARGUMENT, "proj_groups must be 1, 2, 4 or 8 with groups * row threads <= 256");
+    if (t->proj_groups || t->proj_rows) {
+        const int G = t->proj_groups ? t->proj_groups : p->fwd_groups;
+        const int R = t->proj_rows ? t->proj_rows : p->fwd_rows;
+        if (!proj_shape_valid(p->geom.nv, G, R) || proj_smem_bytes(p->geom.nv, p->geom.nx, p->geom.ny, G, R) > 200 * 1024)
+            return fail(CTSIM_ERR_ARGUMENT,
+                        "proj_groups must be 1, 2, 4 or 8 and proj_rows a multiple of 32 up to the rows' need, "
+                        "with groups * rows <= 256");
+    }
     if ((t->back_mz && (!mz_valid(t->back_mz) || !back_mz_fits(p, t->back_mz))) ||
         (t->back_mz_tf && (!mz_valid(t->back_mz_tf) || !back_mz_fits(p, t->back_mz_tf))))
         return fail(CTSIM_ERR_ARGUMENT, "back_mz must be 1, 2, 4 or 8 and fit the row buffer");
     if (t->pd_mz && !mz_valid(t->pd_mz)) return fail(CTSIM_ERR_ARGUMENT, "pd_mz must be 1, 2, 4 or 8");
     if (t->proj_groups) p->fwd_groups = t->proj_groups;
+    if (t->proj_rows) p->fwd_rows = t->proj_rows;
     if (t->back_mz) {
         p->back_mz = t->back_mz;
         p->back_qcap = back_qcap_for(p, t->back_mz);
@@ -616,27 +625,44 @@ extern "C" ctsim_status ctsim_plan_set_tuning(ctsim_plan *p, const ctsim_tuning 
 }
 
 namespace {
-// Choices measured in this process, by shape class: method, the forward projector's row
-// threads (a function of nv), the z passes, the volume and detector sizes.
+// Choices measured in this process, by shape class: method, the volume and detector
+// sizes and the detector type.
 std::mutex g_tune_mutex;
-std::map<std::vector<int>, int> g_tuned;
+std::map<std::vector<int>, ctsim_tuning> g_tuned;
 }  // namespace
-
-// The tuning field a method's launch shape lives in.
-static int &tuning_field(ctsim_tuning &t, int method) {
-    switch (method) {
-    case CTSIM_PROJ_DD:
-    case CTSIM_PROJ_TF: return t.proj_groups;
-    case CTSIM_BACK_DD: return t.back_mz;
-    case CTSIM_BACK_TF: return t.back_mz_tf;
-    default: return t.pd_mz;
-    }
-}
 
 extern "C" ctsim_status ctsim_autotune_clear(void) {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     g_tuned.clear();
     return CTSIM_OK;
+}
+
+// The launch shapes the autotuner tries for a method (only the method's own fields set).
+static std::vector<ctsim_tuning> tuning_candidates(const ctsim_plan *p, int method) {
+    std::vector<ctsim_tuning> out;
+    const ctsim_geom &G = p->geom;
+    if (method == CTSIM_PROJ_DD || method == CTSIM_PROJ_TF) {
+        const int rmax = proj_default_rows(G.nv);
+        std::vector<int> rows = {rmax};
+        if (rmax > 64) rows.push_back(64);
+        if (rmax > 32) rows.push_back(32);
+        for (int R : rows) {
+            for (int Gr : {1, 2, 4, 8})
+                if (proj_shape_valid(G.nv, Gr, R) && proj_smem_bytes(G.nv, G.nx, G.ny, Gr, R) <= 200 * 1024) {
+                    ctsim_tuning t = {Gr, 0, 0, 0, R};
+                    out.push_back(t);
+                }
+        }
+        return out;
+    }
+    for (int mz : {1, 2, 4, 8}) {
+        ctsim_tuning t = {0, 0, 0, 0, 0};
+        if (method == CTSIM_BACK_DD) { if (!back_mz_fits(p, mz)) continue; t.back_mz = mz; }
+        else if (method == CTSIM_BACK_TF) { if (!back_mz_fits(p, mz)) continue; t.back_mz_tf = mz; }
+        else t.pd_mz = mz;
+        out.push_back(t);
+    }
+    return out;
 }
 
 extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sample_views, void *stream,
@@ -646,21 +672,21 @@ extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sampl
     const bool fwd = method == CTSIM_PROJ_DD || method == CTSIM_PROJ_TF;
     const bool vox = method >= CTSIM_BACK_PD;
     if ((fwd || !vox) && !p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
+    if (p->g.det == 2 && method != CTSIM_PROJ_DD && method != CTSIM_BACK_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
     const ctsim_geom &G = p->geom;
     const std::vector<int> key = {method, G.nx, G.ny, G.nz, G.nu, G.nv, G.detector_type};
-    int best = 0;
+    bool have = false;
+    ctsim_tuning best = {0, 0, 0, 0, 0};
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tuned.find(key);
-        if (it != g_tuned.end()) best = it->second;
-    }
-    if (!best) {
-        std::vector<int> cand;
-        for (int c : {1, 2, 4, 8}) {
-            if (fwd ? (proj_groups_valid(G.nv, c) && proj_smem_bytes(G.nv, G.nx, G.ny, c) <= 200 * 1024)
-                    : vox ? true : back_mz_fits(p, c))
-                cand.push_back(c);
+        if (it != g_tuned.end()) {
+            best = it->second;
+            have = true;
         }
+    }
+    if (!have) {
+        const std::vector<ctsim_tuning> cand = tuning_candidates(p, method);
         // the launch shape that wins depends on the grid, so the sample should be the size
         // of the real launches (an OS-PWLS subset, or all views); default: up to 64 views
         if (sample_views < 1) sample_views = 64;
@@ -677,7 +703,8 @@ extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sampl
             ctsim_plan_release(p, img);
             return fail(CTSIM_ERR_ALLOC, std::string("autotune buffers: ") + cudaGetErrorString(e));
         }
-        const ctsim_tuning saved = {p->fwd_groups, p->back_mz, p->pd_mz, p->back_mz_tf};
+        ctsim_tuning saved;
+        ctsim_plan_get_tuning(p, &saved);
         float best_ms = 0.f;
         ctsim_status s = CTSIM_OK;
         if ((e = cudaMemsetAsync(img, 0, nimg * 4, st)) != cudaSuccess ||
@@ -686,9 +713,7 @@ extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sampl
             s = cuda_fail(e, "autotune set-up");
         }
         for (size_t i = 0; s == CTSIM_OK && i < cand.size(); i++) {
-            ctsim_tuning t = {0, 0, 0, 0};
-            tuning_field(t, method) = cand[i];
-            if ((s = ctsim_plan_set_tuning(p, &t)) != CTSIM_OK) break;
+            if ((s = ctsim_plan_set_tuning(p, &cand[i])) != CTSIM_OK) break;
             float ms = 0.f;
             for (int rep = 0; rep < 3 && s == CTSIM_OK; rep++) {  // one warm-up, then the faster of two
                 cudaEventRecord(e0, st);
@@ -705,9 +730,10 @@ extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sampl
                 cudaEventElapsedTime(&t_ms, e0, e1);
                 if (rep == 1 || (rep == 2 && t_ms < ms)) ms = t_ms;
             }
-            if (s == CTSIM_OK && (best == 0 || ms < best_ms)) {
+            if (s == CTSIM_OK && (!have || ms < best_ms)) {
                 best = cand[i];
                 best_ms = ms;
+                have = true;
             }
         }
         if (e0) cudaEventDestroy(e0);
@@ -716,12 +742,11 @@ extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sampl
         ctsim_plan_release(p, sino);
         ctsim_plan_set_tuning(p, &saved);
         if (s != CTSIM_OK) return s;
+        if (!have) return fail(CTSIM_ERR_UNSUPPORTED, "no valid launch shape");
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         g_tuned[key] = best;
     }
-    ctsim_tuning t = {0, 0, 0, 0};
-    tuning_field(t, method) = best;
-    ctsim_status s = ctsim_plan_set_tuning(p, &t);
+    ctsim_status s = ctsim_plan_set_tuning(p, &best);
     if (s == CTSIM_OK && chosen) ctsim_plan_get_tuning(p, chosen);
     return s;
 }
@@ -765,7 +790,7 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
     std::map<std::pair<int, int>, std::vector<int>> classes;
     for (int i = 0; i < n; i++) {
         const ctsim_plan *p = items[i].plan;
-        classes[{proj_row_threads_of(p->g.nv), p->fwd_groups}].push_back(i);
+        classes[{p->fwd_rows, p->fwd_groups}].push_back(i);
     }
     for (auto &cl : classes) {
         const std::vector<int> &idx = cl.second;
@@ -790,7 +815,7 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
                 T.first = b.total;
                 T.margin = p->margin;
                 b.total += proj_task_blocks(p->g, it.view_count);
-                smem = std::max(smem, proj_smem_bytes(p->g.nv, p->g.nx, p->g.ny, p->fwd_groups));
+                smem = std::max(smem, proj_smem_bytes(p->g.nv, p->g.nx, p->g.ny, p->fwd_groups, p->fwd_rows));
             }
             if ((e = launch_proj_batch(method == CTSIM_PROJ_DD ? kDD : kTF, cl.first.second, cl.first.first, smem, b,
                                        st)) != cudaSuccess)

@@ -24,11 +24,14 @@ cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const
 
 cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, cudaStream_t st);
 
-cudaError_t launch_proj(int method, int groups, const Geom &g, const View *views, const float *xs,
+cudaError_t launch_proj(int method, int groups, int rows, const Geom &g, const View *views, const float *xs,
                         const float *ampv, const uint8_t *map, void *proj, int out_dtype, int view_begin,
                         int view_stride, int view_count, float margin, cudaStream_t st);
 int proj_default_groups(int nv);
+int proj_default_rows(int nv);
 bool proj_groups_valid(int nv, int groups);
+bool proj_shape_valid(int nv, int groups, int rows);
+size_t proj_smem_bytes(int nv, int nx, int ny, int groups, int rows);
 
 // voxel-driven bilinear modes: back,pd (v outside the detector skipped), back,hpd (v
 // clamped), back,var (geom/cbct/cbct_back_var.c)

@@ -172,6 +172,9 @@ typedef struct {
     int back_mz;
     int pd_mz;
     int back_mz_tf;
+    int proj_rows;  /* row threads per forward group: a multiple of 32 up to ceil(nv/4) rounded
+                       to whole warps; 32 makes each group one warp that walks only the rows
+                       of each candidate's shadow */
 } ctsim_tuning;
 ctsim_status ctsim_plan_get_tuning(const ctsim_plan *plan, ctsim_tuning *tuning);
 ctsim_status ctsim_plan_set_tuning(ctsim_plan *plan, const ctsim_tuning *tuning);
