@@ -47,7 +47,8 @@ class CtsimFanGeom(C.Structure):
 
 
 class CtsimTuning(C.Structure):
-    _fields_ = [("proj_groups", _i), ("back_mz", _i), ("pd_mz", _i), ("back_mz_tf", _i), ("proj_rows", _i)]
+    _fields_ = [("proj_groups", _i), ("back_mz", _i), ("pd_mz", _i), ("back_mz_tf", _i), ("proj_rows", _i),
+                ("proj_layout", _i)]
 
 
 class CtsimBatchItem(C.Structure):

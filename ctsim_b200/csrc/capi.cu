@@ -58,7 +58,7 @@ struct ctsim_plan {
     View *d_views = nullptr;
     float *d_ampv = nullptr;
     uint8_t *d_map = nullptr;
-    float *d_xs = nullptr;   // axial prefix sums [nx*ny][nz+1] -- forward projector scratch
+    float *d_xs = nullptr;   // axial prefix sums [nx*ny][nz+1] (or pairs [..][2]) -- forward projector scratch
     float *d_ps = nullptr;   // sinogram scaled by ampv [noviews][nu][nv] -- backprojector scratch
     int *d_err = nullptr;
     size_t bytes = 0;
@@ -68,6 +68,8 @@ struct ctsim_plan {
     int back_mz_tf = 1, back_qcap_tf = 0;       // A^T (SF) z-pass depth (tunable)
     int fwd_groups = 1;      // candidate groups of the forward projector (tunable)
     int fwd_rows = 32;       // row threads per group of the forward projector (tunable)
+    bool fwd_pairs = false;  // prefix sums stored as (X, slope) pairs (small volumes; tunable)
+    bool xs_holds_pairs = false;  // the prefix scratch was sized for pairs
     bool fwd_ok = true;
     std::string fwd_reason;
     std::vector<double> betas;  // host copy of the view angles (FDK weights need them)
@@ -349,7 +351,8 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
     CTSIM_ALLOC(p->d_ampv, sizeof(float) * ampv.size());
     CTSIM_ALLOC(p->d_map, mp.size());
     CTSIM_ALLOC(p->d_err, sizeof(int));
-    if (p->fwd_ok) CTSIM_ALLOC(p->d_xs, sizeof(float) * (size_t)nxy * (G.nz + 1));
+    p->fwd_pairs = p->xs_holds_pairs = forward_pairs(nxy, G.nz);
+    if (p->fwd_ok) CTSIM_ALLOC(p->d_xs, sizeof(float) * (p->fwd_pairs ? 2 : 1) * (size_t)nxy * (G.nz + 1));
     CTSIM_ALLOC(p->d_ps, sizeof(float) * (size_t)G.nu * G.nv * G.noviews);
 #undef CTSIM_ALLOC
     p->bytes = bytes;
@@ -395,9 +398,9 @@ extern "C" ctsim_status ctsim_plan_project_ex(ctsim_plan *p, int method, const v
     if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
     cudaStream_t st = (cudaStream_t)stream;
     const int nxy = p->g.nx * p->g.ny;
-    cudaError_t e = launch_prefix(d_image, image_dtype, p->d_xs, nxy, p->g.nz, st);
+    cudaError_t e = launch_prefix(d_image, image_dtype, p->d_xs, nxy, p->g.nz, p->fwd_pairs, st);
     if (e != cudaSuccess) return cuda_fail(e, "prefix kernel");
-    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->fwd_groups, p->fwd_rows, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
+    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->fwd_groups, p->fwd_rows, p->fwd_pairs, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
                     proj_dtype, view_begin, view_stride, view_count, p->margin, st);
     if (e != cudaSuccess) return cuda_fail(e, "forward projection kernel");
     return CTSIM_OK;
@@ -588,6 +591,7 @@ extern "C" ctsim_status ctsim_plan_get_tuning(const ctsim_plan *p, ctsim_tuning 
     if (!p || !t) return fail(CTSIM_ERR_ARGUMENT, "null argument");
     t->proj_groups = p->fwd_groups;
     t->proj_rows = p->fwd_rows;
+    t->proj_layout = p->fwd_pairs ? 2 : 1;
     t->back_mz = p->back_mz;
     t->back_mz_tf = p->back_mz_tf;
     t->pd_mz = p->pd_mz;
@@ -610,8 +614,11 @@ extern "C" ctsim_status ctsim_plan_set_tuning(ctsim_plan *p, const ctsim_tuning 
         (t->back_mz_tf && (!mz_valid(t->back_mz_tf) || !back_mz_fits(p, t->back_mz_tf))))
         return fail(CTSIM_ERR_ARGUMENT, "back_mz must be 1, 2, 4 or 8 and fit the row buffer");
     if (t->pd_mz && !mz_valid(t->pd_mz)) return fail(CTSIM_ERR_ARGUMENT, "pd_mz must be 1, 2, 4 or 8");
+    if (t->proj_layout && t->proj_layout != 1 && !(t->proj_layout == 2 && p->xs_holds_pairs))
+        return fail(CTSIM_ERR_ARGUMENT, "proj_layout must be 1 (sums), or 2 (pairs) on a plan whose volume fits them");
     if (t->proj_groups) p->fwd_groups = t->proj_groups;
     if (t->proj_rows) p->fwd_rows = t->proj_rows;
+    if (t->proj_layout) p->fwd_pairs = t->proj_layout == 2;
     if (t->back_mz) {
         p->back_mz = t->back_mz;
         p->back_qcap = back_qcap_for(p, t->back_mz);
@@ -648,15 +655,16 @@ static std::vector<ctsim_tuning> tuning_candidates(const ctsim_plan *p, int meth
         if (rmax > 32) rows.push_back(32);
         for (int R : rows) {
             for (int Gr : {1, 2, 4, 8})
-                if (proj_shape_valid(G.nv, Gr, R) && proj_smem_bytes(G.nv, G.nx, G.ny, Gr, R) <= 200 * 1024) {
-                    ctsim_tuning t = {Gr, 0, 0, 0, R};
-                    out.push_back(t);
-                }
+                if (proj_shape_valid(G.nv, Gr, R) && proj_smem_bytes(G.nv, G.nx, G.ny, Gr, R) <= 200 * 1024)
+                    for (int lay = p->xs_holds_pairs ? 2 : 1; lay >= 1; lay--) {
+                        ctsim_tuning t = {Gr, 0, 0, 0, R, lay};
+                        out.push_back(t);
+                    }
         }
         return out;
     }
     for (int mz : {1, 2, 4, 8}) {
-        ctsim_tuning t = {0, 0, 0, 0, 0};
+        ctsim_tuning t = {0, 0, 0, 0, 0, 0};
         if (method == CTSIM_BACK_DD) { if (!back_mz_fits(p, mz)) continue; t.back_mz = mz; }
         else if (method == CTSIM_BACK_TF) { if (!back_mz_fits(p, mz)) continue; t.back_mz_tf = mz; }
         else t.pd_mz = mz;
@@ -676,7 +684,7 @@ extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sampl
     const ctsim_geom &G = p->geom;
     const std::vector<int> key = {method, G.nx, G.ny, G.nz, G.nu, G.nv, G.detector_type};
     bool have = false;
-    ctsim_tuning best = {0, 0, 0, 0, 0};
+    ctsim_tuning best = {0, 0, 0, 0, 0, 0};
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tuned.find(key);
@@ -783,14 +791,15 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
     // column prefix sums of every image (each plan's own scratch)
     for (int i = 0; i < n; i++) {
         const ctsim_plan *p = items[i].plan;
-        if ((e = launch_prefix(items[i].in, CTSIM_F32, p->d_xs, p->g.nx * p->g.ny, p->g.nz, st)) != cudaSuccess)
+        if ((e = launch_prefix(items[i].in, CTSIM_F32, p->d_xs, p->g.nx * p->g.ny, p->g.nz, p->fwd_pairs, st)) !=
+            cudaSuccess)
             return cuda_fail(e, "prefix kernel");
     }
     // one persistent launch per launch-shape class (row threads, candidate groups)
-    std::map<std::pair<int, int>, std::vector<int>> classes;
+    std::map<std::vector<int>, std::vector<int>> classes;  // (row threads, groups, prefix layout)
     for (int i = 0; i < n; i++) {
         const ctsim_plan *p = items[i].plan;
-        classes[{p->fwd_rows, p->fwd_groups}].push_back(i);
+        classes[{p->fwd_rows, p->fwd_groups, p->fwd_pairs ? 1 : 0}].push_back(i);
     }
     for (auto &cl : classes) {
         const std::vector<int> &idx = cl.second;
@@ -817,8 +826,8 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
                 b.total += proj_task_blocks(p->g, it.view_count);
                 smem = std::max(smem, proj_smem_bytes(p->g.nv, p->g.nx, p->g.ny, p->fwd_groups, p->fwd_rows));
             }
-            if ((e = launch_proj_batch(method == CTSIM_PROJ_DD ? kDD : kTF, cl.first.second, cl.first.first, smem, b,
-                                       st)) != cudaSuccess)
+            if ((e = launch_proj_batch(method == CTSIM_PROJ_DD ? kDD : kTF, cl.first[1], cl.first[0], cl.first[2] != 0,
+                                       smem, b, st)) != cudaSuccess)
                 return cuda_fail(e, "batched forward projection");
         }
     }

@@ -22,11 +22,14 @@ cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const
                                  const uint8_t *map, float *image, int view_count, int qcap, int *err,
                                  cudaStream_t st);
 
-cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, cudaStream_t st);
+// pairs: the (X, slope) layout of the column prefix sums (forward_pairs below)
+cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, bool pairs, cudaStream_t st);
 
-cudaError_t launch_proj(int method, int groups, int rows, const Geom &g, const View *views, const float *xs,
-                        const float *ampv, const uint8_t *map, void *proj, int out_dtype, int view_begin,
-                        int view_stride, int view_count, float margin, cudaStream_t st);
+cudaError_t launch_proj(int method, int groups, int rows, bool pairs, const Geom &g, const View *views,
+                        const float *xs, const float *ampv, const uint8_t *map, void *proj, int out_dtype,
+                        int view_begin, int view_stride, int view_count, float margin, cudaStream_t st);
+// The paired prefix layout when it is small enough to stay cache-resident (<= 160 MB).
+inline bool forward_pairs(long long nxy, int nz) { return 8LL * nxy * (nz + 1) <= 160LL * 1024 * 1024; }
 int proj_default_groups(int nv);
 int proj_default_rows(int nv);
 bool proj_groups_valid(int nv, int groups);
@@ -81,7 +84,7 @@ struct BackBatch {
 int proj_task_blocks(const Geom &g, int view_count);
 int back_task_blocks(const Geom &g);
 int proj_row_threads_of(int nv);
-cudaError_t launch_proj_batch(int method, int groups, int row_threads, size_t smem, const ProjBatch &b,
+cudaError_t launch_proj_batch(int method, int groups, int row_threads, bool pairs, size_t smem, const ProjBatch &b,
                               cudaStream_t st);
 cudaError_t launch_back_batch(int method, int mz, bool vec, size_t smem, const BackBatch &b, cudaStream_t st);
 

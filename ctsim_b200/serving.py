@@ -78,7 +78,8 @@ def hbm_footprint(req: ReconRequest) -> int:
     L = 64
     while L < 2 * g.nu - 1:
         L *= 2
-    plan = 4 * g.nx * g.ny * (g.nz + 1) + 4 * pix + 4 * g.nu * g.nv + g.nx * g.ny + 64 * g.noViews + 4096
+    xs = 8 * g.nx * g.ny * (g.nz + 1)  # column prefix sums (paired layout at most)
+    plan = xs + 4 * pix + 4 * g.nu * g.nv + g.nx * g.ny + 64 * g.noViews + 4096
     fdk = 4 * pix + 4 * g.nu * g.nv + 12 * L + 4 * g.nu * g.noViews + 4096
     image = 4 * vox
     if req.kind == "fdk":

@@ -175,6 +175,9 @@ typedef struct {
     int proj_rows;  /* row threads per forward group: a multiple of 32 up to ceil(nv/4) rounded
                        to whole warps; 32 makes each group one warp that walks only the rows
                        of each candidate's shadow */
+    int proj_layout; /* column prefix sums: 1 plain sums, 2 (sum, slope) pairs (one 8-byte load
+                        per evaluation; twice the bytes; plans whose pairs take at most 160 MB
+                        start with 2 and may switch) */
 } ctsim_tuning;
 ctsim_status ctsim_plan_get_tuning(const ctsim_plan *plan, ctsim_tuning *tuning);
 ctsim_status ctsim_plan_set_tuning(ctsim_plan *plan, const ctsim_tuning *tuning);

@@ -180,18 +180,19 @@ def test_launch_shapes_keep_parity_and_autotune():
     plan = Plan(g)
     hpd0 = plan.backproject(yd, "hpd").cpu().numpy()
     for G in (1, 2, 4, 8):
-        same = None
-        for R in (64, 32):  # fewer row threads than rows: passes; 32: walks each candidate's rows
-            try:
-                plan.set_tuning(proj_groups=G, proj_rows=R)
-            except CtsimError:
-                continue
-            for m in ("dd", "tf"):
-                a = plan.project(xd, m).cpu().numpy()
-                assert rel_l2(a, oracle_cbct(f"proj,{m}", g, x)) <= REL_L2
-                if m == "dd":  # the row mapping does not change the arithmetic
-                    assert same is None or np.array_equal(a, same)
-                    same = a
+        for layout in (1, 2):  # plain prefix sums / (sum, slope) pairs
+            same = None
+            for R in (64, 32):  # fewer row threads than rows: passes; 32: walks each candidate's rows
+                try:
+                    plan.set_tuning(proj_groups=G, proj_rows=R, proj_layout=layout)
+                except CtsimError:
+                    continue
+                for m in ("dd", "tf"):
+                    a = plan.project(xd, m).cpu().numpy()
+                    assert rel_l2(a, oracle_cbct(f"proj,{m}", g, x)) <= REL_L2
+                    if m == "dd":  # the row mapping does not change the arithmetic
+                        assert same is None or np.array_equal(a, same)
+                        same = a
     for mz in (1, 2, 4, 8):
         plan.set_tuning(pd_mz=mz)
         assert np.array_equal(plan.backproject(yd, "hpd").cpu().numpy(), hpd0)
