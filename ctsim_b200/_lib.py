@@ -30,7 +30,8 @@ EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd
             "ctsim_simulate_counts", "ctsim_log_attenuation", "ctsim_fbct_geom", "ctsim_fan_plan_create",
             "ctsim_fan_plan_destroy", "ctsim_fan_project", "ctsim_fan_backproject",
             "ctsim_plan_get_tuning", "ctsim_plan_set_tuning", "ctsim_plan_autotune", "ctsim_autotune_clear",
-            "ctsim_batch_project", "ctsim_batch_backproject"]
+            "ctsim_batch_project", "ctsim_batch_backproject", "ctsim_host_cache_release",
+            "ctsim_host_cache_enable"]
 
 
 class CtsimGeom(C.Structure):
@@ -94,6 +95,10 @@ def load():
     L.ctsim_back_pd.restype = C.c_bool
     L.ctsim_cbct_geom.argtypes = [C.c_char_p] + GEOM_ARGS + [_p, _p, _p]
     L.ctsim_cbct_geom.restype = C.c_bool
+    L.ctsim_host_cache_release.argtypes = []
+    L.ctsim_host_cache_release.restype = _i
+    L.ctsim_host_cache_enable.argtypes = [_i]
+    L.ctsim_host_cache_enable.restype = _i
     L.ctsim_plan_create.argtypes = [C.POINTER(CtsimGeom), _p, _p, _p, C.POINTER(_p)]
     L.ctsim_plan_create.restype = _i
     L.ctsim_plan_create_async.argtypes = [C.POINTER(CtsimGeom), _p, _p, _p, _p, C.POINTER(_p)]

@@ -1,5 +1,6 @@
 // C ABI: plans (device-resident geometry tables + scratch) and the drop-in
 // host-pointer entry points that replace the reference's cbct_*_gpu functions.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -386,9 +387,22 @@ static bool dtype_ok(int d) { return d == CTSIM_F32 || d == CTSIM_BF16 || d == C
 static const char *kArcOnlyDD =
     "the arc detector (detector_type 2) is defined for the distance-driven pair only (geom/cbct/cbct_proj3.c)";
 
+static ctsim_status plan_project(ctsim_plan *p, int method, const void *d_image, int image_dtype, void *d_proj,
+                                 int proj_dtype, int view_begin, int view_stride, int view_count, void *stream,
+                                 bool prefix);
+
 extern "C" ctsim_status ctsim_plan_project_ex(ctsim_plan *p, int method, const void *d_image, int image_dtype,
                                               void *d_proj, int proj_dtype, int view_begin, int view_stride,
                                               int view_count, void *stream) {
+    return plan_project(p, method, d_image, image_dtype, d_proj, proj_dtype, view_begin, view_stride, view_count,
+                        stream, true);
+}
+
+// prefix = false reuses the column prefix sums of the previous call on the same image
+// (the host-pointer path projects one image in view chunks).
+static ctsim_status plan_project(ctsim_plan *p, int method, const void *d_image, int image_dtype, void *d_proj,
+                                 int proj_dtype, int view_begin, int view_stride, int view_count, void *stream,
+                                 bool prefix) {
     if (!p || !d_image || !d_proj) return fail(CTSIM_ERR_ARGUMENT, "null argument");
     if (method != CTSIM_PROJ_DD && method != CTSIM_PROJ_TF) return fail(CTSIM_ERR_ARGUMENT, "unknown forward method");
     if (p->g.det == 2 && method != CTSIM_PROJ_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
@@ -398,8 +412,9 @@ extern "C" ctsim_status ctsim_plan_project_ex(ctsim_plan *p, int method, const v
     if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
     cudaStream_t st = (cudaStream_t)stream;
     const int nxy = p->g.nx * p->g.ny;
-    cudaError_t e = launch_prefix(d_image, image_dtype, p->d_xs, nxy, p->g.nz, p->fwd_pairs, st);
-    if (e != cudaSuccess) return cuda_fail(e, "prefix kernel");
+    cudaError_t e;
+    if (prefix && (e = launch_prefix(d_image, image_dtype, p->d_xs, nxy, p->g.nz, p->fwd_pairs, st)) != cudaSuccess)
+        return cuda_fail(e, "prefix kernel");
     e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->fwd_groups, p->fwd_rows, p->fwd_pairs, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
                     proj_dtype, view_begin, view_stride, view_count, p->margin, st);
     if (e != cudaSuccess) return cuda_fail(e, "forward projection kernel");
@@ -456,6 +471,25 @@ extern "C" ctsim_status ctsim_plan_backproject_ex(ctsim_plan *p, int method, con
     return CTSIM_OK;
 }
 
+// A^T (DD or SF) of views [vb, vb + vc) of FP32 d_proj into the FP32 image, scale 1; with
+// accumulate the image holds the sum over the earlier views and the kernel continues it,
+// so a sinogram backprojected chunk by chunk gives the one-pass result bit for bit.
+static ctsim_status plan_back_views(ctsim_plan *p, int method, const float *d_proj, float *d_image, int vb, int vc,
+                                    bool accumulate, cudaStream_t st) {
+    if (p->g.det == 2 && method != CTSIM_BACK_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
+    if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
+    ctsim_status s = check_views(p, vb, 1, vc);
+    if (s != CTSIM_OK) return s;
+    const size_t nuv = (size_t)p->g.nu * p->g.nv;
+    cudaError_t e = launch_prescale(d_proj, CTSIM_F32, p->d_ampv, p->d_ps, nuv, nuv * vc, st);
+    if (e != cudaSuccess) return cuda_fail(e, "prescale kernel");
+    const bool dd = method == CTSIM_BACK_DD;
+    e = launch_back(dd ? kDD : kTF, dd ? p->back_mz : p->back_mz_tf, p->g, p->d_views, p->d_ps, p->d_map, d_image,
+                    CTSIM_F32, vb, 1, vc, 1.0f, dd ? p->back_qcap : p->back_qcap_tf, p->d_err, st, accumulate);
+    if (e != cudaSuccess) return cuda_fail(e, "backprojection kernel");
+    return CTSIM_OK;
+}
+
 extern "C" ctsim_status ctsim_plan_backproject(ctsim_plan *p, int method, const float *d_proj, float *d_image,
                                                int view_begin, int view_stride, int view_count, float scale,
                                                void *stream) {
@@ -479,10 +513,85 @@ extern "C" ctsim_status ctsim_plan_check(ctsim_plan *p) {
 // ---------------------------------------------------------------------------
 namespace {
 
-struct DeviceBuf {
-    void *p = nullptr;
-    ~DeviceBuf() { cudaFree(p); }
+// ---------------------------------------------------------------------------
+// Host-pointer entry points.  Each call is synchronous, as the reference MEX back ends
+// are.  Unlike them, the last geometry's plan, device buffers and streams stay on the
+// device between calls (a reconstruction calls the gateway again and again with one
+// geometry), until the geometry changes or ctsim_host_cache_release; and the forward
+// projection runs in view chunks whose results go back to the host while the next
+// chunk computes.
+// ---------------------------------------------------------------------------
+namespace {
+struct HostCache {
+    std::mutex m;
+    bool enabled = true;
+    int device = -1;
+    ctsim_geom G{};
+    std::vector<double> betas;
+    std::vector<float> couch;
+    std::vector<uint8_t> map;  // empty: no map
+    ctsim_plan *plan = nullptr;
+    void *dimg = nullptr, *dsino = nullptr;
+    cudaStream_t st = nullptr, copy = nullptr;
+    static constexpr int kChunks = 8;
+    cudaEvent_t done[kChunks] = {};
+
+    void release() {
+        int cur = -1;
+        if (device >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != device) cudaSetDevice(device);
+        if (plan) ctsim_plan_destroy(plan);
+        plan = nullptr;
+        cudaFree(dimg);
+        cudaFree(dsino);
+        dimg = dsino = nullptr;
+        for (auto &e : done) {
+            if (e) cudaEventDestroy(e);
+            e = nullptr;
+        }
+        if (st) cudaStreamDestroy(st);
+        if (copy) cudaStreamDestroy(copy);
+        st = copy = nullptr;
+        if (cur >= 0 && cur != device) cudaSetDevice(cur);
+        device = -1;
+    }
+    bool matches(int dev, const ctsim_geom &g, const double *b, const float *c, const bool *mp) const {
+        if (!plan || dev != device || std::memcmp(&g, &G, sizeof(G)) != 0) return false;
+        if (std::memcmp(b, betas.data(), sizeof(double) * g.noviews) || std::memcmp(c, couch.data(), sizeof(float) * g.noviews))
+            return false;
+        if ((mp == nullptr) != map.empty()) return false;
+        if (mp)
+            for (size_t i = 0; i < map.size(); i++)
+                if ((mp[i] ? 1 : 0) != map[i]) return false;
+        return true;
+    }
+    cudaError_t set_up(int dev, const ctsim_geom &g, const double *b, const float *c, const bool *mp, bool *ok) {
+        release();
+        *ok = false;
+        if (ctsim_plan_create(&g, b, c, mp, &plan) != CTSIM_OK) return cudaSuccess;  // message already set
+        const size_t nimg = (size_t)g.nx * g.ny * g.nz, nsino = (size_t)g.nu * g.nv * g.noviews;
+        cudaError_t e;
+        if ((e = cudaMalloc(&dimg, nimg * sizeof(float))) != cudaSuccess ||
+            (e = cudaMalloc(&dsino, nsino * sizeof(float))) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking)) != cudaSuccess)
+            return e;
+        for (auto &ev : done)
+            if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+        device = dev;
+        G = g;
+        betas.assign(b, b + g.noviews);
+        couch.assign(c, c + g.noviews);
+        map.clear();
+        if (mp) {
+            map.resize((size_t)g.nx * g.ny);
+            for (size_t i = 0; i < map.size(); i++) map[i] = mp[i] ? 1 : 0;
+        }
+        *ok = true;
+        return cudaSuccess;
+    }
 };
+HostCache g_host;
+}  // namespace
 
 bool run_host(int method, const ctsim_geom &G, const double *betas, const float *couchz, const bool *map,
               const float *in, float *out) {
@@ -490,40 +599,118 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
         fail(CTSIM_ERR_ARGUMENT, "null argument");
         return false;
     }
-    ctsim_plan *p = nullptr;
-    if (ctsim_plan_create(&G, betas, couchz, map, &p) != CTSIM_OK) return false;
+    std::lock_guard<std::mutex> lock(g_host.m);
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        fail(CTSIM_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+        return false;
+    }
+    if (!g_host.matches(dev, G, betas, couchz, map)) {
+        bool made = false;
+        if ((e = g_host.set_up(dev, G, betas, couchz, map, &made)) != cudaSuccess) {
+            g_host.release();
+            fail(CTSIM_ERR_ALLOC, std::string("device set-up: ") + cudaGetErrorString(e));
+            return false;
+        }
+        if (!made) {
+            g_host.release();
+            return false;
+        }
+    }
+    HostCache &h = g_host;
+    ctsim_plan *p = h.plan;
     const bool fwd = method == CTSIM_PROJ_DD || method == CTSIM_PROJ_TF;
-    const size_t nimg = (size_t)G.nx * G.ny * G.nz, nsino = (size_t)G.nu * G.nv * G.noviews;
-    const size_t nin = fwd ? nimg : nsino, nout = fwd ? nsino : nimg;
-    DeviceBuf din, dout;
-    cudaStream_t st = nullptr;
+    const size_t nimg = (size_t)G.nx * G.ny * G.nz, nuv = (size_t)G.nu * G.nv, nsino = nuv * G.noviews;
     bool ok = false;
-    cudaError_t e;
     do {
-        if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) { cuda_fail(e, "stream"); break; }
-        if ((e = cudaMalloc(&din.p, nin * sizeof(float))) != cudaSuccess ||
-            (e = cudaMalloc(&dout.p, nout * sizeof(float))) != cudaSuccess) {
-            fail(CTSIM_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-            break;
+        if (fwd) {
+            // the image, then the views in chunks; each chunk's sinogram is copied back on the
+            // copy stream while the later chunks compute (the views are independent).  All
+            // chunks are queued before the first copy: a copy to pageable memory returns
+            // only when it has finished.
+            if ((e = cudaMemcpyAsync(h.dimg, in, nimg * sizeof(float), cudaMemcpyHostToDevice, h.st)) != cudaSuccess) {
+                cuda_fail(e, "host to device copy");
+                break;
+            }
+            const int nch = std::min(HostCache::kChunks, G.noviews);
+            auto first_view = [&](int c) { return (int)((long long)G.noviews * c / nch); };
+            ctsim_status s = CTSIM_OK;
+            for (int c = 0; c < nch && s == CTSIM_OK; c++) {
+                const int vb = first_view(c), ve = first_view(c + 1);
+                float *dproj = static_cast<float *>(h.dsino) + (size_t)vb * nuv;
+                s = plan_project(p, method, h.dimg, CTSIM_F32, dproj, CTSIM_F32, vb, 1, ve - vb, h.st, c == 0);
+                if (s == CTSIM_OK && (e = cudaEventRecord(h.done[c], h.st)) != cudaSuccess) s = cuda_fail(e, "event");
+            }
+            for (int c = 0; c < nch && s == CTSIM_OK; c++) {
+                const int vb = first_view(c), ve = first_view(c + 1);
+                if ((e = cudaStreamWaitEvent(h.copy, h.done[c], 0)) != cudaSuccess ||
+                    (e = cudaMemcpyAsync(out + (size_t)vb * nuv, static_cast<float *>(h.dsino) + (size_t)vb * nuv,
+                                         (size_t)(ve - vb) * nuv * sizeof(float), cudaMemcpyDeviceToHost, h.copy)) !=
+                        cudaSuccess)
+                    s = cuda_fail(e, "device to host copy");
+            }
+            if (s != CTSIM_OK) {
+                cudaStreamSynchronize(h.st);
+                cudaStreamSynchronize(h.copy);
+                break;
+            }
+            if ((e = cudaStreamSynchronize(h.copy)) != cudaSuccess || (e = cudaStreamSynchronize(h.st)) != cudaSuccess) {
+                cuda_fail(e, "kernel execution");
+                break;
+            }
+        } else if (method == CTSIM_BACK_DD || method == CTSIM_BACK_TF) {
+            // the sinogram in view chunks on the copy stream; each chunk is backprojected,
+            // continuing the image's view sums, while the next one is copied in
+            const int nch = std::min(HostCache::kChunks, G.noviews);
+            auto first_view = [&](int c) { return (int)((long long)G.noviews * c / nch); };
+            ctsim_status s = CTSIM_OK;
+            for (int c = 0; c < nch && s == CTSIM_OK; c++) {
+                const int vb = first_view(c), ve = first_view(c + 1);
+                float *dproj = static_cast<float *>(h.dsino) + (size_t)vb * nuv;
+                if ((e = cudaMemcpyAsync(dproj, in + (size_t)vb * nuv, (size_t)(ve - vb) * nuv * sizeof(float),
+                                         cudaMemcpyHostToDevice, h.copy)) != cudaSuccess ||
+                    (e = cudaEventRecord(h.done[c], h.copy)) != cudaSuccess ||
+                    (e = cudaStreamWaitEvent(h.st, h.done[c], 0)) != cudaSuccess) {
+                    s = cuda_fail(e, "host to device copy");
+                    break;
+                }
+                s = plan_back_views(p, method, dproj, static_cast<float *>(h.dimg), vb, ve - vb, c > 0, h.st);
+            }
+            if (s != CTSIM_OK) {
+                cudaStreamSynchronize(h.copy);
+                cudaStreamSynchronize(h.st);
+                break;
+            }
+            if ((e = cudaMemcpyAsync(out, h.dimg, nimg * sizeof(float), cudaMemcpyDeviceToHost, h.st)) != cudaSuccess) {
+                cuda_fail(e, "device to host copy");
+                break;
+            }
+            if ((e = cudaStreamSynchronize(h.st)) != cudaSuccess || (e = cudaStreamSynchronize(h.copy)) != cudaSuccess) {
+                cuda_fail(e, "kernel execution");
+                break;
+            }
+        } else {
+            if ((e = cudaMemcpyAsync(h.dsino, in, nsino * sizeof(float), cudaMemcpyHostToDevice, h.st)) != cudaSuccess) {
+                cuda_fail(e, "host to device copy");
+                break;
+            }
+            if (ctsim_plan_backproject(p, method, (const float *)h.dsino, (float *)h.dimg, 0, 1, G.noviews, 1.0f,
+                                       h.st) != CTSIM_OK)
+                break;
+            if ((e = cudaMemcpyAsync(out, h.dimg, nimg * sizeof(float), cudaMemcpyDeviceToHost, h.st)) != cudaSuccess) {
+                cuda_fail(e, "device to host copy");
+                break;
+            }
+            if ((e = cudaStreamSynchronize(h.st)) != cudaSuccess) {
+                cuda_fail(e, "kernel execution");
+                break;
+            }
         }
-        if ((e = cudaMemcpyAsync(din.p, in, nin * sizeof(float), cudaMemcpyHostToDevice, st)) != cudaSuccess) {
-            cuda_fail(e, "host to device copy");
-            break;
-        }
-        ctsim_status s = fwd ? ctsim_plan_project(p, method, (const float *)din.p, (float *)dout.p, 0, 1, G.noviews, st)
-                             : ctsim_plan_backproject(p, method, (const float *)din.p, (float *)dout.p, 0, 1,
-                                                      G.noviews, 1.0f, st);
-        if (s != CTSIM_OK) break;
-        if ((e = cudaMemcpyAsync(out, dout.p, nout * sizeof(float), cudaMemcpyDeviceToHost, st)) != cudaSuccess) {
-            cuda_fail(e, "device to host copy");
-            break;
-        }
-        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) { cuda_fail(e, "kernel execution"); break; }
         if (ctsim_plan_check(p) != CTSIM_OK) break;
         ok = true;
     } while (0);
-    if (st) cudaStreamDestroy(st);
-    ctsim_plan_destroy(p);
+    if (!ok || !h.enabled) h.release();  // after an error, nothing of the failed call is kept
     return ok;
 }
 
@@ -539,6 +726,19 @@ ctsim_geom make_geom(int nx, int ny, int nz, float dx, float dy, float dz, float
 }
 
 }  // namespace
+
+extern "C" ctsim_status ctsim_host_cache_release(void) {
+    std::lock_guard<std::mutex> lock(g_host.m);
+    g_host.release();
+    return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_host_cache_enable(int enabled) {
+    std::lock_guard<std::mutex> lock(g_host.m);
+    g_host.enabled = enabled != 0;
+    if (!g_host.enabled) g_host.release();
+    return CTSIM_OK;
+}
 
 #define CTSIM_GEOM_PARAMS                                                                                        \
     int nx, int ny, int nz, float dx, float dy, float dz, float offset_x, float offset_y, float offset_z, int nu, \

@@ -31,7 +31,7 @@ constexpr unsigned kFull = 0xffffffffu;
 // ---------------------------------------------------------------------------
 // The work of one block (8 columns of one row iy), as a device function: the plain
 // kernel runs it for blockIdx.x, the batched kernel for each of its work items.
-template <int METHOD, int MZ, bool VEC, bool PRESCALED>
+template <int METHOD, int MZ, bool VEC, bool PRESCALED, bool SUM = false>
 __device__ __forceinline__ void back_block(const Geom g, const View *__restrict__ views, const float *__restrict__ ps,
                                            const uint8_t *__restrict__ map, void *__restrict__ image, int out_dtype,
                                            int view_begin, int view_stride, int view_count, float scale, int qcap,
@@ -59,6 +59,14 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
         for (int m = 0; m < MZ; m++) {
             acc[m] = 0.0f;
             izf[m] = (float)(iz0 + lane + 32 * m);
+        }
+        if (SUM) {
+            // continue the per-voxel view sum (scale 1) that the previous view chunk left in
+            // the FP32 image; the sum runs in view order either way
+            const float *src = static_cast<const float *>(image) + (size_t)(iz0 + lane) * nxy + (size_t)iy * g.nx + ix;
+#pragma unroll
+            for (int m = 0; m < MZ; m++)
+                if (lane + 32 * m < izn) acc[m] = src[(size_t)(32 * m) * nxy];
         }
         if (on) {
             for (int k0 = 0; k0 < view_count; k0 += 32) {
@@ -187,15 +195,15 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
 // view in place, geom/cbct/cbct_back.c:196-214), into scratch.
 // Four resident blocks per SM (registers capped at 64): measured on B200 at config 2,
 // DD 110 -> 100 ms and SF 143 -> 104 ms against the uncapped 80-118 registers.
-template <int METHOD, int MZ, bool VEC, bool PRESCALED = true>
+template <int METHOD, int MZ, bool VEC, bool PRESCALED = true, bool SUM = false>
 __global__ void __launch_bounds__(256, 4) back_kernel(Geom g, const View *__restrict__ views,
                                                    const float *__restrict__ ps, const uint8_t *__restrict__ map,
                                                    void *__restrict__ image, int out_dtype, int view_begin,
                                                    int view_stride, int view_count, float scale, int qcap,
                                                    int *__restrict__ err, const float *__restrict__ ampv) {
     extern __shared__ float smem[];
-    back_block<METHOD, MZ, VEC, PRESCALED>(g, views, ps, map, image, out_dtype, view_begin, view_stride, view_count,
-                                           scale, qcap, err, ampv, smem, blockIdx.x);
+    back_block<METHOD, MZ, VEC, PRESCALED, SUM>(g, views, ps, map, image, out_dtype, view_begin, view_stride,
+                                                view_count, scale, qcap, err, ampv, smem, blockIdx.x);
 }
 
 __global__ void prescale_kernel(const void *__restrict__ proj, int in_dtype, const float *__restrict__ ampv,
@@ -660,13 +668,13 @@ cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes) {
 
 size_t back_smem_bytes(int qcap) { return (size_t)8 * (32 * 17 + 2 * qcap) * sizeof(float); }
 
-template <int METHOD, int MZ, bool VEC>
+template <int METHOD, int MZ, bool VEC, bool SUM>
 static cudaError_t launch_back_mz(const Geom &g, const View *views, const float *ps, const uint8_t *map,
                                   void *image, int out_dtype, int vb, int vs, int vc, float scale, int qcap,
                                   int *err, cudaStream_t st) {
     const int blocks = g.ny * ((g.nx + 7) / 8);
     const size_t sm = back_smem_bytes(qcap);
-    auto kfn = back_kernel<METHOD, MZ, VEC>;
+    auto kfn = back_kernel<METHOD, MZ, VEC, true, SUM>;
     cudaError_t e = allow_dynamic_smem((const void *)kfn, sm);
     if (e != cudaSuccess) return e;
     kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap, err, nullptr);
@@ -683,14 +691,23 @@ cudaError_t launch_prescale(const void *proj, int in_dtype, const float *ampv, f
 
 cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *ps, const uint8_t *map,
                         void *image, int out_dtype, int vb, int vs, int vc, float scale, int qcap, int *err,
-                        cudaStream_t st) {
+                        cudaStream_t st, bool accumulate) {
+    if (accumulate && (out_dtype != kF32 || scale != 1.0f)) return cudaErrorInvalidValue;
     const bool vec = (g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(ps) % 16) == 0;
+    // accumulate: the image holds the FP32 view sum of earlier views, which the kernel
+    // continues (separate instantiations, so the plain kernel keeps its registers)
 #define CTSIM_BACK_CASE(M, Z)                                                                                      \
-    if (method == M && mz == Z)                                                                                    \
-        return vec ? launch_back_mz<M, Z, true>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap, err, \
-                                                st)                                                                \
-                   : launch_back_mz<M, Z, false>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap,     \
-                                                 err, st);
+    if (method == M && mz == Z) {                                                                                  \
+        if (accumulate)                                                                                            \
+            return vec ? launch_back_mz<M, Z, true, true>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale,  \
+                                                          qcap, err, st)                                           \
+                       : launch_back_mz<M, Z, false, true>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, \
+                                                           qcap, err, st);                                         \
+        return vec ? launch_back_mz<M, Z, true, false>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale,     \
+                                                       qcap, err, st)                                              \
+                   : launch_back_mz<M, Z, false, false>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale,    \
+                                                        qcap, err, st);                                            \
+    }
     CTSIM_BACK_CASE(kDD, 1) CTSIM_BACK_CASE(kDD, 2) CTSIM_BACK_CASE(kDD, 4) CTSIM_BACK_CASE(kDD, 8)
     CTSIM_BACK_CASE(kTF, 1) CTSIM_BACK_CASE(kTF, 2) CTSIM_BACK_CASE(kTF, 4) CTSIM_BACK_CASE(kTF, 8)
 #undef CTSIM_BACK_CASE

@@ -122,6 +122,16 @@ bool ctsim_cbct_geom(const char *type, int nx, int ny, int nz, float dx, float d
                      float offset_v, float sad, float add, float sdd, int noviews, const double *betas,
                      const float *couchz, int detector_type, const float *data, float *out, const bool *map);
 
+/* The drop-in entry points above keep the last geometry's plan, device buffers and streams
+ * between calls (same device, geometry scalars, betas, couchz and map: reused; anything
+ * else: rebuilt), and return the forward projection to the host in view chunks while the
+ * later chunks compute.  No reference counterpart (the reference MEX back ends allocate
+ * and free per call).  Results do not depend on the cache. */
+/* Frees the kept plan, buffers and streams now. */
+ctsim_status ctsim_host_cache_release(void);
+/* enabled = 0: free after every call, as the reference does; 1 (the default): keep. */
+ctsim_status ctsim_host_cache_enable(int enabled);
+
 /* ---------------------------------------------------------------------------
  * Family 2: device-resident plans.
  * ------------------------------------------------------------------------- */

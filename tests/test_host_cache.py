@@ -1,0 +1,80 @@
+"""The host-pointer entry points keep the last geometry's plan and buffers between calls
+and return the forward projection in view chunks.  Neither may change a result: every
+call must equal a fresh, uncached call and the device-plan path bit for bit."""
+import numpy as np
+import pytest
+
+from cases import KINDS, case_inputs, make_cases
+from ctsim_b200 import CTGeometry, circular_betas
+from ctsim_b200 import _lib
+from ctsim_b200.projector import Plan, cbct_geom_mex
+
+pytestmark = pytest.mark.gpu
+
+
+def mex(kind, g, data):
+    return cbct_geom_mex(kind, g.reconSize, g.reconSpacing, g.reconOffset, g.detSize, g.detSpacing, g.detOffset,
+                         g.SAD, g.ADD, g.SDD, g.noViews, g.betas, g.couchZ, g.flatPanel, data, g.map)
+
+
+def _geom(views, offset=0.0, turn=0.0, map=None):
+    return CTGeometry((96, 80, 24), (1.0, 1.0, 1.0), (0.5, -0.25, 0), (160, 40), (1.2, 1.2), (offset, 0), 1000.0,
+                      500.0, 1500.0, circular_betas(views) + turn, map=map)
+
+
+def _uncached(kind, g, data):
+    L = _lib.load()
+    L.ctsim_host_cache_enable(0)
+    try:
+        return mex(kind, g, data)
+    finally:
+        L.ctsim_host_cache_enable(1)
+
+
+@pytest.mark.parametrize("views", [1, 5, 37])
+def test_cached_calls_equal_uncached_and_plan(views):
+    import torch
+    g = _geom(views)
+    x, y = case_inputs(g, seed=views)
+    plan = Plan(g)
+    _lib.load().ctsim_host_cache_release()
+    for kind in KINDS:
+        src = x if kind.startswith("proj") else y
+        fresh = _uncached(kind, g, src)
+        first = mex(kind, g, src)   # builds the cache (or reuses it from the previous kind)
+        again = mex(kind, g, src)   # reuses it
+        assert np.array_equal(first, fresh), kind
+        assert np.array_equal(again, fresh), kind
+        method = kind.split(",")[1]
+        if kind.startswith("proj"):
+            dev = plan.project(torch.from_numpy(x).cuda(), method).cpu().numpy()
+        else:
+            dev = plan.backproject(torch.from_numpy(y).cuda(), method).cpu().numpy()
+        assert np.array_equal(first, dev), kind
+    plan.close()
+
+
+def test_geometry_change_rebuilds():
+    """Alternating geometries (views, a detector offset, betas, a map) never serve a
+    result from the other geometry's tables."""
+    m = np.ones((80, 96), dtype=bool)
+    m[:10] = False
+    g1, g2, g3, g4, g5 = _geom(12), _geom(12, offset=1.5), _geom(13), _geom(12, turn=0.01), _geom(12, map=m)
+    x, _ = case_inputs(g1, seed=2)
+    want = {id(g): _uncached("proj,dd", g, x) for g in (g1, g2, g3, g4, g5)}
+    assert not np.array_equal(want[id(g1)], want[id(g2)])
+    assert not np.array_equal(want[id(g1)], want[id(g4)])
+    assert not np.array_equal(want[id(g1)], want[id(g5)])
+    for g in (g1, g2, g1, g3, g3, g4, g1, g5, g1):
+        assert np.array_equal(mex("proj,dd", g, x), want[id(g)])
+    _lib.load().ctsim_host_cache_release()
+    assert np.array_equal(mex("proj,dd", g1, x), want[id(g1)])
+
+
+@pytest.mark.parametrize("name", ["ragged", "offsets_curved"])
+def test_reference_cases_through_the_cache(name):
+    g = make_cases()[name]
+    x, y = case_inputs(g, seed=9)
+    for kind in KINDS:
+        src = x if kind.startswith("proj") else y
+        assert np.array_equal(mex(kind, g, src), _uncached(kind, g, src)), (name, kind)
