@@ -471,21 +471,34 @@ extern "C" ctsim_status ctsim_plan_backproject_ex(ctsim_plan *p, int method, con
     return CTSIM_OK;
 }
 
+// Column prefix sums of an FP32 image for the forward projection of a later plan_project
+// with prefix = false.
+static ctsim_status plan_prefix(ctsim_plan *p, int method, const void *d_image, cudaStream_t st) {
+    if (method != CTSIM_PROJ_DD && method != CTSIM_PROJ_TF) return fail(CTSIM_ERR_ARGUMENT, "unknown forward method");
+    if (p->g.det == 2 && method != CTSIM_PROJ_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
+    if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
+    const cudaError_t e = launch_prefix(d_image, CTSIM_F32, p->d_xs, p->g.nx * p->g.ny, p->g.nz, p->fwd_pairs, st);
+    return e == cudaSuccess ? CTSIM_OK : cuda_fail(e, "prefix kernel");
+}
+
 // A^T (DD or SF) of views [vb, vb + vc) of FP32 d_proj into the FP32 image, scale 1; with
 // accumulate the image holds the sum over the earlier views and the kernel continues it,
 // so a sinogram backprojected chunk by chunk gives the one-pass result bit for bit.
 static ctsim_status plan_back_views(ctsim_plan *p, int method, const float *d_proj, float *d_image, int vb, int vc,
-                                    bool accumulate, cudaStream_t st) {
+                                    bool accumulate, cudaStream_t st, bool prescale = true, int y_begin = 0,
+                                    int y_end = -1) {
     if (p->g.det == 2 && method != CTSIM_BACK_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
     if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
     ctsim_status s = check_views(p, vb, 1, vc);
     if (s != CTSIM_OK) return s;
     const size_t nuv = (size_t)p->g.nu * p->g.nv;
-    cudaError_t e = launch_prescale(d_proj, CTSIM_F32, p->d_ampv, p->d_ps, nuv, nuv * vc, st);
-    if (e != cudaSuccess) return cuda_fail(e, "prescale kernel");
+    cudaError_t e;
+    if (prescale && (e = launch_prescale(d_proj, CTSIM_F32, p->d_ampv, p->d_ps, nuv, nuv * vc, st)) != cudaSuccess)
+        return cuda_fail(e, "prescale kernel");
     const bool dd = method == CTSIM_BACK_DD;
     e = launch_back(dd ? kDD : kTF, dd ? p->back_mz : p->back_mz_tf, p->g, p->d_views, p->d_ps, p->d_map, d_image,
-                    CTSIM_F32, vb, 1, vc, 1.0f, dd ? p->back_qcap : p->back_qcap_tf, p->d_err, st, accumulate);
+                    CTSIM_F32, vb, 1, vc, 1.0f, dd ? p->back_qcap : p->back_qcap_tf, p->d_err, st, accumulate,
+                    y_begin, y_end);
     if (e != cudaSuccess) return cuda_fail(e, "backprojection kernel");
     return CTSIM_OK;
 }
@@ -532,9 +545,11 @@ struct HostCache {
     std::vector<uint8_t> map;  // empty: no map
     ctsim_plan *plan = nullptr;
     void *dimg = nullptr, *dsino = nullptr;
-    cudaStream_t st = nullptr, copy = nullptr;
-    static constexpr int kChunks = 8;
-    cudaEvent_t done[kChunks] = {};
+    cudaStream_t st = nullptr, st2 = nullptr, copy = nullptr;
+    static constexpr int kChunks = 8;  // view chunks of a call
+    static constexpr int kSlabs = 4;   // y slabs of the last backprojection chunk
+    cudaEvent_t done[kChunks + kSlabs] = {};
+    cudaEvent_t ready = nullptr;
 
     void release() {
         int cur = -1;
@@ -548,9 +563,11 @@ struct HostCache {
             if (e) cudaEventDestroy(e);
             e = nullptr;
         }
-        if (st) cudaStreamDestroy(st);
-        if (copy) cudaStreamDestroy(copy);
-        st = copy = nullptr;
+        if (ready) cudaEventDestroy(ready);
+        ready = nullptr;
+        for (cudaStream_t s : {st, st2, copy})
+            if (s) cudaStreamDestroy(s);
+        st = st2 = copy = nullptr;
         if (cur >= 0 && cur != device) cudaSetDevice(cur);
         device = -1;
     }
@@ -573,7 +590,9 @@ struct HostCache {
         if ((e = cudaMalloc(&dimg, nimg * sizeof(float))) != cudaSuccess ||
             (e = cudaMalloc(&dsino, nsino * sizeof(float))) != cudaSuccess ||
             (e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess ||
-            (e = cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking)) != cudaSuccess)
+            (e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming)) != cudaSuccess)
             return e;
         for (auto &ev : done)
             if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return e;
@@ -625,22 +644,27 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
     bool ok = false;
     do {
         if (fwd) {
-            // the image, then the views in chunks; each chunk's sinogram is copied back on the
-            // copy stream while the later chunks compute (the views are independent).  All
-            // chunks are queued before the first copy: a copy to pageable memory returns
-            // only when it has finished.
+            // the image and its column prefix sums, then the views in chunks on two compute
+            // streams (one chunk's tail overlaps the next one's start); each chunk's sinogram is
+            // copied back on the copy stream while later chunks compute (the views are
+            // independent).  All chunks are queued before the first copy: a copy to pageable
+            // memory returns only when it has finished.
             if ((e = cudaMemcpyAsync(h.dimg, in, nimg * sizeof(float), cudaMemcpyHostToDevice, h.st)) != cudaSuccess) {
                 cuda_fail(e, "host to device copy");
                 break;
             }
+            ctsim_status s = plan_prefix(p, method, h.dimg, h.st);
+            if (s == CTSIM_OK && ((e = cudaEventRecord(h.ready, h.st)) != cudaSuccess ||
+                                  (e = cudaStreamWaitEvent(h.st2, h.ready, 0)) != cudaSuccess))
+                s = cuda_fail(e, "event");
             const int nch = std::min(HostCache::kChunks, G.noviews);
             auto first_view = [&](int c) { return (int)((long long)G.noviews * c / nch); };
-            ctsim_status s = CTSIM_OK;
             for (int c = 0; c < nch && s == CTSIM_OK; c++) {
                 const int vb = first_view(c), ve = first_view(c + 1);
+                cudaStream_t sc = (c & 1) ? h.st2 : h.st;
                 float *dproj = static_cast<float *>(h.dsino) + (size_t)vb * nuv;
-                s = plan_project(p, method, h.dimg, CTSIM_F32, dproj, CTSIM_F32, vb, 1, ve - vb, h.st, c == 0);
-                if (s == CTSIM_OK && (e = cudaEventRecord(h.done[c], h.st)) != cudaSuccess) s = cuda_fail(e, "event");
+                s = plan_project(p, method, h.dimg, CTSIM_F32, dproj, CTSIM_F32, vb, 1, ve - vb, sc, false);
+                if (s == CTSIM_OK && (e = cudaEventRecord(h.done[c], sc)) != cudaSuccess) s = cuda_fail(e, "event");
             }
             for (int c = 0; c < nch && s == CTSIM_OK; c++) {
                 const int vb = first_view(c), ve = first_view(c + 1);
@@ -650,20 +674,21 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
                         cudaSuccess)
                     s = cuda_fail(e, "device to host copy");
             }
-            if (s != CTSIM_OK) {
-                cudaStreamSynchronize(h.st);
-                cudaStreamSynchronize(h.copy);
-                break;
-            }
-            if ((e = cudaStreamSynchronize(h.copy)) != cudaSuccess || (e = cudaStreamSynchronize(h.st)) != cudaSuccess) {
+            const cudaError_t e1 = cudaStreamSynchronize(h.st), e2 = cudaStreamSynchronize(h.st2),
+                              e3 = cudaStreamSynchronize(h.copy);
+            if (s != CTSIM_OK) break;
+            if ((e = e1) != cudaSuccess || (e = e2) != cudaSuccess || (e = e3) != cudaSuccess) {
                 cuda_fail(e, "kernel execution");
                 break;
             }
         } else if (method == CTSIM_BACK_DD || method == CTSIM_BACK_TF) {
             // the sinogram in view chunks on the copy stream; each chunk is backprojected,
-            // continuing the image's view sums, while the next one is copied in
+            // continuing the image's view sums, while the next one is copied in.  The last
+            // chunk runs in y slabs, and each finished slab goes back to the host while the
+            // next one computes (voxels are independent).
             const int nch = std::min(HostCache::kChunks, G.noviews);
             auto first_view = [&](int c) { return (int)((long long)G.noviews * c / nch); };
+            auto first_row = [&](int k) { return (int)((long long)G.ny * k / HostCache::kSlabs); };
             ctsim_status s = CTSIM_OK;
             for (int c = 0; c < nch && s == CTSIM_OK; c++) {
                 const int vb = first_view(c), ve = first_view(c + 1);
@@ -675,18 +700,31 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
                     s = cuda_fail(e, "host to device copy");
                     break;
                 }
-                s = plan_back_views(p, method, dproj, static_cast<float *>(h.dimg), vb, ve - vb, c > 0, h.st);
+                if (c + 1 < nch) {
+                    s = plan_back_views(p, method, dproj, static_cast<float *>(h.dimg), vb, ve - vb, c > 0, h.st);
+                    continue;
+                }
+                for (int k = 0; k < HostCache::kSlabs && s == CTSIM_OK; k++) {
+                    s = plan_back_views(p, method, dproj, static_cast<float *>(h.dimg), vb, ve - vb, c > 0, h.st,
+                                        k == 0, first_row(k), first_row(k + 1));
+                    if (s == CTSIM_OK && (e = cudaEventRecord(h.done[HostCache::kChunks + k], h.st)) != cudaSuccess)
+                        s = cuda_fail(e, "event");
+                }
             }
-            if (s != CTSIM_OK) {
-                cudaStreamSynchronize(h.copy);
-                cudaStreamSynchronize(h.st);
-                break;
+            const size_t plane = (size_t)G.nx * G.ny;
+            for (int k = 0; k < HostCache::kSlabs && s == CTSIM_OK; k++) {
+                const int y0 = first_row(k), y1 = first_row(k + 1);
+                if (y1 == y0) continue;
+                if ((e = cudaStreamWaitEvent(h.copy, h.done[HostCache::kChunks + k], 0)) != cudaSuccess ||
+                    (e = cudaMemcpy2DAsync(out + (size_t)y0 * G.nx, plane * sizeof(float),
+                                           static_cast<float *>(h.dimg) + (size_t)y0 * G.nx, plane * sizeof(float),
+                                           (size_t)(y1 - y0) * G.nx * sizeof(float), G.nz, cudaMemcpyDeviceToHost,
+                                           h.copy)) != cudaSuccess)
+                    s = cuda_fail(e, "device to host copy");
             }
-            if ((e = cudaMemcpyAsync(out, h.dimg, nimg * sizeof(float), cudaMemcpyDeviceToHost, h.st)) != cudaSuccess) {
-                cuda_fail(e, "device to host copy");
-                break;
-            }
-            if ((e = cudaStreamSynchronize(h.st)) != cudaSuccess || (e = cudaStreamSynchronize(h.copy)) != cudaSuccess) {
+            const cudaError_t e1 = cudaStreamSynchronize(h.st), e2 = cudaStreamSynchronize(h.copy);
+            if (s != CTSIM_OK) break;
+            if ((e = e1) != cudaSuccess || (e = e2) != cudaSuccess) {
                 cuda_fail(e, "kernel execution");
                 break;
             }

@@ -200,10 +200,11 @@ __global__ void __launch_bounds__(256, 4) back_kernel(Geom g, const View *__rest
                                                    const float *__restrict__ ps, const uint8_t *__restrict__ map,
                                                    void *__restrict__ image, int out_dtype, int view_begin,
                                                    int view_stride, int view_count, float scale, int qcap,
-                                                   int *__restrict__ err, const float *__restrict__ ampv) {
+                                                   int *__restrict__ err, const float *__restrict__ ampv,
+                                                   int block_base) {
     extern __shared__ float smem[];
     back_block<METHOD, MZ, VEC, PRESCALED, SUM>(g, views, ps, map, image, out_dtype, view_begin, view_stride,
-                                                view_count, scale, qcap, err, ampv, smem, blockIdx.x);
+                                                view_count, scale, qcap, err, ampv, smem, block_base + blockIdx.x);
 }
 
 __global__ void prescale_kernel(const void *__restrict__ proj, int in_dtype, const float *__restrict__ ampv,
@@ -671,13 +672,16 @@ size_t back_smem_bytes(int qcap) { return (size_t)8 * (32 * 17 + 2 * qcap) * siz
 template <int METHOD, int MZ, bool VEC, bool SUM>
 static cudaError_t launch_back_mz(const Geom &g, const View *views, const float *ps, const uint8_t *map,
                                   void *image, int out_dtype, int vb, int vs, int vc, float scale, int qcap,
-                                  int *err, cudaStream_t st) {
-    const int blocks = g.ny * ((g.nx + 7) / 8);
+                                  int *err, int y_begin, int y_end, cudaStream_t st) {
+    const int tiles_x = (g.nx + 7) / 8;
+    const int blocks = (y_end - y_begin) * tiles_x;
+    if (blocks <= 0) return cudaSuccess;
     const size_t sm = back_smem_bytes(qcap);
     auto kfn = back_kernel<METHOD, MZ, VEC, true, SUM>;
     cudaError_t e = allow_dynamic_smem((const void *)kfn, sm);
     if (e != cudaSuccess) return e;
-    kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap, err, nullptr);
+    kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap, err, nullptr,
+                                 y_begin * tiles_x);
     return cudaGetLastError();
 }
 
@@ -691,22 +695,24 @@ cudaError_t launch_prescale(const void *proj, int in_dtype, const float *ampv, f
 
 cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *ps, const uint8_t *map,
                         void *image, int out_dtype, int vb, int vs, int vc, float scale, int qcap, int *err,
-                        cudaStream_t st, bool accumulate) {
+                        cudaStream_t st, bool accumulate, int y_begin, int y_end) {
     if (accumulate && (out_dtype != kF32 || scale != 1.0f)) return cudaErrorInvalidValue;
+    if (y_end < 0) y_end = g.ny;
+    if (y_begin < 0 || y_end > g.ny || y_begin > y_end) return cudaErrorInvalidValue;
     const bool vec = (g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(ps) % 16) == 0;
     // accumulate: the image holds the FP32 view sum of earlier views, which the kernel
     // continues (separate instantiations, so the plain kernel keeps its registers)
-#define CTSIM_BACK_CASE(M, Z)                                                                                      \
-    if (method == M && mz == Z) {                                                                                  \
-        if (accumulate)                                                                                            \
-            return vec ? launch_back_mz<M, Z, true, true>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale,  \
-                                                          qcap, err, st)                                           \
-                       : launch_back_mz<M, Z, false, true>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, \
-                                                           qcap, err, st);                                         \
-        return vec ? launch_back_mz<M, Z, true, false>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale,     \
-                                                       qcap, err, st)                                              \
-                   : launch_back_mz<M, Z, false, false>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale,    \
-                                                        qcap, err, st);                                            \
+#define CTSIM_BACK_CASE(M, Z)                                                                            \
+    if (method == M && mz == Z) {                                                                        \
+        if (accumulate)                                                                                  \
+            return vec ? launch_back_mz<M, Z, true, true>(g, views, ps, map, image, out_dtype, vb, vs, vc, \
+                                                          scale, qcap, err, y_begin, y_end, st)          \
+                       : launch_back_mz<M, Z, false, true>(g, views, ps, map, image, out_dtype, vb, vs,  \
+                                                           vc, scale, qcap, err, y_begin, y_end, st);    \
+        return vec ? launch_back_mz<M, Z, true, false>(g, views, ps, map, image, out_dtype, vb, vs, vc,  \
+                                                       scale, qcap, err, y_begin, y_end, st)             \
+                   : launch_back_mz<M, Z, false, false>(g, views, ps, map, image, out_dtype, vb, vs, vc, \
+                                                        scale, qcap, err, y_begin, y_end, st);           \
     }
     CTSIM_BACK_CASE(kDD, 1) CTSIM_BACK_CASE(kDD, 2) CTSIM_BACK_CASE(kDD, 4) CTSIM_BACK_CASE(kDD, 8)
     CTSIM_BACK_CASE(kTF, 1) CTSIM_BACK_CASE(kTF, 2) CTSIM_BACK_CASE(kTF, 4) CTSIM_BACK_CASE(kTF, 8)
@@ -811,7 +817,7 @@ static cudaError_t launch_back_unscaled_mz(const Geom &g, const View *views, con
     auto kfn = back_kernel<METHOD, MZ, false, false>;
     cudaError_t e = allow_dynamic_smem((const void *)kfn, sm);
     if (e != cudaSuccess) return e;
-    kfn<<<blocks, 256, sm, st>>>(g, views, proj, map, image, kF32, 0, 1, vc, 1.0f, qcap, err, ampv);
+    kfn<<<blocks, 256, sm, st>>>(g, views, proj, map, image, kF32, 0, 1, vc, 1.0f, qcap, err, ampv, 0);
     return cudaGetLastError();
 }
 

@@ -16,7 +16,8 @@ cudaError_t launch_prescale(const void *proj, int in_dtype, const float *ampv, f
 
 cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *ps, const uint8_t *map,
                         void *image, int out_dtype, int view_begin, int view_stride, int view_count, float scale,
-                        int qcap, int *err, cudaStream_t st, bool accumulate = false);
+                        int qcap, int *err, cudaStream_t st, bool accumulate = false, int y_begin = 0,
+                        int y_end = -1);
 size_t back_smem_bytes(int qcap);
 cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const float *proj, const float *ampv,
                                  const uint8_t *map, float *image, int view_count, int qcap, int *err,

@@ -17,8 +17,8 @@ def mex(kind, g, data):
                          g.SAD, g.ADD, g.SDD, g.noViews, g.betas, g.couchZ, g.flatPanel, data, g.map)
 
 
-def _geom(views, offset=0.0, turn=0.0, map=None):
-    return CTGeometry((96, 80, 24), (1.0, 1.0, 1.0), (0.5, -0.25, 0), (160, 40), (1.2, 1.2), (offset, 0), 1000.0,
+def _geom(views, offset=0.0, turn=0.0, map=None, size=(96, 80, 24)):
+    return CTGeometry(size, (1.0, 1.0, 1.0), (0.5, -0.25, 0), (160, 40), (1.2, 1.2), (offset, 0), 1000.0,
                       500.0, 1500.0, circular_betas(views) + turn, map=map)
 
 
@@ -31,10 +31,13 @@ def _uncached(kind, g, data):
         L.ctsim_host_cache_enable(1)
 
 
-@pytest.mark.parametrize("views", [1, 5, 37])
-def test_cached_calls_equal_uncached_and_plan(views):
+@pytest.mark.parametrize("views,size", [(1, (96, 80, 24)), (5, (96, 80, 24)), (37, (96, 80, 24)),
+                                        (11, (7, 3, 40))])
+def test_cached_calls_equal_uncached_and_plan(views, size):
+    """Chunks of one view, fewer views than chunks, uneven chunks; fewer image rows than
+    y slabs."""
     import torch
-    g = _geom(views)
+    g = _geom(views, size=size)
     x, y = case_inputs(g, seed=views)
     plan = Plan(g)
     _lib.load().ctsim_host_cache_release()
