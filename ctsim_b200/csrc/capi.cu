@@ -1074,7 +1074,7 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
 
 extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_item *items, int n, void *stream) {
     ctsim_status s = batch_check(method, items, n, false);
-    if (s != CTSIM_OK) return s;
+    if (s != CTSIM_OK || n == 0) return s;
     cudaStream_t st = (cudaStream_t)stream;
     const bool dd = method == CTSIM_BACK_DD;
     cudaError_t e;
@@ -1085,9 +1085,24 @@ extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_it
             cudaSuccess)
             return cuda_fail(e, "prescale kernel");
     }
+    // An item of at least four waves of the single-plan kernel gains nothing from sharing a
+    // launch and runs on that kernel (64 registers, four blocks per SM, against up to 128
+    // registers in the batched one, whose task table is indexed at run time); the same
+    // block body computes every voxel, so the images do not change.
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, items[0].plan->device);
+    const int large = 4 * 4 * sms;
     std::map<std::pair<int, bool>, std::vector<int>> classes;  // (z blocks per lane, float4 rows)
     for (int i = 0; i < n; i++) {
-        const ctsim_plan *p = items[i].plan;
+        const ctsim_batch_item &it = items[i];
+        const ctsim_plan *p = it.plan;
+        if (back_task_blocks(p->g) >= large) {
+            if ((e = launch_back(dd ? kDD : kTF, dd ? p->back_mz : p->back_mz_tf, p->g, p->d_views, p->d_ps, p->d_map,
+                                 it.out, CTSIM_F32, it.view_begin, it.view_stride, it.view_count, it.scale,
+                                 dd ? p->back_qcap : p->back_qcap_tf, p->d_err, st)) != cudaSuccess)
+                return cuda_fail(e, "backprojection kernel");
+            continue;
+        }
         const bool vec = (p->g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(p->d_ps) % 16) == 0;
         classes[{dd ? p->back_mz : p->back_mz_tf, vec}].push_back(i);
     }

@@ -52,13 +52,14 @@ def test_batched_launches_equal_per_plan_calls(method):
 @pytest.mark.parametrize("method", ["dd", "tf"])
 def test_batched_backprojection_with_different_row_buffers(method):
     """Plans whose A^T row buffers differ (detector height and magnification) in one
-    persistent grid, with ragged column tiles (nx not a multiple of 8)."""
+    persistent grid, with ragged column tiles (nx not a multiple of 8); the 160 x 162
+    image (over four waves of the single-plan kernel) runs on that kernel instead."""
     import torch
     from ctsim_b200 import CTGeometry, Plan, circular_betas
     from ctsim_b200.projector import batch_backproject
     ents, refs = [], []
     for k, (n, nz, nv, dz) in enumerate([(21, 40, 96, 1.0), (19, 8, 24, 1.0), (27, 60, 200, 0.5), (13, 20, 48, 2.0),
-                                         (30, 33, 140, 1.0), (17, 70, 260, 0.7)]):
+                                         (30, 33, 140, 1.0), (17, 70, 260, 0.7), (160, 16, 48, 1.0)]):
         g = CTGeometry((n, n + 2, nz), (1.0, 1.0, dz), (0, 0, 0), (40, nv), (1.6, 1.0), (0, 0), 1000.0, 500.0, 1500.0,
                        circular_betas(9 + k))
         p = Plan(g)
