@@ -54,7 +54,7 @@ class CtsimTuning(C.Structure):
 
 class CtsimBatchItem(C.Structure):
     _fields_ = [("plan", _p), ("in_", _p), ("out", _p), ("view_begin", _i), ("view_stride", _i),
-                ("view_count", _i), ("scale", _f)]
+                ("view_count", _i), ("scale", _f), ("in_dtype", _i), ("out_dtype", _i)]
 
 
 class CtsimError(RuntimeError):

@@ -1008,6 +1008,7 @@ static ctsim_status batch_check(int method, const ctsim_batch_item *items, int n
     for (int i = 0; i < n; i++) {
         const ctsim_batch_item &it = items[i];
         if (!it.plan || !it.in || !it.out) return fail(CTSIM_ERR_ARGUMENT, "null plan or buffer in the batch");
+        if (!dtype_ok(it.in_dtype) || !dtype_ok(it.out_dtype)) return fail(CTSIM_ERR_ARGUMENT, "unknown storage type");
         if (!it.plan->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, it.plan->fwd_reason);
         if (it.plan->g.det == 2 && method != (fwd ? CTSIM_PROJ_DD : CTSIM_BACK_DD))
             return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
@@ -1029,15 +1030,15 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
     // column prefix sums of every image (each plan's own scratch)
     for (int i = 0; i < n; i++) {
         const ctsim_plan *p = items[i].plan;
-        if ((e = launch_prefix(items[i].in, CTSIM_F32, p->d_xs, p->g.nx * p->g.ny, p->g.nz, p->fwd_pairs, st)) !=
-            cudaSuccess)
+        if ((e = launch_prefix(items[i].in, items[i].in_dtype, p->d_xs, p->g.nx * p->g.ny, p->g.nz, p->fwd_pairs,
+                               st)) != cudaSuccess)
             return cuda_fail(e, "prefix kernel");
     }
     // one persistent launch per launch-shape class (row threads, candidate groups)
-    std::map<std::vector<int>, std::vector<int>> classes;  // (row threads, groups, prefix layout)
+    std::map<std::vector<int>, std::vector<int>> classes;  // (row threads, groups, prefix layout, FP32 out)
     for (int i = 0; i < n; i++) {
         const ctsim_plan *p = items[i].plan;
-        classes[{p->fwd_rows, p->fwd_groups, p->fwd_pairs ? 1 : 0}].push_back(i);
+        classes[{p->fwd_rows, p->fwd_groups, p->fwd_pairs ? 1 : 0, items[i].out_dtype == CTSIM_F32 ? 0 : 1}].push_back(i);
     }
     for (auto &cl : classes) {
         const std::vector<int> &idx = cl.second;
@@ -1055,7 +1056,8 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
                 T.xs = p->d_xs;
                 T.ampv = p->d_ampv;
                 T.map = p->d_map;
-                T.proj = static_cast<float *>(it.out);
+                T.proj = it.out;
+                T.out_dtype = it.out_dtype;
                 T.vb = it.view_begin;
                 T.vs = it.view_stride;
                 T.gx = (p->g.nu + proj_group_width() - 1) / proj_group_width();
@@ -1065,7 +1067,7 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
                 smem = std::max(smem, proj_smem_bytes(p->g.nv, p->g.nx, p->g.ny, p->fwd_groups, p->fwd_rows));
             }
             if ((e = launch_proj_batch(method == CTSIM_PROJ_DD ? kDD : kTF, cl.first[1], cl.first[0], cl.first[2] != 0,
-                                       smem, b, st)) != cudaSuccess)
+                                       cl.first[3] != 0, smem, b, st)) != cudaSuccess)
                 return cuda_fail(e, "batched forward projection");
         }
     }
@@ -1081,8 +1083,8 @@ extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_it
     for (int i = 0; i < n; i++) {  // sinograms times ampv into each plan's scratch
         const ctsim_plan *p = items[i].plan;
         const size_t nuv = (size_t)p->g.nu * p->g.nv;
-        if ((e = launch_prescale(items[i].in, CTSIM_F32, p->d_ampv, p->d_ps, nuv, nuv * items[i].view_count, st)) !=
-            cudaSuccess)
+        if ((e = launch_prescale(items[i].in, items[i].in_dtype, p->d_ampv, p->d_ps, nuv, nuv * items[i].view_count,
+                                 st)) != cudaSuccess)
             return cuda_fail(e, "prescale kernel");
     }
     // An item of at least four waves of the single-plan kernel gains nothing from sharing a
@@ -1092,19 +1094,19 @@ extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_it
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, items[0].plan->device);
     const int large = 4 * 4 * sms;
-    std::map<std::pair<int, bool>, std::vector<int>> classes;  // (z blocks per lane, float4 rows)
+    std::map<std::vector<int>, std::vector<int>> classes;  // (z blocks per lane, float4 rows, FP32 out)
     for (int i = 0; i < n; i++) {
         const ctsim_batch_item &it = items[i];
         const ctsim_plan *p = it.plan;
         if (back_task_blocks(p->g) >= large) {
             if ((e = launch_back(dd ? kDD : kTF, dd ? p->back_mz : p->back_mz_tf, p->g, p->d_views, p->d_ps, p->d_map,
-                                 it.out, CTSIM_F32, it.view_begin, it.view_stride, it.view_count, it.scale,
+                                 it.out, it.out_dtype, it.view_begin, it.view_stride, it.view_count, it.scale,
                                  dd ? p->back_qcap : p->back_qcap_tf, p->d_err, st)) != cudaSuccess)
                 return cuda_fail(e, "backprojection kernel");
             continue;
         }
         const bool vec = (p->g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(p->d_ps) % 16) == 0;
-        classes[{dd ? p->back_mz : p->back_mz_tf, vec}].push_back(i);
+        classes[{dd ? p->back_mz : p->back_mz_tf, vec ? 1 : 0, it.out_dtype == CTSIM_F32 ? 0 : 1}].push_back(i);
     }
     for (auto &cl : classes) {
         const std::vector<int> &idx = cl.second;
@@ -1121,7 +1123,8 @@ extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_it
                 T.views = p->d_views;
                 T.ps = p->d_ps;
                 T.map = p->d_map;
-                T.image = static_cast<float *>(it.out);
+                T.image = it.out;
+                T.out_dtype = it.out_dtype;
                 T.err = p->d_err;
                 T.vb = it.view_begin;
                 T.vs = it.view_stride;
@@ -1132,8 +1135,8 @@ extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_it
                 b.total += back_task_blocks(p->g);
                 qcap = std::max(qcap, T.qcap);
             }
-            if ((e = launch_back_batch(dd ? kDD : kTF, cl.first.first, cl.first.second, back_smem_bytes(qcap), b, st)) !=
-                cudaSuccess)
+            if ((e = launch_back_batch(dd ? kDD : kTF, cl.first[0], cl.first[1] != 0, cl.first[2] != 0,
+                                       back_smem_bytes(qcap), b, st)) != cudaSuccess)
                 return cuda_fail(e, "batched backprojection");
         }
     }

@@ -838,7 +838,8 @@ cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const
 // runs each block's work with its task's tables; the task table is a __grid_constant__
 // kernel parameter, so a batch needs no device allocation and can be graph-captured.
 // ---------------------------------------------------------------------------
-template <int METHOD, int GROUPS, bool PAIRS>
+// LOWP: outputs in each task's storage type; otherwise FP32 (a compile-time store).
+template <int METHOD, int GROUPS, bool PAIRS, bool LOWP>
 __global__ void __launch_bounds__(kProjMaxThreads) proj_batch_kernel(const __grid_constant__ ProjBatch b) {
     extern __shared__ float4 acc4_batch[];
     for (int blk = blockIdx.x; blk < b.total; blk += gridDim.x) {
@@ -849,13 +850,14 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_batch_kernel(const __gri
         }
         const ProjTask &T = b.t[lo];
         const int local = blk - T.first;
-        proj_block<METHOD, GROUPS, PAIRS>(T.g, T.views, T.xs, T.ampv, T.map, T.proj, kF32, T.vb, T.vs, T.margin,
+        proj_block<METHOD, GROUPS, PAIRS>(T.g, T.views, T.xs, T.ampv, T.map, T.proj, LOWP ? T.out_dtype : kF32, T.vb,
+                                          T.vs, T.margin,
                                           acc4_batch, local % T.gx, local / T.gx);
         __syncthreads();  // the next block reuses the shared accumulators
     }
 }
 
-template <int METHOD, int MZ, bool VEC>
+template <int METHOD, int MZ, bool VEC, bool LOWP>
 __global__ void __launch_bounds__(256) back_batch_kernel(const __grid_constant__ BackBatch b) {
     extern __shared__ float smem_batch[];
     for (int blk = blockIdx.x; blk < b.total; blk += gridDim.x) {
@@ -865,8 +867,8 @@ __global__ void __launch_bounds__(256) back_batch_kernel(const __grid_constant__
             if (b.t[mid].first <= blk) lo = mid; else hi = mid - 1;
         }
         const BackTask &T = b.t[lo];
-        back_block<METHOD, MZ, VEC, true>(T.g, T.views, T.ps, T.map, T.image, kF32, T.vb, T.vs, T.vc, T.scale, T.qcap,
-                                          T.err, nullptr, smem_batch, blk - T.first);
+        back_block<METHOD, MZ, VEC, true>(T.g, T.views, T.ps, T.map, T.image, LOWP ? T.out_dtype : kF32, T.vb, T.vs,
+                                          T.vc, T.scale, T.qcap, T.err, nullptr, smem_batch, blk - T.first);
         // the per-warp row buffers are laid out with the task's own stride, so a warp may
         // not start the next item (possibly another task) while its neighbours still work
         __syncthreads();
@@ -886,13 +888,14 @@ static int persistent_grid(K kernel, int threads, size_t smem, int total) {
     return std::max(1, std::min(total, sms * per_sm));
 }
 
-cudaError_t launch_proj_batch(int method, int groups, int row_threads, bool pairs, size_t smem, const ProjBatch &b,
-                              cudaStream_t st) {
+cudaError_t launch_proj_batch(int method, int groups, int row_threads, bool pairs, bool lowp, size_t smem,
+                              const ProjBatch &b, cudaStream_t st) {
     if (b.n < 1 || b.total < 1) return cudaSuccess;
     const int nt = row_threads * groups;
 #define CTSIM_PB_CASE(M, GR)                                                                          \
     if (method == M && groups == GR) {                                                                \
-        auto k = pairs ? proj_batch_kernel<M, GR, true> : proj_batch_kernel<M, GR, false>;            \
+        auto k = pairs ? (lowp ? proj_batch_kernel<M, GR, true, true> : proj_batch_kernel<M, GR, true, false>) \
+                       : (lowp ? proj_batch_kernel<M, GR, false, true> : proj_batch_kernel<M, GR, false, false>); \
         cudaError_t e = allow_dynamic_smem((const void *)k, smem);                                    \
         if (e != cudaSuccess) return e;                                                               \
         k<<<persistent_grid(k, nt, smem, b.total), nt, smem, st>>>(b);                                \
@@ -904,11 +907,12 @@ cudaError_t launch_proj_batch(int method, int groups, int row_threads, bool pair
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_back_batch(int method, int mz, bool vec, size_t smem, const BackBatch &b, cudaStream_t st) {
+cudaError_t launch_back_batch(int method, int mz, bool vec, bool lowp, size_t smem, const BackBatch &b,
+                              cudaStream_t st) {
     if (b.n < 1 || b.total < 1) return cudaSuccess;
 #define CTSIM_BB_CASE(M, Z, V)                                                                        \
     if (method == M && mz == Z && vec == V) {                                                         \
-        auto k = back_batch_kernel<M, Z, V>;                                                          \
+        auto k = lowp ? back_batch_kernel<M, Z, V, true> : back_batch_kernel<M, Z, V, false>;         \
         cudaError_t e = allow_dynamic_smem((const void *)k, smem);                                    \
         if (e != cudaSuccess) return e;                                                               \
         k<<<persistent_grid(k, 256, smem, b.total), 256, smem, st>>>(b);                              \

@@ -57,7 +57,8 @@ struct ProjTask {
     const float *xs;
     const float *ampv;
     const uint8_t *map;
-    float *proj;
+    void *proj;
+    int out_dtype;
     int vb, vs, gx, first;  // view selection, blocks along u, first flat block of the task
     float margin;
 };
@@ -71,7 +72,8 @@ struct BackTask {
     const View *views;
     const float *ps;
     const uint8_t *map;
-    float *image;
+    void *image;
+    int out_dtype;
     int *err;
     int vb, vs, vc, qcap, first;
     float scale;
@@ -85,9 +87,11 @@ struct BackBatch {
 int proj_task_blocks(const Geom &g, int view_count);
 int back_task_blocks(const Geom &g);
 int proj_row_threads_of(int nv);
-cudaError_t launch_proj_batch(int method, int groups, int row_threads, bool pairs, size_t smem, const ProjBatch &b,
+// lowp: some task stores BF16/FP16 (each task's out_dtype); otherwise all store FP32
+cudaError_t launch_proj_batch(int method, int groups, int row_threads, bool pairs, bool lowp, size_t smem,
+                              const ProjBatch &b, cudaStream_t st);
+cudaError_t launch_back_batch(int method, int mz, bool vec, bool lowp, size_t smem, const BackBatch &b,
                               cudaStream_t st);
-cudaError_t launch_back_batch(int method, int mz, bool vec, size_t smem, const BackBatch &b, cudaStream_t st);
 
 // Raises (never lowers) a kernel's dynamic shared-memory limit on the current device.
 cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes);

@@ -345,9 +345,10 @@ def _batch(fn_name, method_id, entries):
     keep = []
     for k, (plan, x, y, vb, vs, vc, scale) in enumerate(entries):
         for t in (x, y):
-            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
-                raise TypeError("batched launches take contiguous float32 CUDA tensors")
-        arr[k] = _lib.CtsimBatchItem(plan._h, x.data_ptr(), y.data_ptr(), int(vb), int(vs), int(vc), float(scale))
+            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype in _DTYPES and t.is_contiguous()):
+                raise TypeError("batched launches take contiguous float32, bfloat16 or float16 CUDA tensors")
+        arr[k] = _lib.CtsimBatchItem(plan._h, x.data_ptr(), y.data_ptr(), int(vb), int(vs), int(vc), float(scale),
+                                     _DTYPES[x.dtype], _DTYPES[y.dtype])
         keep.append(plan)
     st = torch.cuda.current_stream(entries[0][0].device).cuda_stream
     _lib.check(getattr(L, fn_name)(method_id, arr, n, st), fn_name)

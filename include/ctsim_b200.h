@@ -203,7 +203,8 @@ ctsim_status ctsim_autotune_clear(void);
 
 /* Batched launches (no reference counterpart): the distance-driven or separable-footprint
  * A (CTSIM_PROJ_DD/TF) or A^T (CTSIM_BACK_DD/TF) of n plans -- different geometries, one
- * device -- with FP32 device buffers: `in` is the image (A) or the selected views' sinogram
+ * device -- with device buffers of any ctsim_dtype (per item; FP32 arithmetic, as the _ex
+ * plan calls): `in` is the image (A) or the selected views' sinogram
  * (A^T), `out` the sinogram of the selected views or the image (overwritten; A^T times
  * scale).  After the per-plan pre-passes (column prefix sums, or the ampv pre-scaling)
  * the projector blocks of all plans run in ONE persistent grid per launch-shape class
@@ -212,10 +213,11 @@ ctsim_status ctsim_autotune_clear(void);
  * per call.  Results equal the per-plan calls bit for bit. */
 typedef struct {
     ctsim_plan *plan;
-    const float *in;
-    float *out;
+    const void *in;
+    void *out;
     int view_begin, view_stride, view_count;
     float scale;
+    int in_dtype, out_dtype; /* ctsim_dtype of in and out (0: FP32); arithmetic is FP32 */
 } ctsim_batch_item;
 ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *items, int n, void *stream);
 ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_item *items, int n, void *stream);

@@ -119,3 +119,29 @@ def test_batched_pwls_equals_each_solver():
         x_ref, phis, rmsds = reconPwlsSeSqs(y, w, g, 2.0, "huber", 3, 0.01, 4, x0, stopCrt=-1.0)
         assert torch.equal(s.x, x_ref)
         assert np.allclose([h[k][0] for h in hist], phis, rtol=1e-9)
+
+
+@pytest.mark.parametrize("method", ["dd", "tf"])
+def test_batched_low_precision_storage_equals_per_plan_calls(method):
+    """bfloat16 / float16 / float32 buffers per item (FP32 arithmetic): each result equals
+    its plan's own _ex call bit for bit, for A and A^T, in both directions of widening."""
+    import torch
+    from ctsim_b200.projector import batch_backproject, batch_project
+    gp = _plans()[:4]
+    dts = [(torch.bfloat16, torch.float32), (torch.float16, torch.float16), (torch.float32, torch.bfloat16),
+           (torch.bfloat16, torch.bfloat16)]
+    fwd, back, refs = [], [], []
+    for k, ((g, p), (din, dout)) in enumerate(zip(gp, dts)):
+        x, y = case_inputs(g, seed=40 + k)
+        xd = torch.from_numpy(x).cuda().to(din)
+        yd = torch.from_numpy(y).cuda().to(din)
+        so = torch.empty(g.sino_shape, dtype=dout, device="cuda")
+        io = torch.empty(g.image_shape, dtype=dout, device="cuda")
+        fwd.append((p, xd, so, 0, 1, g.noViews))
+        back.append((p, yd, io, 0, 1, g.noViews, 0.5))
+        refs.append((p, xd, yd, dout))
+    batch_project(method, fwd)
+    batch_backproject(method, back)
+    for (p, xd, yd, dout), f, b in zip(refs, fwd, back):
+        assert torch.equal(f[2], p.project(xd, method, out_dtype=dout))
+        assert torch.equal(b[2], p.backproject(yd, method, scale=0.5, out_dtype=dout))
