@@ -531,6 +531,75 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def run_recon(args):
+    """Config-2 reconstructions on the device: reconFDK ('hann' window, crop 1) and OS-SQS
+    PWLS (reconPwlsSeSqs: SF pair, 24 ordered subsets, Huber delta 0.001, beta 5e4) started
+    from the FDK image, from log Poisson data (I0 1e5, counts clamped at 10) with the
+    weights w = counts (computeWeightsPwls(counts, 0, 0)).  FP32; CUDA-event timing of
+    the FDK call, of the PWLS set-up (A 1 and A^T (w A 1), the subset copies) and of the
+    outer iterations (each ends with the host read of phi and rmsd)."""
+    import torch
+    from ctsim_b200.fdk import FDK
+    from ctsim_b200.projector import Plan
+    from ctsim_b200.pwls import PwlsSolver
+    torch.cuda.set_device(0)
+    g, x = make_workload(args.views)
+    plan = Plan(g)
+    xd = torch.from_numpy(x).cuda()
+    with torch.no_grad():
+        p = plan.project(xd, "tf")
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(4321)
+        counts = torch.poisson(1e5 * torch.exp(-p), generator=gen)
+        y = torch.log(1e5 / torch.clamp(counts, min=10.0)).contiguous()
+        w = counts.contiguous()
+        del p
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        r = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(b)
+
+    def rel_rmse(img):
+        return float(torch.sqrt(torch.mean((img - xd) ** 2)) / torch.sqrt(torch.mean(xd ** 2)))
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    f = FDK(g, "hann", 1.0, plan=plan)
+    f(y)
+    torch.cuda.synchronize()
+    fdk_ms = min(timed(lambda: f(y))[1] for _ in range(3))
+    x0 = f(y)
+    solver, setup_ms = timed(lambda: PwlsSolver(y, w, g, 5e4, "huber", 0.001, 24, x0, plan=plan))
+    its = args.iterations
+    phis, rmsds, it_ms = [], [], []
+    for _ in range(its):
+        (phi, rmsd), ms = timed(solver.step)
+        phis.append(phi)
+        rmsds.append(rmsd)
+        it_ms.append(ms)
+    ck = clocks.stop()
+    vv = float(g.nx * g.ny * g.nz * g.noViews)
+    steady = it_ms[1:] if len(it_ms) > 1 else it_ms
+    line = {
+        "metric": "config-2 reconstruction times", "unit": "ms", "impl": "ours", "n_gpus": 1, "dtype": "f32",
+        "higher_is_better": False, "data": "synthetic (seeded 20-ellipsoid phantom, log Poisson data I0=1e5)",
+        "config": {"workload": "reconFDK hann + OS-SQS PWLS (SF, 24 subsets, huber 0.001, beta 5e4)",
+                   "volume": [g.nx, g.ny, g.nz], "views": g.noViews, "detector": [g.nu, g.nv],
+                   "iterations": its},
+        "fdk_ms": fdk_ms, "fdk_gvv_s": vv / (fdk_ms / 1e3) / 1e9,
+        "pwls_setup_ms": setup_ms, "pwls_iteration_ms": float(np.mean(steady)),
+        "pwls_iteration_gvv_s": 2 * vv / (float(np.mean(steady)) / 1e3) / 1e9,
+        "pwls_iteration_ms_each": it_ms, "phi": phis, "rmsd": rmsds,
+        "rel_rmse_vs_phantom": {"fdk": rel_rmse(x0), "pwls": rel_rmse(solver.x)},
+        "clocks": ck,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -552,8 +621,12 @@ def main():
     ap.add_argument("--batch-pwls", dest="batch_pwls", action="store_true",
                     help="serving: batch the OS-PWLS requests per scheduler tick")
     ap.add_argument("--instances", type=int, default=16, help="instances of the batched run")
+    ap.add_argument("--recon", action="store_true", help="config-2 reconFDK and OS-SQS PWLS times")
+    ap.add_argument("--iterations", type=int, default=5, help="OS-SQS iterations of the --recon run")
     args = ap.parse_args()
-    if args.batched:
+    if args.recon:
+        run_recon(args)
+    elif args.batched:
         run_batched(args)
     elif args.serving:
         run_serving(args)
