@@ -1,10 +1,12 @@
 // C ABI: plans (device-resident geometry tables + scratch) and the drop-in
 // host-pointer entry points that replace the reference's cbct_*_gpu functions.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -537,7 +539,6 @@ namespace {
 namespace {
 struct HostCache {
     std::mutex m;
-    bool enabled = true;
     int device = -1;
     ctsim_geom G{};
     std::vector<double> betas;
@@ -609,7 +610,26 @@ struct HostCache {
         return cudaSuccess;
     }
 };
-HostCache g_host;
+// One cache per device, so that threads driving different GPUs neither wait for nor
+// evict each other.
+std::mutex g_host_map_m;
+std::map<int, std::unique_ptr<HostCache>> g_host_by_dev;
+std::atomic<bool> g_host_enabled{true};
+
+HostCache &host_cache(int dev) {
+    std::lock_guard<std::mutex> lock(g_host_map_m);
+    std::unique_ptr<HostCache> &c = g_host_by_dev[dev];
+    if (!c) c.reset(new HostCache);
+    return *c;
+}
+
+void release_host_caches() {
+    std::lock_guard<std::mutex> lock(g_host_map_m);
+    for (auto &kv : g_host_by_dev) {
+        std::lock_guard<std::mutex> l(kv.second->m);
+        kv.second->release();
+    }
+}
 }  // namespace
 
 bool run_host(int method, const ctsim_geom &G, const double *betas, const float *couchz, const bool *map,
@@ -618,26 +638,26 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
         fail(CTSIM_ERR_ARGUMENT, "null argument");
         return false;
     }
-    std::lock_guard<std::mutex> lock(g_host.m);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) {
         fail(CTSIM_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
         return false;
     }
-    if (!g_host.matches(dev, G, betas, couchz, map)) {
+    HostCache &h = host_cache(dev);
+    std::lock_guard<std::mutex> lock(h.m);
+    if (!h.matches(dev, G, betas, couchz, map)) {
         bool made = false;
-        if ((e = g_host.set_up(dev, G, betas, couchz, map, &made)) != cudaSuccess) {
-            g_host.release();
+        if ((e = h.set_up(dev, G, betas, couchz, map, &made)) != cudaSuccess) {
+            h.release();
             fail(CTSIM_ERR_ALLOC, std::string("device set-up: ") + cudaGetErrorString(e));
             return false;
         }
         if (!made) {
-            g_host.release();
+            h.release();
             return false;
         }
     }
-    HostCache &h = g_host;
     ctsim_plan *p = h.plan;
     const bool fwd = method == CTSIM_PROJ_DD || method == CTSIM_PROJ_TF;
     const size_t nimg = (size_t)G.nx * G.ny * G.nz, nuv = (size_t)G.nu * G.nv, nsino = nuv * G.noviews;
@@ -748,7 +768,7 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
         if (ctsim_plan_check(p) != CTSIM_OK) break;
         ok = true;
     } while (0);
-    if (!ok || !h.enabled) h.release();  // after an error, nothing of the failed call is kept
+    if (!ok || !g_host_enabled.load()) h.release();  // after an error, nothing of the failed call is kept
     return ok;
 }
 
@@ -766,15 +786,13 @@ ctsim_geom make_geom(int nx, int ny, int nz, float dx, float dy, float dz, float
 }  // namespace
 
 extern "C" ctsim_status ctsim_host_cache_release(void) {
-    std::lock_guard<std::mutex> lock(g_host.m);
-    g_host.release();
+    release_host_caches();
     return CTSIM_OK;
 }
 
 extern "C" ctsim_status ctsim_host_cache_enable(int enabled) {
-    std::lock_guard<std::mutex> lock(g_host.m);
-    g_host.enabled = enabled != 0;
-    if (!g_host.enabled) g_host.release();
+    g_host_enabled.store(enabled != 0);
+    if (!enabled) release_host_caches();
     return CTSIM_OK;
 }
 

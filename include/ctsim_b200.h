@@ -122,8 +122,8 @@ bool ctsim_cbct_geom(const char *type, int nx, int ny, int nz, float dx, float d
                      float offset_v, float sad, float add, float sdd, int noviews, const double *betas,
                      const float *couchz, int detector_type, const float *data, float *out, const bool *map);
 
-/* The drop-in entry points above keep the last geometry's plan, device buffers and streams
- * between calls (same device, geometry scalars, betas, couchz and map: reused; anything
+/* The drop-in entry points above keep, per device, the last geometry's plan, device buffers
+ * and streams between calls (same geometry scalars, betas, couchz and map: reused; anything
  * else: rebuilt), and return the forward projection to the host in view chunks while the
  * later chunks compute.  No reference counterpart (the reference MEX back ends allocate
  * and free per call).  Results do not depend on the cache. */

@@ -81,3 +81,22 @@ def test_reference_cases_through_the_cache(name):
     for kind in KINDS:
         src = x if kind.startswith("proj") else y
         assert np.array_equal(mex(kind, g, src), _uncached(kind, g, src)), (name, kind)
+
+
+def test_threads_with_different_geometries():
+    """Threads calling the drop-in functions at once, each with its own geometry, on one
+    device: every result equals the uncached one."""
+    from concurrent.futures import ThreadPoolExecutor
+    gs = [_geom(9), _geom(10, offset=0.5), _geom(9, turn=0.2)]
+    x, y = case_inputs(gs[0], seed=4)
+    want = [(_uncached("proj,dd", g, x), _uncached("back,tf", g, case_inputs(g, seed=4)[1])) for g in gs]
+
+    def work(k):
+        g = gs[k % len(gs)]
+        yk = case_inputs(g, seed=4)[1]
+        return k, [(mex("proj,dd", g, x), mex("back,tf", g, yk)) for _ in range(3)]
+
+    with ThreadPoolExecutor(4) as ex:
+        for k, outs in ex.map(work, range(8)):
+            for a, b in outs:
+                assert np.array_equal(a, want[k % len(gs)][0]) and np.array_equal(b, want[k % len(gs)][1]), k
