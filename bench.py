@@ -573,7 +573,8 @@ def run_recon(args):
     torch.cuda.synchronize()
     fdk_ms = min(timed(lambda: f(y))[1] for _ in range(3))
     x0 = f(y)
-    solver, setup_ms = timed(lambda: PwlsSolver(y, w, g, 5e4, "huber", 0.001, 24, x0, plan=plan))
+    solver, setup_ms = timed(lambda: PwlsSolver(y, w, g, 5e4, "huber", 0.001, 24, x0, plan=plan,
+                                                autotune=args.autotune))
     its = args.iterations
     phis, rmsds, it_ms = [], [], []
     for _ in range(its):
@@ -589,7 +590,7 @@ def run_recon(args):
         "higher_is_better": False, "data": "synthetic (seeded 20-ellipsoid phantom, log Poisson data I0=1e5)",
         "config": {"workload": "reconFDK hann + OS-SQS PWLS (SF, 24 subsets, huber 0.001, beta 5e4)",
                    "volume": [g.nx, g.ny, g.nz], "views": g.noViews, "detector": [g.nu, g.nv],
-                   "iterations": its},
+                   "iterations": its, "autotune": bool(args.autotune), "tuning": plan.tuning},
         "fdk_ms": fdk_ms, "fdk_gvv_s": vv / (fdk_ms / 1e3) / 1e9,
         "pwls_setup_ms": setup_ms, "pwls_iteration_ms": float(np.mean(steady)),
         "pwls_iteration_gvv_s": 2 * vv / (float(np.mean(steady)) / 1e3) / 1e9,
