@@ -41,6 +41,24 @@ def rank_info():
             int(os.environ.get("WORLD_SIZE", "1")))
 
 
+def max_over_ranks(ms: float, dist: bool, device) -> float:
+    """The slowest rank's time: every rank of a replica run calls this in the same order
+    (an all-reduce with MAX); a single process returns its own."""
+    if not dist:
+        return ms
+    import torch
+    import torch.distributed as td
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(vv_per_step: float, steps: int, world: int, total_ms: float) -> float:
+    """Whole-job GVoxel-views/s: every rank runs `steps` A + A^T steps of `vv_per_step`
+    voxel-views each, and the job takes the slowest rank's `total_ms`."""
+    return 2.0 * vv_per_step * steps * world / (total_ms / 1e3) / 1e9
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -262,12 +280,9 @@ def run_ours(args):
     total_ms = start.elapsed_time(end)
     t_a = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
     t_b = float(np.mean([e[1].elapsed_time(e[2]) for e in ev]))
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, dev)
     ms_per_step = total_ms / K
-    value = 2.0 * vv * K * world / (total_ms / 1e3) / 1e9
+    value = replica_value(vv, K, world, total_ms)
 
     # roofline of the dominant kernel (streaming model: every view reads the volume and writes/reads its view)
     peak, peak_src = measured_peaks()
@@ -333,7 +348,6 @@ def run_ours(args):
 
 
 def run_e2e(e2e_step, K, dist, dev, vv, world):
-    import torch
     e2e_step()
     ke = max(2, min(K, 5))
     if dist:
@@ -342,12 +356,8 @@ def run_e2e(e2e_step, K, dist, dev, vv, world):
     t0 = time.perf_counter()
     for _ in range(ke):
         e2e_step()
-    e2e_s = (time.perf_counter() - t0) / ke
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    return 2.0 * vv * world / e2e_s / 1e9, e2e_s
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / ke * 1e3, dist, dev) / 1e3
+    return replica_value(vv, 1, world, e2e_s * 1e3), e2e_s
 
 
 def extras(plan, xd, yd, sino, img, vv):
