@@ -541,6 +541,91 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_gpu(args):
+    """The reference's own CUDA distance-driven pair (geom/dd_cuda: cbct_proj_dd_gpu and
+    cbct_back_dd_gpu, compiled unmodified for sm_100a into oracle/_ref) on this GPU, through
+    its synchronous host-pointer drivers, beside this project's drop-in host-pointer calls
+    on the same inputs: one A and one A^T each, wall clock (both APIs are synchronous and
+    include their host copies).  The two outputs are compared; the reference's GPU code
+    is not the parity target (its CPU C is) and differs from it at the volume's z edges."""
+    import ctypes as C
+    import torch
+    from ctsim_b200 import _lib
+    from oracle.bindings import refgpu_available, refgpu_cbct
+    rank, local, world = rank_info()
+    if rank != 0:
+        return
+    if not refgpu_available():
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref/librefgpu_dd.so was not built"}))
+        return
+    torch.cuda.set_device(0)
+    g, x = make_workload(args.views)
+    rng = np.random.default_rng(3)
+    y = rng.random(g.sino_shape, dtype=np.float32)
+    from dataclasses import replace
+    warm = replace(g, betas=g.betas[:2].copy(), couchZ=g.couchZ[:2].copy())
+    refgpu_cbct("proj,dd", warm, x)
+    refgpu_cbct("back,dd", warm, y[:2])
+    t0 = time.perf_counter()
+    ref_a = refgpu_cbct("proj,dd", g, x)
+    t1 = time.perf_counter()
+    ref_at = refgpu_cbct("back,dd", g, y)
+    t2 = time.perf_counter()
+    L = _lib.load()
+    betas, couch, mp = np.ascontiguousarray(g.betas), np.ascontiguousarray(g.couchZ), np.ascontiguousarray(g.map)
+    ours_a = np.empty(g.sino_shape, np.float32)
+    ours_at = np.empty(g.image_shape, np.float32)
+    sc = g.scalars()
+
+    def ours():
+        ok = L.ctsim_proj_dd(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, x.ctypes.data,
+                             ours_a.ctypes.data, mp.ctypes.data)
+        ok = ok and L.ctsim_back_dd(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, ours_at.ctypes.data,
+                                    y.ctypes.data, mp.ctypes.data)
+        if not ok:
+            raise RuntimeError(_lib.last_error())
+
+    ours()
+    t3 = time.perf_counter()
+    ours()
+    t4 = time.perf_counter()
+
+    def rel(a, b):
+        a64, b64 = a.astype(np.float64), b.astype(np.float64)
+        return float(np.linalg.norm(a64 - b64) / max(np.linalg.norm(b64), 1e-300))
+
+    # against the parity target, the reference's CPU C, on two views of the same volume
+    from oracle.bindings import ref_available, ref_cbct
+    cpu_check = None
+    if ref_available():
+        g2 = replace(g, betas=g.betas[:2].copy(), couchZ=g.couchZ[:2].copy())
+        y2 = np.ascontiguousarray(y[:2])
+        nthr = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        cpu_a = ref_cbct("proj,dd", g2, x, nthreads=2)
+        cpu_at = ref_cbct("back,dd", g2, y2, nthreads=min(2, nthr))
+        ours_at2 = np.empty(g2.image_shape, np.float32)
+        b2, c2 = np.ascontiguousarray(g2.betas), np.ascontiguousarray(g2.couchZ)
+        if not L.ctsim_back_dd(*g2.scalars(), b2.ctypes.data, c2.ctypes.data, g2.flatPanel, ours_at2.ctypes.data,
+                               y2.ctypes.data, mp.ctypes.data):
+            raise RuntimeError(_lib.last_error())
+        cpu_check = {"views": 2,
+                     "A": {"ours": rel(ours_a[:2], cpu_a), "reference_gpu": rel(ref_a[:2], cpu_a)},
+                     "A^T": {"ours": rel(ours_at2, cpu_at),
+                             "reference_gpu": rel(refgpu_cbct("back,dd", g2, y2), cpu_at)}}
+    vv = float(g.nx * g.ny * g.nz * g.noViews)
+    line = {"metric": METRIC, "impl": "reference-gpu", "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "value": 2 * vv / (t2 - t0) / 1e9, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"DD A + A^T, {g.nx}x{g.ny}x{g.nz}, {g.noViews} views, {g.nu}x{g.nv} detector",
+                       "api": "host pointers, synchronous (cbct_proj_dd_gpu / cbct_back_dd_gpu)"},
+            "reference_gpu_ms": {"A": (t1 - t0) * 1e3, "A^T": (t2 - t1) * 1e3},
+            "ours_host_pointer_ms": {"A+A^T": (t4 - t3) * 1e3},
+            "ours_host_pointer_value": 2 * vv / (t4 - t3) / 1e9,
+            "speedup": (t2 - t0) / (t4 - t3),
+            "rel_l2_reference_gpu_vs_ours": {"A": rel(ref_a, ours_a), "A^T": rel(ref_at, ours_at)},
+            "rel_l2_vs_reference_cpu": cpu_check}
+    print(json.dumps(line), flush=True)
+
+
 def run_recon(args):
     """Config-2 reconstructions on the device: reconFDK ('hann' window, crop 1) and OS-SQS
     PWLS (reconPwlsSeSqs: SF pair, 24 ordered subsets, Huber delta 0.001, beta 5e4) started
@@ -633,9 +718,13 @@ def main():
                     help="serving: batch the OS-PWLS requests per scheduler tick")
     ap.add_argument("--instances", type=int, default=16, help="instances of the batched run")
     ap.add_argument("--recon", action="store_true", help="config-2 reconFDK and OS-SQS PWLS times")
+    ap.add_argument("--reference-gpu", dest="reference_gpu", action="store_true",
+                    help="the reference's own CUDA DD pair on this GPU beside the drop-in calls")
     ap.add_argument("--iterations", type=int, default=5, help="OS-SQS iterations of the --recon run")
     args = ap.parse_args()
-    if args.recon:
+    if args.reference_gpu:
+        run_reference_gpu(args)
+    elif args.recon:
         run_recon(args)
     elif args.batched:
         run_batched(args)

@@ -5,6 +5,8 @@
                       (single-threaded, or over view chunks with ``nthreads``)
 * ``ref3_cbct``    -> the reference's arc-detector DD pair (geom/cbct/cbct_proj3.c,
                       cbct_back3.c), ``_ref/libcbct_ref3.so``
+* ``refgpu_cbct``  -> the reference's CUDA DD pair (geom/dd_cuda), ``_ref/librefgpu_dd.so``:
+                      a timing baseline on the GPU, not a parity target
 
 Both take and return numpy arrays in the package conventions
 (image ``[nz, ny, nx]``, sino ``[noViews, nu, nv]``, float32).
@@ -22,6 +24,7 @@ ORACLE_SO = os.path.join(HERE, "_build", "libcbct_oracle.so")
 ORACLE64_SO = os.path.join(HERE, "_build", "libcbct_oracle64.so")
 REF_SO = os.path.join(HERE, "_ref", "libcbct_ref.so")
 REF3_SO = os.path.join(HERE, "_ref", "libcbct_ref3.so")
+REFGPU_SO = os.path.join(HERE, "_ref", "librefgpu_dd.so")
 
 KINDS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3,
          "back,pd": 4, "back,hpd": 5, "back,var": 6}
@@ -56,6 +59,10 @@ def _load(path):
         elif path == REF3_SO:
             lib.ref3_cbct_call.argtypes = [_i] + _GEOM_ARGS
             lib.ref3_cbct_call.restype = _i
+        elif path == REFGPU_SO:
+            for fn in (lib.refgpu_proj_dd, lib.refgpu_back_dd):
+                fn.argtypes = _GEOM_ARGS
+                fn.restype = C.c_bool
         else:
             lib.ref_cbct_call.argtypes = [_i] + _GEOM_ARGS
             lib.ref_cbct_call.restype = _i
@@ -131,6 +138,29 @@ def ref3_cbct(kind: str, geom, data) -> np.ndarray:
     data, out, args, keep = _prep(kind, geom, data)
     if not lib.ref3_cbct_call(KINDS[kind], *args):
         raise RuntimeError("reference call failed")
+    return out
+
+
+def refgpu_available() -> bool:
+    return os.path.exists(REFGPU_SO)
+
+
+def refgpu_cbct(kind: str, geom, data) -> np.ndarray:
+    """The reference's own GPU drivers cbct_proj_dd_gpu / cbct_back_dd_gpu
+    (geom/dd_cuda/cbct_dd_proj.c:407, cbct_dd_back.c:299) on the current CUDA device:
+    host arrays in and out, synchronous."""
+    if kind not in ("proj,dd", "back,dd"):
+        raise ValueError("the reference GPU build covers proj,dd and back,dd")
+    lib = _load(REFGPU_SO)
+    data, out, args, keep = _prep(kind, geom, data)
+    if kind == "proj,dd":
+        ok = lib.refgpu_proj_dd(*args)
+    else:  # the driver takes (image, proj): the output image first
+        a = list(args)
+        a[-3], a[-2] = a[-2], a[-3]
+        ok = lib.refgpu_back_dd(*a)
+    if not ok:
+        raise RuntimeError("reference GPU call failed")
     return out
 
 
