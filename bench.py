@@ -612,6 +612,36 @@ def run_reference_gpu(args):
                      "A": {"ours": rel(ours_a[:2], cpu_a), "reference_gpu": rel(ref_a[:2], cpu_a)},
                      "A^T": {"ours": rel(ours_at2, cpu_at),
                              "reference_gpu": rel(refgpu_cbct("back,dd", g2, y2), cpu_at)}}
+    # FDK back,hpd: the reference's cbct_back_pd_gpu against the drop-in ctsim_back_pd
+    fdk = None
+    from oracle.bindings import REFGPU_PD_SO
+    if os.path.exists(REFGPU_PD_SO):
+        refgpu_cbct("back,hpd", warm, y[:2])
+        t5 = time.perf_counter()
+        ref_pd = refgpu_cbct("back,hpd", g, y)
+        t6 = time.perf_counter()
+        ours_pd = np.empty(g.image_shape, np.float32)
+
+        def ours_hpd():
+            if not L.ctsim_back_pd(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, ours_pd.ctypes.data,
+                                   y.ctypes.data, mp.ctypes.data, False):
+                raise RuntimeError(_lib.last_error())
+
+        ours_hpd()
+        t7 = time.perf_counter()
+        ours_hpd()
+        t8 = time.perf_counter()
+        fdk = {"reference_gpu_ms": (t6 - t5) * 1e3, "ours_host_pointer_ms": (t8 - t7) * 1e3,
+               "speedup": (t6 - t5) / (t8 - t7), "rel_l2_reference_gpu_vs_ours": rel(ref_pd, ours_pd)}
+        if ref_available():
+            cpu_pd = ref_cbct("back,hpd", g2, y2)  # one thread: the reference's own summation order
+            ours_pd2 = np.empty(g2.image_shape, np.float32)
+            if not L.ctsim_back_pd(*g2.scalars(), b2.ctypes.data, c2.ctypes.data, g2.flatPanel,
+                                   ours_pd2.ctypes.data, y2.ctypes.data, mp.ctypes.data, False):
+                raise RuntimeError(_lib.last_error())
+            fdk["vs_reference_cpu_2_views"] = {"ours_bit_identical": bool(np.array_equal(ours_pd2, cpu_pd)),
+                                               "ours": rel(ours_pd2, cpu_pd),
+                                               "reference_gpu": rel(refgpu_cbct("back,hpd", g2, y2), cpu_pd)}
     vv = float(g.nx * g.ny * g.nz * g.noViews)
     line = {"metric": METRIC, "impl": "reference-gpu", "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
             "value": 2 * vv / (t2 - t0) / 1e9, "dtype": "f32", "data": "synthetic",
@@ -622,7 +652,7 @@ def run_reference_gpu(args):
             "ours_host_pointer_value": 2 * vv / (t4 - t3) / 1e9,
             "speedup": (t2 - t0) / (t4 - t3),
             "rel_l2_reference_gpu_vs_ours": {"A": rel(ref_a, ours_a), "A^T": rel(ref_at, ours_at)},
-            "rel_l2_vs_reference_cpu": cpu_check}
+            "rel_l2_vs_reference_cpu": cpu_check, "fdk_back_hpd": fdk}
     print(json.dumps(line), flush=True)
 
 

@@ -25,6 +25,7 @@ ORACLE64_SO = os.path.join(HERE, "_build", "libcbct_oracle64.so")
 REF_SO = os.path.join(HERE, "_ref", "libcbct_ref.so")
 REF3_SO = os.path.join(HERE, "_ref", "libcbct_ref3.so")
 REFGPU_SO = os.path.join(HERE, "_ref", "librefgpu_dd.so")
+REFGPU_PD_SO = os.path.join(HERE, "_ref", "librefgpu_pd.so")
 
 KINDS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3,
          "back,pd": 4, "back,hpd": 5, "back,var": 6}
@@ -63,6 +64,9 @@ def _load(path):
             for fn in (lib.refgpu_proj_dd, lib.refgpu_back_dd):
                 fn.argtypes = _GEOM_ARGS
                 fn.restype = C.c_bool
+        elif path == REFGPU_PD_SO:
+            lib.refgpu_back_pd.argtypes = _GEOM_ARGS + [C.c_bool]
+            lib.refgpu_back_pd.restype = C.c_bool
         else:
             lib.ref_cbct_call.argtypes = [_i] + _GEOM_ARGS
             lib.ref_cbct_call.restype = _i
@@ -147,18 +151,21 @@ def refgpu_available() -> bool:
 
 def refgpu_cbct(kind: str, geom, data) -> np.ndarray:
     """The reference's own GPU drivers cbct_proj_dd_gpu / cbct_back_dd_gpu
-    (geom/dd_cuda/cbct_dd_proj.c:407, cbct_dd_back.c:299) on the current CUDA device:
-    host arrays in and out, synchronous."""
-    if kind not in ("proj,dd", "back,dd"):
-        raise ValueError("the reference GPU build covers proj,dd and back,dd")
-    lib = _load(REFGPU_SO)
+    (geom/dd_cuda/cbct_dd_proj.c:407, cbct_dd_back.c:299) and cbct_back_pd_gpu
+    (geom/fdk_cuda/cbct_back_pd.c:230) on the current CUDA device: host arrays in and
+    out, synchronous."""
+    if kind not in ("proj,dd", "back,dd", "back,pd", "back,hpd"):
+        raise ValueError("the reference GPU builds cover proj,dd, back,dd, back,pd and back,hpd")
     data, out, args, keep = _prep(kind, geom, data)
-    if kind == "proj,dd":
-        ok = lib.refgpu_proj_dd(*args)
-    else:  # the driver takes (image, proj): the output image first
-        a = list(args)
+    a = list(args)
+    if kind != "proj,dd":  # the back drivers take (image, proj): the output image first
         a[-3], a[-2] = a[-2], a[-3]
-        ok = lib.refgpu_back_dd(*a)
+    if kind == "proj,dd":
+        ok = _load(REFGPU_SO).refgpu_proj_dd(*a)
+    elif kind == "back,dd":
+        ok = _load(REFGPU_SO).refgpu_back_dd(*a)
+    else:
+        ok = _load(REFGPU_PD_SO).refgpu_back_pd(*a, kind == "back,pd")
     if not ok:
         raise RuntimeError("reference GPU call failed")
     return out
