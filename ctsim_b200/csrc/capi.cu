@@ -490,9 +490,14 @@ static ctsim_status plan_back_views(ctsim_plan *p, int method, const float *d_pr
                                     bool accumulate, cudaStream_t st, bool prescale = true, int y_begin = 0,
                                     int y_end = -1) {
     if (p->g.det == 2 && method != CTSIM_BACK_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
-    if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
     ctsim_status s = check_views(p, vb, 1, vc);
     if (s != CTSIM_OK) return s;
+    if (method == CTSIM_BACK_PD || method == CTSIM_BACK_HPD) {  // FP32 sinogram read as it is; no y slabs
+        const cudaError_t e = launch_pd(method == CTSIM_BACK_PD ? kPdOff : kPdClamp, p->pd_mz, p->g, p->d_views,
+                                        d_proj, p->d_map, d_image, CTSIM_F32, vb, 1, vc, 1.0f, st, accumulate);
+        return e == cudaSuccess ? CTSIM_OK : cuda_fail(e, "backprojection kernel");
+    }
+    if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
     const size_t nuv = (size_t)p->g.nu * p->g.nv;
     cudaError_t e;
     if (prescale && (e = launch_prescale(d_proj, CTSIM_F32, p->d_ampv, p->d_ps, nuv, nuv * vc, st)) != cudaSuccess)
@@ -701,11 +706,13 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
                 cuda_fail(e, "kernel execution");
                 break;
             }
-        } else if (method == CTSIM_BACK_DD || method == CTSIM_BACK_TF) {
+        } else if (method == CTSIM_BACK_DD || method == CTSIM_BACK_TF || method == CTSIM_BACK_PD ||
+                   method == CTSIM_BACK_HPD) {
             // the sinogram in view chunks on the copy stream; each chunk is backprojected,
-            // continuing the image's view sums, while the next one is copied in.  The last
-            // chunk runs in y slabs, and each finished slab goes back to the host while the
-            // next one computes (voxels are independent).
+            // continuing the image's view sums, while the next one is copied in.  For DD/SF
+            // the last chunk runs in y slabs, and each finished slab goes back to the host
+            // while the next one computes (voxels are independent).
+            const bool slabs = method == CTSIM_BACK_DD || method == CTSIM_BACK_TF;
             const int nch = std::min(HostCache::kChunks, G.noviews);
             auto first_view = [&](int c) { return (int)((long long)G.noviews * c / nch); };
             auto first_row = [&](int k) { return (int)((long long)G.ny * k / HostCache::kSlabs); };
@@ -720,7 +727,7 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
                     s = cuda_fail(e, "host to device copy");
                     break;
                 }
-                if (c + 1 < nch) {
+                if (c + 1 < nch || !slabs) {
                     s = plan_back_views(p, method, dproj, static_cast<float *>(h.dimg), vb, ve - vb, c > 0, h.st);
                     continue;
                 }
@@ -732,7 +739,10 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
                 }
             }
             const size_t plane = (size_t)G.nx * G.ny;
-            for (int k = 0; k < HostCache::kSlabs && s == CTSIM_OK; k++) {
+            if (!slabs && s == CTSIM_OK &&
+                (e = cudaMemcpyAsync(out, h.dimg, nimg * sizeof(float), cudaMemcpyDeviceToHost, h.st)) != cudaSuccess)
+                s = cuda_fail(e, "device to host copy");
+            for (int k = 0; slabs && k < HostCache::kSlabs && s == CTSIM_OK; k++) {
                 const int y0 = first_row(k), y1 = first_row(k + 1);
                 if (y1 == y0) continue;
                 if ((e = cudaStreamWaitEvent(h.copy, h.done[HostCache::kChunks + k], 0)) != cudaSuccess ||

@@ -539,7 +539,9 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
 // by lane j for view k0+j and broadcast; every voxel accumulates the views in the
 // reference's order with its exact float operations.
 // ---------------------------------------------------------------------------
-template <int MODE, int MZ>
+// SUM: the FP32 image holds the view sum of earlier view chunks (scale 1), which the
+// kernel continues in the same view order (separate instantiations).
+template <int MODE, int MZ, bool SUM = false>
 __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict__ views,
                                                  const float *__restrict__ proj, const uint8_t *__restrict__ map,
                                                  void *__restrict__ image, int out_dtype, int view_begin,
@@ -562,6 +564,12 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
         for (int m = 0; m < MZ; m++) {
             acc[m] = 0.0f;
             zc0[m] = fmul(fadd((float)(iz0 + lane + 32 * m), g.wz_pd), g.dz);  // (iz + wz) * dz, cbct_back.c:100
+        }
+        if (SUM) {
+            const float *src = static_cast<const float *>(image) + (size_t)(iz0 + lane) * nxy + (size_t)iy * g.nx + ix;
+#pragma unroll
+            for (int m = 0; m < MZ; m++)
+                if (lane + 32 * m < izn) acc[m] = src[(size_t)(32 * m) * nxy];
         }
         if (on) {
             for (int k0 = 0; k0 < view_count; k0 += 32) {
@@ -782,16 +790,23 @@ cudaError_t launch_proj(int method, int groups, int rows, bool pairs, const Geom
 
 template <int MODE, int MZ>
 static cudaError_t launch_pd_mz(const Geom &g, const View *views, const float *proj, const uint8_t *map,
-                                void *image, int out_dtype, int vb, int vs, int vc, float scale, cudaStream_t st) {
+                                void *image, int out_dtype, int vb, int vs, int vc, float scale, bool accumulate,
+                                cudaStream_t st) {
     const int blocks = g.ny * ((g.nx + 7) / 8);
-    pd_kernel<MODE, MZ><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale);
+    if (accumulate)
+        pd_kernel<MODE, MZ, true><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale);
+    else
+        pd_kernel<MODE, MZ><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pd(int mode, int mz, const Geom &g, const View *views, const float *proj, const uint8_t *map,
-                      void *image, int out_dtype, int vb, int vs, int vc, float scale, cudaStream_t st) {
-#define CTSIM_PD_CASE(O, Z) \
-    if (mode == O && mz == Z) return launch_pd_mz<O, Z>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale, st);
+                      void *image, int out_dtype, int vb, int vs, int vc, float scale, cudaStream_t st,
+                      bool accumulate) {
+    if (accumulate && (out_dtype != kF32 || scale != 1.0f)) return cudaErrorInvalidValue;
+#define CTSIM_PD_CASE(O, Z)                                                                                    \
+    if (mode == O && mz == Z)                                                                                  \
+        return launch_pd_mz<O, Z>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale, accumulate, st);
     CTSIM_PD_CASE(kPdOff, 1) CTSIM_PD_CASE(kPdOff, 2) CTSIM_PD_CASE(kPdOff, 4) CTSIM_PD_CASE(kPdOff, 8)
     CTSIM_PD_CASE(kPdClamp, 1) CTSIM_PD_CASE(kPdClamp, 2) CTSIM_PD_CASE(kPdClamp, 4) CTSIM_PD_CASE(kPdClamp, 8)
     CTSIM_PD_CASE(kPdVar, 1) CTSIM_PD_CASE(kPdVar, 2) CTSIM_PD_CASE(kPdVar, 4) CTSIM_PD_CASE(kPdVar, 8)

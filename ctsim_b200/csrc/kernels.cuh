@@ -42,7 +42,7 @@ size_t proj_smem_bytes(int nv, int nx, int ny, int groups, int rows);
 enum PdMode { kPdOff = 0, kPdClamp = 1, kPdVar = 2 };
 cudaError_t launch_pd(int mode, int mz, const Geom &g, const View *views, const float *proj,
                       const uint8_t *map, void *image, int out_dtype, int view_begin, int view_stride,
-                      int view_count, float scale, cudaStream_t st);
+                      int view_count, float scale, cudaStream_t st, bool accumulate = false);
 
 cudaError_t launch_scale(float *y, size_t n, float s, cudaStream_t st);
 
