@@ -537,9 +537,8 @@ namespace {
 // Host-pointer entry points.  Each call is synchronous, as the reference MEX back ends
 // are.  Unlike them, the last geometry's plan, device buffers and streams stay on the
 // device between calls (a reconstruction calls the gateway again and again with one
-// geometry), until the geometry changes or ctsim_host_cache_release; and the forward
-// projection runs in view chunks whose results go back to the host while the next
-// chunk computes.
+// geometry), until the geometry changes or ctsim_host_cache_release; and the data moves
+// in view chunks that overlap the kernels (forward results out, backprojection inputs in).
 // ---------------------------------------------------------------------------
 namespace {
 struct HostCache {

@@ -124,9 +124,12 @@ bool ctsim_cbct_geom(const char *type, int nx, int ny, int nz, float dx, float d
 
 /* The drop-in entry points above keep, per device, the last geometry's plan, device buffers
  * and streams between calls (same geometry scalars, betas, couchz and map: reused; anything
- * else: rebuilt), and return the forward projection to the host in view chunks while the
- * later chunks compute.  No reference counterpart (the reference MEX back ends allocate
- * and free per call).  Results do not depend on the cache. */
+ * else: rebuilt).  They move the data in view chunks that overlap the kernels: the forward
+ * projection goes back to the host chunk by chunk while later chunks compute, and the DD,
+ * SF and pd/hpd backprojections take the sinogram in chunk by chunk while earlier chunks
+ * are backprojected.  No reference counterpart (the reference MEX back ends allocate and
+ * free per call and copy one view at a time).  Results do not depend on the cache or the
+ * chunks, bit for bit. */
 /* Frees the kept plan, buffers and streams now. */
 ctsim_status ctsim_host_cache_release(void);
 /* enabled = 0: free after every call, as the reference does; 1 (the default): keep. */
