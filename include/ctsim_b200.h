@@ -45,7 +45,8 @@ typedef enum {
     CTSIM_ERR_ARGUMENT = 1,    /* invalid sizes, null pointers, unknown method */
     CTSIM_ERR_CUDA = 2,        /* a CUDA runtime call or kernel launch failed */
     CTSIM_ERR_ALLOC = 3,       /* device or host allocation failed */
-    CTSIM_ERR_UNSUPPORTED = 4, /* geometry outside what the kernels implement (see the DESIGN notes) */
+    CTSIM_ERR_UNSUPPORTED = 4, /* geometry outside what the kernels implement (a footprint wider than a
+                                  kernel's row buffer, a non-DD method on the arc detector) */
     CTSIM_ERR_NO_DEVICE = 5    /* no usable sm_100 device */
 } ctsim_status;
 
