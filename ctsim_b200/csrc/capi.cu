@@ -492,9 +492,11 @@ static ctsim_status plan_back_views(ctsim_plan *p, int method, const float *d_pr
     if (p->g.det == 2 && method != CTSIM_BACK_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
     ctsim_status s = check_views(p, vb, 1, vc);
     if (s != CTSIM_OK) return s;
-    if (method == CTSIM_BACK_PD || method == CTSIM_BACK_HPD) {  // FP32 sinogram read as it is; no y slabs
-        const cudaError_t e = launch_pd(method == CTSIM_BACK_PD ? kPdOff : kPdClamp, p->pd_mz, p->g, p->d_views,
-                                        d_proj, p->d_map, d_image, CTSIM_F32, vb, 1, vc, 1.0f, st, accumulate);
+    if (method == CTSIM_BACK_PD || method == CTSIM_BACK_HPD || method == CTSIM_BACK_VAR) {
+        // FP32 sinogram read as it is; no y slabs
+        const int mode = method == CTSIM_BACK_PD ? kPdOff : method == CTSIM_BACK_HPD ? kPdClamp : kPdVar;
+        const cudaError_t e = launch_pd(mode, p->pd_mz, p->g, p->d_views, d_proj, p->d_map, d_image, CTSIM_F32, vb,
+                                        1, vc, 1.0f, st, accumulate);
         return e == cudaSuccess ? CTSIM_OK : cuda_fail(e, "backprojection kernel");
     }
     if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
@@ -706,7 +708,7 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
                 break;
             }
         } else if (method == CTSIM_BACK_DD || method == CTSIM_BACK_TF || method == CTSIM_BACK_PD ||
-                   method == CTSIM_BACK_HPD) {
+                   method == CTSIM_BACK_HPD || method == CTSIM_BACK_VAR) {
             // the sinogram in view chunks on the copy stream; each chunk is backprojected,
             // continuing the image's view sums, while the next one is copied in.  For DD/SF
             // the last chunk runs in y slabs, and each finished slab goes back to the host

@@ -127,7 +127,7 @@ bool ctsim_cbct_geom(const char *type, int nx, int ny, int nz, float dx, float d
  * and streams between calls (same geometry scalars, betas, couchz and map: reused; anything
  * else: rebuilt).  They move the data in view chunks that overlap the kernels: the forward
  * projection goes back to the host chunk by chunk while later chunks compute, and the DD,
- * SF and pd/hpd backprojections take the sinogram in chunk by chunk while earlier chunks
+ * SF, pd/hpd and var backprojections take the sinogram in chunk by chunk while earlier chunks
  * are backprojected.  No reference counterpart (the reference MEX back ends allocate and
  * free per call and copy one view at a time).  Results do not depend on the cache or the
  * chunks, bit for bit. */
