@@ -21,13 +21,14 @@ constexpr unsigned kFull = 0xffffffffu;
 // A^T: one warp per voxel column, lanes along z; 8 columns (consecutive ix) per block.
 // For each view the warp forms, in shared memory, the u-weighted detector column
 //     q[iv] = sum_iu w_u(iu) * ps[iu][iv]        (ps = proj * ampv, pre-scaled)
-// over the rows the column's voxels can touch (4 rows per lane, float4 loads), and
-// its running sum C.  The distance-driven axial weights of a voxel are the overlaps
-// of its extent [t_iz, t_iz+1] with the detector rows (geom/cbct/cbct_back.c:318-357),
-// so its value is the integral of the piecewise-constant q over that extent:
-//     F(t_iz+1) - F(t_iz),   F(t) = C[k] + (t - k - 1) q[k],  k = floor(t)
-// Adjacent voxels share their common edge (warp shuffles), so each voxel costs one
-// edge evaluation.  Accumulation over views stays in registers; no atomics.
+// over the rows the column's voxels can touch (4 rows per lane, float4 loads).  Each
+// voxel then sums q over the rows its axial extent covers with the distance-driven
+// row weights of geom/cbct/cbct_back.c:318-357, its edges vmin/vmax computed with the
+// reference's float operations (usually two or three rows per voxel).  The edges sit
+// hundreds of rows up the detector, where one float rounding moves a voxel's weight by
+// ~1e-5 of itself; evaluating them exactly as the reference does keeps each voxel's
+// value within a few float roundings of the reference's instead of adding noise of
+// that size.  Accumulation over views stays in registers; no atomics.
 // ---------------------------------------------------------------------------
 // The work of one block (8 columns of one row iy), as a device function: the plain
 // kernel runs it for blockIdx.x, the batched kernel for each of its work items.
@@ -39,8 +40,8 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                                            int block) {
     constexpr int kWS = 17;  // row stride of the per-warp weight table (conflict-free writes)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float *wtab = smem + warp * (32 * kWS + 2 * qcap);   // [32 views][17] u weights of the view chunk
-    float2 *CQ = reinterpret_cast<float2 *>(wtab + 32 * kWS);  // [qcap] (running sum, q) per row
+    float *wtab = smem + warp * (32 * kWS + qcap);  // [32 views][17] u weights of the view chunk
+    float *Q = wtab + 32 * kWS;                     // [qcap] q per row (16-byte aligned: 32 * 17 * 4 = 2176)
     const int tiles_x = (g.nx + 7) >> 3;
     const int iy = block / tiles_x;
     const int ix = (block % tiles_x) * 8 + warp;
@@ -49,17 +50,15 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
     const size_t nuv = (size_t)g.nu * g.nv;
     const bool on = map[iy * g.nx + ix] != 0;
     const float fnv = (float)g.nv;
+    const int nvm1 = g.nv - 1;
     const int zpass = 32 * MZ;
     for (int iz0 = 0; iz0 < g.nz; iz0 += zpass) {
         const int izn = min(zpass, g.nz - iz0);
         const float fz_first = (float)iz0, fz_last = (float)(iz0 + izn - 1);
-        const float fz_top = (float)(iz0 + zpass);
-        float acc[MZ], izf[MZ];
+        float acc[MZ];
 #pragma unroll
-        for (int m = 0; m < MZ; m++) {
-            acc[m] = 0.0f;
-            izf[m] = (float)(iz0 + lane + 32 * m);
-        }
+        for (int m = 0; m < MZ; m++) acc[m] = 0.0f;
+        const float fz_lane = (float)(iz0 + lane);
         if (SUM) {
             // continue the per-voxel view sum (scale 1) that the previous view chunk left in
             // the FP32 image; the sum runs in view order either way
@@ -90,27 +89,27 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                     const float zinc = __shfl_sync(kFull, my.zinc, j);
                     const float vstart = __shfl_sync(kFull, my.vstart, j);
                     // rows reachable by voxels [iz0, iz0+izn) (the reference's clamped extents, monotone in iz)
-                    float a0 = fadd(fadd(vstart, fmul(fz_first, zinc)), 0.5f);
-                    a0 = fmaxf(a0, 0.0f);
-                    float b1 = fadd(fadd(fadd(vstart, fmul(fz_last, zinc)), zinc), 0.5f);
-                    b1 = fminf(b1, fnv);
+                    const float a0u = fadd(fadd(vstart, fmul(fz_first, zinc)), 0.5f);
+                    const float b1u = fadd(fadd(fadd(vstart, fmul(fz_last, zinc)), zinc), 0.5f);
+                    const float a0 = fmaxf(a0u, 0.0f), b1 = fminf(b1u, fnv);
                     if (!(a0 < fnv) || !(b1 >= 0.0f)) continue;
                     const int r_lo = floor_pos(a0);
-                    int r_hi = min(floor_pos(b1), g.nv - 1);
+                    int r_hi = min(floor_pos(b1), nvm1);
                     if (r_lo > r_hi) continue;
                     const int rbase = r_lo & ~3;
-                    if (r_hi - rbase + 2 > qcap) {  // rows rbase..r_hi+1 must fit
+                    // every voxel of the pass exists and lies inside the detector (no clamps)
+                    bool inside = a0u > 0.0f && b1u < fnv && izn == zpass;
+                    if (r_hi - rbase + 1 > qcap) {  // rows rbase..r_hi must fit
                         if (lane == 0) atomicOr(err, 1);
-                        r_hi = rbase + qcap - 2;
+                        r_hi = rbase + qcap - 1;
+                        inside = false;
                     }
-                    // q and its running sum over rows [rbase, r_hi], 128 rows per pass
+                    // q over rows [rbase, r_hi], 128 rows per pass (the voxels read rows
+                    // [r_lo, r_hi] only)
                     const int nb = iumax - iumin + 1;
                     const float *wj = wtab + j * kWS;
                     const float *pv = ps + (size_t)(k0 + j) * nuv + (size_t)iumin * g.nv;
-                    // Rows outside [r_lo, r_hi] only shift C by a constant (below) or are never
-                    // read past (above r_hi + 1), so no row masks are needed.
-                    float carry = 0.0f;
-                    for (int c = rbase; c <= r_hi + 1; c += 128) {
+                    for (int c = rbase; c <= r_hi; c += 128) {
                         const int r0 = c + 4 * lane;
                         float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f;
                         if (r0 <= r_hi) {
@@ -137,44 +136,83 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                                 q2 = fmaf(w, p.z, q2); q3 = fmaf(w, p.w, q3);
                             }
                         }
-                        const float s1 = q0 + q1, s2 = s1 + q2, s3 = s2 + q3;
-                        float incl = s3;
-#pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const float n = __shfl_up_sync(kFull, incl, o);
-                            if (lane >= o) incl += n;
-                        }
-                        const float base = carry + (incl - s3);
-                        float4 *dst = reinterpret_cast<float4 *>(CQ + (r0 - rbase));
-                        dst[0] = make_float4(base + q0, q0, base + s1, q1);
-                        dst[1] = make_float4(base + s2, q2, base + s3, q3);
-                        carry += __shfl_sync(kFull, incl, 31);
+                        *reinterpret_cast<float4 *>(Q + (r0 - rbase)) = make_float4(q0, q1, q2, q3);
                     }
                     __syncwarp();
-                    // F at every voxel edge t = vstart + 0.5 + iz*zinc, clamped to the covered rows
-                    const float fr_lo = small_int_to_float(r_lo);
-                    const float fr_top = small_int_to_float(r_hi + 1);
-                    const float vs_half = vstart + 0.5f;
-                    const float2 *cqb = CQ - rbase;
-                    auto edge = [&](float izv) -> float {
-                        // F(t) = C[k] - (k + 1 - t) q[k] with k = floor(t); at t = r_hi + 1 the row
-                        // r_hi + 1 entry gives C[r_hi] exactly
-                        const float t = fminf(fmaxf(fmaf(izv, zinc, vs_half), fr_lo), fr_top);
-                        const float tt = __fadd_rd(t, kTwo23);
-                        const int k = __float_as_int(tt) - 0x4B000000;
-                        const float2 cq = cqb[k];
-                        return fmaf(t - (tt - (kTwo23 - 1.0f)), cq.y, cq.x);
-                    };
-                    float Fl[MZ];
+                    // Each voxel: the reference's clamped extent and row weights
+                    // (geom/cbct/cbct_back.c:318-357); rows [k_lo, k_hi] lie in [r_lo, r_hi]
+                    // because the edges are monotone in iz.
+                    const float *qb = Q - rbase;
+                    // vmax - vmin is zinc within 1.5 float ulps of nv (< 2^-10 for nv <= 8192), so
+                    // away from zinc = 1 and 2 by a margin every voxel of the view covers the same
+                    // number of rows give or take one: n = k_hi - k_lo is 0 or 1 (zinc < 1) or 1 or
+                    // 2 (1 < zinc < 2).  Those views run branch-free: the rows k_lo .. k_lo + 1 (+ 2)
+                    // are always read (the row buffer has 4 spare floats; rows past r_hi may hold
+                    // anything, so their terms are selected, never multiplied by zero).
+                    constexpr float kMargin = 1.0f / 256.0f;
+                    const int path = !inside ? 0 : zinc < 1.0f - kMargin ? 1
+                                                 : (zinc > 1.0f + kMargin && zinc < 2.0f - kMargin) ? 2 : 0;
+                    if (path == 1) {
 #pragma unroll
-                    for (int m = 0; m < MZ; m++) Fl[m] = edge(izf[m]);
-                    const float Ftop = edge(fz_top);
+                        for (int m = 0; m < MZ; m++) {
+                            const float izv = fz_lane + (float)(32 * m);  // exact
+                            const float vpre = fadd(vstart, fmul(izv, zinc));
+                            const float vmin = fadd(vpre, 0.5f);
+                            const float vmax = fadd(fadd(vpre, zinc), 0.5f);
+                            const float tlo = __fadd_rd(vmin, kTwo23), thi = __fadd_rd(vmax, kTwo23);
+                            const float *qk = qb + (__float_as_int(tlo) - 0x4B000000);
+                            const float q0 = qk[0], q1 = qk[1];
+                            // one row: (vmax - vmin) q0; two: (k_lo + 1 - vmin) q0 + (vmax - k_hi) q1
+                            const float one = fsub(vmax, vmin) * q0;
+                            const float two = fmaf(fsub(vmax, fsub(thi, kTwo23)), q1,
+                                                   fsub(fsub(tlo, kTwo23 - 1.0f), vmin) * q0);
+                            acc[m] = fmaf(ampu, thi == tlo ? one : two, acc[m]);
+                        }
+                    } else if (path == 2) {
 #pragma unroll
-                    for (int m = 0; m < MZ; m++) {
-                        float Fh = __shfl_down_sync(kFull, Fl[m], 1);
-                        const float nxt = __shfl_sync(kFull, m + 1 < MZ ? Fl[m + 1 < MZ ? m + 1 : m] : Ftop, 0);
-                        if (lane == 31) Fh = (m + 1 < MZ) ? nxt : Ftop;
-                        acc[m] = fmaf(ampu, Fh - Fl[m], acc[m]);
+                        for (int m = 0; m < MZ; m++) {
+                            const float izv = fz_lane + (float)(32 * m);
+                            const float vpre = fadd(vstart, fmul(izv, zinc));
+                            const float vmin = fadd(vpre, 0.5f);
+                            const float vmax = fadd(fadd(vpre, zinc), 0.5f);
+                            const float tlo = __fadd_rd(vmin, kTwo23), thi = __fadd_rd(vmax, kTwo23);
+                            const float *qk = qb + (__float_as_int(tlo) - 0x4B000000);
+                            const float q0 = qk[0], q1 = qk[1], q2 = qk[2];
+                            const bool three = fsub(thi, tlo) == 2.0f;
+                            const float wl = fsub(vmax, fsub(thi, kTwo23));
+                            // two rows: w0 q0 + wl q1; three: w0 q0 + q1 + wl q2 (the reference's row order)
+                            float vox = fmaf(three ? 1.0f : wl, q1, fsub(fsub(tlo, kTwo23 - 1.0f), vmin) * q0);
+                            vox = three ? fmaf(wl, q2, vox) : vox;
+                            acc[m] = fmaf(ampu, vox, acc[m]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int m = 0; m < MZ; m++) {
+                            const float izv = fz_lane + (float)(32 * m);  // exact
+                            const float vpre = fadd(vstart, fmul(izv, zinc));                // vstart + iz * zinc
+                            const float vmin = fmaxf(fadd(vpre, 0.5f), 0.0f);                 // max(vmin + 0.5, 0)
+                            const float vmax = fminf(fadd(fadd(vpre, zinc), 0.5f), fnv);      // min(vmax + 0.5, nv)
+                            if (izv <= fz_last && vmin <= vmax) {
+                                float flo, fhi;
+                                const int klo = floor_pos(vmin, &flo);
+                                int khi = floor_pos(vmax, &fhi);
+                                if (khi > nvm1) { khi = nvm1; fhi = fsub(fnv, 1.0f); }
+                                if (khi > klo + (kMaxRowsV - 1)) {
+                                    khi = klo + (kMaxRowsV - 1);
+                                    fhi = fadd(flo, (float)(kMaxRowsV - 1));
+                                }
+                                khi = min(khi, r_hi);  // only after a row-buffer overflow (flagged above)
+                                float vox = 0.0f;
+                                if (klo == khi) {
+                                    vox = fsub(vmax, vmin) * qb[klo];
+                                } else if (klo < khi) {
+                                    vox = fsub(fadd(flo, 1.0f), vmin) * qb[klo];
+                                    for (int k = klo + 1; k < khi; k++) vox += qb[k];
+                                    vox = fmaf(fsub(vmax, fhi), qb[khi], vox);
+                                }
+                                acc[m] = fmaf(ampu, vox, acc[m]);
+                            }
+                        }
                     }
                     __syncwarp();
                 }
@@ -675,7 +713,9 @@ cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes) {
     return e;
 }
 
-size_t back_smem_bytes(int qcap) { return (size_t)8 * (32 * 17 + 2 * qcap) * sizeof(float); }
+// per warp: the u weights of 32 views and the row buffer; 4 spare floats past the last
+// warp's buffer for the branch-free row reads
+size_t back_smem_bytes(int qcap) { return ((size_t)8 * (32 * 17 + qcap) + 4) * sizeof(float); }
 
 template <int METHOD, int MZ, bool VEC, bool SUM>
 static cudaError_t launch_back_mz(const Geom &g, const View *views, const float *ps, const uint8_t *map,

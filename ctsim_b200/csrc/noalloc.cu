@@ -1,13 +1,13 @@
 // Matched distance-driven backprojection that allocates no memory.
 //
-// For callers that may not call cudaMalloc themselves or through a library: code
-// that runs while a CUDA graph is being captured on a shared stream, host
+// For callers that may not call cudaMalloc themselves or through a library: host
 // frameworks that own all device memory through their own pool (MATLAB's
 // gpuArray, a serving process with a fixed memory budget), or real-time loops
 // where an allocation's implicit synchronisation is not acceptable.  The caller
 // passes device pointers for the sinogram and the image and host pointers for
 // the geometry; the per-view table, the detector amplitude table and the map
 // are built on the device in one fixed, file-scope scratch array.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -24,7 +24,9 @@ constexpr size_t kScratchBytes = (size_t)8 << 20;
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
-void *g_scratch_ptr[kMaxDevices] = {};  // device address of g_scratch, per device
+// Device address of g_scratch, per device.  Threads that make their first call on a
+// device at the same time all look up and store the same address.
+std::atomic<void *> g_scratch_ptr[kMaxDevices] = {};
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
@@ -94,16 +96,16 @@ extern "C" ctsim_status ctsim_back_dd_noalloc(const ctsim_geom *geom, const doub
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_NO_DEVICE, cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return ctsim_set_last_error(CTSIM_ERR_NO_DEVICE, "device index out of range");
-    if (!g_scratch_ptr[dev]) {
+    void *scratch = g_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!scratch) {
         // once per device, with that device current: the host-side symbol is a stand-in,
         // the kernels need the device address
-        void *ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_scratch);
-        if (e != cudaSuccess || !ptr)
+        e = cudaGetSymbolAddress(&scratch, g_scratch);
+        if (e != cudaSuccess || !scratch)
             return ctsim_set_last_error(CTSIM_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed");
-        g_scratch_ptr[dev] = ptr;
+        g_scratch_ptr[dev].store(scratch, std::memory_order_release);
     }
-    unsigned char *base = static_cast<unsigned char *>(g_scratch_ptr[dev]);
+    unsigned char *base = static_cast<unsigned char *>(scratch);
     int *err = reinterpret_cast<int *>(base);
     View *views = reinterpret_cast<View *>(base + off_views);
     double *dbetas = reinterpret_cast<double *>(base + off_betas);
@@ -159,5 +161,15 @@ extern "C" ctsim_status ctsim_back_dd_noalloc(const ctsim_geom *geom, const doub
     if ((e = cudaGetLastError()) != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
     e = launch_back_unscaled(mz, g, views, d_proj, ampv, dmap, d_image, G.noviews, qcap, err, st);
     if (e != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
+    // The kernel sets the flag when a voxel column's detector rows exceed its row buffer
+    // (sized from the largest axial footprint, so never for an accepted geometry); the
+    // image would then be incomplete.  Reading it back waits for the backprojection.
+    int flag = 0;
+    if ((e = cudaMemcpyAsync(&flag, err, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
+    if (flag)
+        return ctsim_set_last_error(CTSIM_ERR_UNSUPPORTED,
+                                    "a voxel column's detector rows exceeded the backprojection's row buffer");
     return CTSIM_OK;
 }

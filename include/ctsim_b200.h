@@ -404,8 +404,10 @@ ctsim_status ctsim_log_attenuation(const float *d_counts, size_t n, float source
  * The first call on a device looks up that array's device address (set-up, once per
  * device); make that first call before any stream capture.  Every call rewrites the
  * shared array, so calls that overlap on the GPU (other streams, other host threads)
- * race; serialise them.  Asynchronous on `stream` (the geometry copies from pageable
- * host memory are synchronous). */
+ * race; serialise them.  The work runs on `stream`, and the call returns when it has
+ * finished: it reads back the kernel's row-buffer flag and returns CTSIM_ERR_UNSUPPORTED
+ * if a column's detector rows did not fit (never for a geometry the size checks accept;
+ * the image would be incomplete). */
 ctsim_status ctsim_back_dd_noalloc(const ctsim_geom *geom, const double *betas, const float *couchz,
                                    const bool *map, const float *d_proj, float *d_image, void *stream);
 

@@ -121,6 +121,37 @@ def oracle_cbct(kind: str, geom, data, fp64: bool = False) -> np.ndarray:
     return out
 
 
+def oracle_cbct_mt(kind: str, geom, data, nthreads: int = 0) -> np.ndarray:
+    """``oracle_cbct`` over contiguous view chunks in host threads (ctypes releases the
+    GIL), like the reference harness ``ref_cbct_call_mt`` (oracle/ref_shim.c): forward
+    projections fill disjoint view slices, backprojections fill one image per chunk and
+    the images are summed in chunk order (so only the view-sum order differs from the
+    single-thread oracle)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from dataclasses import replace
+
+    if nthreads < 1:
+        nthreads = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    n = geom.noViews
+    chunks = max(1, min(nthreads, n))
+    bounds = [n * c // chunks for c in range(chunks + 1)]
+    data = np.ascontiguousarray(data, dtype=np.float32)
+
+    def part(c):
+        b, e = bounds[c], bounds[c + 1]
+        g = replace(geom, betas=np.ascontiguousarray(geom.betas[b:e]), couchZ=np.ascontiguousarray(geom.couchZ[b:e]))
+        return oracle_cbct(kind, g, data if kind.startswith("proj") else data[b:e])
+
+    with ThreadPoolExecutor(chunks) as ex:
+        parts = list(ex.map(part, range(chunks)))
+    if kind.startswith("proj"):
+        return np.concatenate(parts, axis=0)
+    out = np.zeros(geom.image_shape, np.float32)
+    for p in parts:
+        out += p
+    return out
+
+
 def ref_cbct(kind: str, geom, data, nthreads: int = 1) -> np.ndarray:
     """Run the reference's own compiled geom/cbct projector (needs _ref/libcbct_ref.so)."""
     lib = _load(REF_SO)

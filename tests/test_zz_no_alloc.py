@@ -5,9 +5,11 @@ themselves (a framework owning all device memory through its own pool, a
 serving loop with a fixed budget, code that cannot afford the device
 synchronisation of cudaMalloc/cudaFree).  It keeps its tables in one fixed
 device array shared by all calls, so the GPU test calls it twice in a row with
-different sinograms and checks each result against the plan API's matched
-distance-driven backprojection, with the parity tolerance of the other tests.
-Collected last so that a failure here comes after every other test has run.
+different sinograms, on a flat detector and on a curved one with couch shifts,
+and checks each result against the plan API's matched distance-driven
+backprojection and against the oracle, with the parity tolerance of the other
+tests.  Collected last so that a failure here comes after every other test has
+run.
 """
 import ctypes
 
@@ -29,13 +31,26 @@ def _rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
+def _flat():
+    return CTGeometry((96, 80, 40), (1.0, 1.0, 1.0), (0.5, -0.25, 0.0), (192, 72), (1.6, 1.6), (1.0, 0.0), 1000.0,
+                      500.0, 1500.0, circular_betas(90), map=np.random.default_rng(4).random((80, 96)) > 0.1)
+
+
+def _curved_couch():
+    n = 60
+    return CTGeometry((72, 88, 36), (1.0, 1.0, 1.2), (-1.0, 0.5, 2.0), (160, 64), (1.4, 1.5), (-2.0, 1.5), 1000.0,
+                      500.0, 1500.0, circular_betas(n), couchZ=np.linspace(-6.0, 6.0, n).astype(np.float32),
+                      flatPanel=0)
+
+
 @pytest.mark.gpu
-def test_noalloc_backprojection_matches_plan_on_two_calls():
+@pytest.mark.parametrize("make", [_flat, _curved_couch], ids=["flat", "curved_couch"])
+def test_noalloc_backprojection_matches_plan_on_two_calls(make):
     import torch
     from ctsim_b200.projector import Plan
+    from oracle.bindings import oracle_cbct
 
-    g = CTGeometry((96, 80, 40), (1.0, 1.0, 1.0), (0.5, -0.25, 0.0), (192, 72), (1.6, 1.6), (1.0, 0.0), 1000.0,
-                   500.0, 1500.0, circular_betas(90), map=np.random.default_rng(4).random((80, 96)) > 0.1)
+    g = make()
     L = _lib.load()
     gs = _geom_struct(g)
     betas = np.ascontiguousarray(g.betas)
@@ -45,7 +60,8 @@ def test_noalloc_backprojection_matches_plan_on_two_calls():
     rng = np.random.default_rng(12)
     stream = torch.cuda.current_stream()
     for call in range(2):
-        y = torch.from_numpy(rng.random(g.sino_shape, dtype=np.float32) * (call + 1)).cuda()
+        y_host = rng.random(g.sino_shape, dtype=np.float32) * (call + 1)
+        y = torch.from_numpy(y_host).cuda()
         want = plan.backproject(y, "dd").cpu().numpy()
         out = torch.full(g.image_shape, float("nan"), dtype=torch.float32, device="cuda")
         st = L.ctsim_back_dd_noalloc(ctypes.byref(gs), betas.ctypes.data, couch.ctypes.data, mp.ctypes.data,
@@ -55,7 +71,9 @@ def test_noalloc_backprojection_matches_plan_on_two_calls():
         got = out.cpu().numpy()
         assert np.all(np.isfinite(got))
         err = _rel_l2(got, want)
-        assert err <= REL_L2, f"call {call}: rel L2 {err:.2e}"
+        assert err <= REL_L2, f"call {call}: rel L2 {err:.2e} against the plan API"
+        err = _rel_l2(got, oracle_cbct("back,dd", g, y_host))
+        assert err <= REL_L2, f"call {call}: rel L2 {err:.2e} against the oracle"
         assert np.all(got[:, ~g.map] == 0)
 
 
