@@ -146,8 +146,15 @@ def make_workload(views: int = 0):
     return g, to_projector_units(x_mm)
 
 
-def cpu_reference_sample(g, x, y, seconds_hint=True):
-    """Time the reference C (all host cores) on a bounded sample of the workload's views."""
+def sample_views(g, nviews):
+    """Indices of the CPU sample's views: every (views / nviews)-th view of the scan."""
+    return np.arange(0, g.noViews, max(1, g.noViews // nviews))[:nviews]
+
+
+def cpu_reference_sample(g, x, y, keep_outputs=False):
+    """Time the reference C (all host cores) on a bounded sample of the workload's views.
+    With ``keep_outputs`` the sample's A and A^T results come back too (under "outputs",
+    with the view indices), for the parity check of the GPU step."""
     from oracle.bindings import ref_available, ref_cbct, oracle_cbct
     ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     nxyz = g.nx * g.ny * g.nz
@@ -158,30 +165,49 @@ def cpu_reference_sample(g, x, y, seconds_hint=True):
         avail = 16 << 30
     # the threaded backprojection keeps one image per thread
     threads = max(1, min(ncores, int(avail * 0.5 // (nxyz * 4))))
-    nviews = threads
-    gs = g.subset(1, 0)
     from dataclasses import replace
-    gs = replace(g, betas=g.betas[:: g.noViews // nviews][:nviews].copy(),
-                 couchZ=g.couchZ[:: g.noViews // nviews][:nviews].copy())
-    ys = np.ascontiguousarray(y[:: g.noViews // nviews][:nviews])
+    idx = sample_views(g, threads)
+    if not ref_available():  # the oracle port, single-threaded, one view
+        threads, idx = 1, idx[:1]
+    gs = replace(g, betas=g.betas[idx].copy(), couchZ=g.couchZ[idx].copy())
+    ys = np.ascontiguousarray(y[idx])
     if ref_available():
         kind = "reference"
         t0 = time.perf_counter()
-        ref_cbct("proj,dd", gs, x, nthreads=threads)
-        ref_cbct("back,dd", gs, ys, nthreads=threads)
+        a = ref_cbct("proj,dd", gs, x, nthreads=threads)
+        at = ref_cbct("back,dd", gs, ys, nthreads=threads)
         dt = time.perf_counter() - t0
-    else:  # the oracle port, single-threaded, one view
-        kind, threads = "port", 1
-        gs = replace(gs, betas=gs.betas[:1].copy(), couchZ=gs.couchZ[:1].copy())
-        ys = ys[:1]
+    else:
+        kind = "port"
         t0 = time.perf_counter()
-        oracle_cbct("proj,dd", gs, x)
-        oracle_cbct("back,dd", gs, ys)
+        a = oracle_cbct("proj,dd", gs, x)
+        at = oracle_cbct("back,dd", gs, ys)
         dt = time.perf_counter() - t0
     vv = 2.0 * nxyz * gs.noViews
-    return {"value": vv / dt / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"DD A then A^T of {gs.noViews} of the {g.noViews} views on the full "
-                      f"{g.nx}x{g.ny}x{g.nz} volume ({dt:.1f} s)"}
+    out = {"value": vv / dt / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
+           "sample": f"DD A then A^T of {gs.noViews} of the {g.noViews} views on the full "
+                     f"{g.nx}x{g.ny}x{g.nz} volume ({dt:.1f} s)"}
+    if keep_outputs:
+        out["outputs"] = (idx, gs, a, at)
+    return out
+
+
+def rel_l2(a, b):
+    a64, b64 = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a64 - b64) / max(np.linalg.norm(b64), 1e-300))
+
+
+def step_parity(plan_cls, sino, yd, sample):
+    """The timed step's own results against the reference C on the CPU sample's views:
+    A from the step's sinogram at those views, A^T from a plan of those views over the
+    step's data (the full A^T sums all views; the CPU sample backprojects its own)."""
+    import torch
+    idx, gs, ref_a, ref_at = sample
+    ours_a = sino[torch.as_tensor(idx, device=sino.device)].cpu().numpy()
+    ys = yd[torch.as_tensor(idx, device=yd.device)].contiguous()
+    ours_at = plan_cls(gs).backproject(ys, "dd").cpu().numpy()
+    return {"views": [int(i) for i in idx], "against": "reference C" if len(idx) > 1 else "oracle",
+            "A_rel_l2": rel_l2(ours_a, ref_a), "AT_rel_l2": rel_l2(ours_at, ref_at), "bar": 1e-5}
 
 
 def run_reference(args):
@@ -302,23 +328,32 @@ def run_ours(args):
     mp = np.ascontiguousarray(g.map)
     sc = g.scalars()
 
-    def e2e_step():
-        ok1 = L.ctsim_proj_dd(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, h_img.data_ptr(),
-                              h_sino_out.data_ptr(), mp.ctypes.data)
-        ok2 = L.ctsim_back_dd(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, h_img_out.data_ptr(),
-                              h_sino_in.data_ptr(), mp.ctypes.data)
+    def e2e_step(img_in, sino_out, img_out, sino_in):
+        ok1 = L.ctsim_proj_dd(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, img_in, sino_out,
+                              mp.ctypes.data)
+        ok2 = L.ctsim_back_dd(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, img_out, sino_in,
+                              mp.ctypes.data)
         if not (ok1 and ok2):
             raise RuntimeError(_lib.last_error())
 
-    e2e_val, e2e_s = None, None
+    pinned = (h_img.data_ptr(), h_sino_out.data_ptr(), h_img_out.data_ptr(), h_sino_in.data_ptr())
+    e2e_val = e2e_pageable = None
     if not args.no_e2e:
-        e2e_val, e2e_s = run_e2e(e2e_step, K, dist, dev, vv, world)
+        e2e_val, _ = run_e2e(lambda: e2e_step(*pinned), K, dist, dev, vv, world)
+        # pageable host memory, what a MATLAB MEX caller hands over (mxArray data)
+        p_img, p_sino_in = h_img.numpy().copy(), h_sino_in.numpy().copy()
+        p_sino_out = np.empty(g.sino_shape, np.float32)
+        p_img_out = np.empty(g.image_shape, np.float32)
+        pageable = (p_img.ctypes.data, p_sino_out.ctypes.data, p_img_out.ctypes.data, p_sino_in.ctypes.data)
+        e2e_pageable, _ = run_e2e(lambda: e2e_step(*pageable), K, dist, dev, vv, world)
+        del p_img, p_sino_in, p_sino_out, p_img_out
     nbytes_img = g.nx * g.ny * g.nz * 4
     nbytes_sino = g.nu * g.nv * g.noViews * 4
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_reference_sample(g, x, yd.cpu().numpy())
+        cpu = cpu_reference_sample(g, x, yd.cpu().numpy(), keep_outputs=True)
+        parity = step_parity(Plan, sino, yd, cpu.pop("outputs"))
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
@@ -335,8 +370,10 @@ def run_ours(args):
                 "kernels_ms": {"A (prefix+proj)": t_a, "A^T (back)": t_b},
                 "A_gvv_s": vv / (t_a / 1e3) / 1e9, "AT_gvv_s": vv / (t_b / 1e3) / 1e9,
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nbytes_img + nbytes_sino,
-                        "d2h_bytes_per_step": nbytes_sino + nbytes_img,
-                        "api": "ctsim_proj_dd + ctsim_back_dd (host pointers, pinned)"},
+                        "d2h_bytes_per_step": nbytes_sino + nbytes_img, "steps": K,
+                        "api": "ctsim_proj_dd + ctsim_back_dd (host pointers, pinned)",
+                        "pageable_value": e2e_pageable},
+                "parity": parity,
                 "gpu_launches": 4 * K,
                 "clocks": clk,
                 "cpu_baseline": cpu}
@@ -348,15 +385,16 @@ def run_ours(args):
 
 
 def run_e2e(e2e_step, K, dist, dev, vv, world):
+    """K synchronous drop-in steps after one untimed call (wall clock: the C ABI returns
+    after its device->host copies); the slowest rank's time."""
     e2e_step()
-    ke = max(2, min(K, 5))
     if dist:
         import torch.distributed as td
         td.barrier()
     t0 = time.perf_counter()
-    for _ in range(ke):
+    for _ in range(K):
         e2e_step()
-    e2e_s = max_over_ranks((time.perf_counter() - t0) / ke * 1e3, dist, dev) / 1e3
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / K * 1e3, dist, dev) / 1e3
     return replica_value(vv, 1, world, e2e_s * 1e3), e2e_s
 
 

@@ -49,7 +49,7 @@ class CtsimFanGeom(C.Structure):
 
 class CtsimTuning(C.Structure):
     _fields_ = [("proj_groups", _i), ("back_mz", _i), ("pd_mz", _i), ("back_mz_tf", _i), ("proj_rows", _i),
-                ("proj_layout", _i)]
+                ("proj_layout", _i), ("proj_slots", _i)]
 
 
 class CtsimBatchItem(C.Structure):

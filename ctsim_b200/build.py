@@ -34,17 +34,34 @@ def needs_rebuild() -> bool:
 
 
 def build(verbose_ptxas: bool = False, force: bool = False) -> str:
+    """Compile every source to an object (in parallel), then link the shared library."""
     if not force and not verbose_ptxas and not needs_rebuild():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(OUT_DIR, exist_ok=True)
-    cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose_ptxas else [])
-    cmd += [os.path.join(CSRC, s) for s in SOURCES] + ["-o", LIB]
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    compile_flags = [f for f in FLAGS if f not in ("--shared", "-cudart", "static")]
+
+    def compile_one(src):
+        obj = os.path.join(OUT_DIR, os.path.splitext(src)[0] + ".o")
+        cmd = [NVCC] + compile_flags + (["-Xptxas", "-v"] if verbose_ptxas else [])
+        cmd += ["-c", os.path.join(CSRC, src), "-o", obj]
+        return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    for obj, r in results:
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed compiling {os.path.basename(obj)}")
+        if verbose_ptxas:
+            sys.stdout.write(r.stderr)
+    r = subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "--shared", "-cudart", "static"] +
+                       [o for o, _ in results] + ["-o", LIB], capture_output=True, text=True)
+    for o, _ in results:
+        os.remove(o)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libctsim_b200.so")
-    if verbose_ptxas:
-        sys.stdout.write(r.stderr)
+        raise RuntimeError("nvcc failed linking libctsim_b200.so")
     return LIB
 
 

@@ -61,7 +61,7 @@ struct ctsim_plan {
     View *d_views = nullptr;
     float *d_ampv = nullptr;
     uint8_t *d_map = nullptr;
-    float *d_xs = nullptr;   // axial prefix sums [nx*ny][nz+1] (or pairs [..][2]) -- forward projector scratch
+    float *d_xs = nullptr;   // axial prefix sums [nx*ny][g.xstride] (or pairs [nx*ny][nz+1][2]) -- forward projector scratch
     float *d_ps = nullptr;   // sinogram scaled by ampv [noviews][nu][nv] -- backprojector scratch
     int *d_err = nullptr;
     size_t bytes = 0;
@@ -72,6 +72,8 @@ struct ctsim_plan {
     int fwd_groups = 1;      // candidate groups of the forward projector (tunable)
     int fwd_rows = 32;       // row threads per group of the forward projector (tunable)
     bool fwd_pairs = false;  // prefix sums stored as (X, slope) pairs (small volumes; tunable)
+    bool fwd_staged = false; // plain sums, candidate columns staged in shared memory (tunable)
+    int fwd_slots = 8;       // prefix columns per stage buffer of the staged projector (tunable)
     bool xs_holds_pairs = false;  // the prefix scratch was sized for pairs
     bool fwd_ok = true;
     std::string fwd_reason;
@@ -221,6 +223,7 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
     g.sdd_du = G.sdd / G.du;
     g.dz_dv = G.dz / G.dv;
     g.wz_pd = centre(G.nz, G.offset_z);
+    g.xstride = prefix_stride(G.nz);
     g.roff = G.offset_u * G.du * G.sad / G.sdd;
     g.roff_var = G.offset_u * G.sad / G.sdd;
     g.add = G.add;
@@ -355,7 +358,14 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
     CTSIM_ALLOC(p->d_map, mp.size());
     CTSIM_ALLOC(p->d_err, sizeof(int));
     p->fwd_pairs = p->xs_holds_pairs = forward_pairs(nxy, G.nz);
-    if (p->fwd_ok) CTSIM_ALLOC(p->d_xs, sizeof(float) * (p->fwd_pairs ? 2 : 1) * (size_t)nxy * (G.nz + 1));
+    // volumes whose prefix sums do not stay cache-resident: candidate columns staged in
+    // shared memory (B200, config 2: DD A 167 -> 146 ms)
+    p->fwd_slots = 8;
+    p->fwd_staged = !p->fwd_pairs && proj_slots_valid(g.xstride, p->fwd_slots) &&
+                    proj_staged_smem_bytes(G.nv, G.nx, G.ny, g.xstride, p->fwd_groups, p->fwd_rows, p->fwd_slots) <=
+                        200 * 1024;
+    if (p->fwd_ok)
+        CTSIM_ALLOC(p->d_xs, sizeof(float) * (size_t)nxy * (p->xs_holds_pairs ? 2 * (G.nz + 1) : g.xstride));
     CTSIM_ALLOC(p->d_ps, sizeof(float) * (size_t)G.nu * G.nv * G.noviews);
 #undef CTSIM_ALLOC
     p->bytes = bytes;
@@ -415,10 +425,16 @@ static ctsim_status plan_project(ctsim_plan *p, int method, const void *d_image,
     cudaStream_t st = (cudaStream_t)stream;
     const int nxy = p->g.nx * p->g.ny;
     cudaError_t e;
-    if (prefix && (e = launch_prefix(d_image, image_dtype, p->d_xs, nxy, p->g.nz, p->fwd_pairs, st)) != cudaSuccess)
+    if (prefix && (e = launch_prefix(d_image, image_dtype, p->d_xs, nxy, p->g.nz, p->fwd_pairs, p->g.xstride, st)) != cudaSuccess)
         return cuda_fail(e, "prefix kernel");
-    e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->fwd_groups, p->fwd_rows, p->fwd_pairs, p->g, p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj,
-                    proj_dtype, view_begin, view_stride, view_count, p->margin, st);
+    if (p->fwd_staged && !p->fwd_pairs)
+        e = launch_proj_staged(method == CTSIM_PROJ_DD ? kDD : kTF, p->fwd_groups, p->fwd_rows, p->fwd_slots, p->g,
+                               p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj, proj_dtype, view_begin, view_stride,
+                               view_count, p->margin, p->d_err, st);
+    else
+        e = launch_proj(method == CTSIM_PROJ_DD ? kDD : kTF, p->fwd_groups, p->fwd_rows, p->fwd_pairs, p->g,
+                        p->d_views, p->d_xs, p->d_ampv, p->d_map, d_proj, proj_dtype, view_begin, view_stride,
+                        view_count, p->margin, st);
     if (e != cudaSuccess) return cuda_fail(e, "forward projection kernel");
     return CTSIM_OK;
 }
@@ -479,7 +495,7 @@ static ctsim_status plan_prefix(ctsim_plan *p, int method, const void *d_image, 
     if (method != CTSIM_PROJ_DD && method != CTSIM_PROJ_TF) return fail(CTSIM_ERR_ARGUMENT, "unknown forward method");
     if (p->g.det == 2 && method != CTSIM_PROJ_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
     if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
-    const cudaError_t e = launch_prefix(d_image, CTSIM_F32, p->d_xs, p->g.nx * p->g.ny, p->g.nz, p->fwd_pairs, st);
+    const cudaError_t e = launch_prefix(d_image, CTSIM_F32, p->d_xs, p->g.nx * p->g.ny, p->g.nz, p->fwd_pairs, p->g.xstride, st);
     return e == cudaSuccess ? CTSIM_OK : cuda_fail(e, "prefix kernel");
 }
 
@@ -858,7 +874,8 @@ extern "C" ctsim_status ctsim_plan_get_tuning(const ctsim_plan *p, ctsim_tuning 
     if (!p || !t) return fail(CTSIM_ERR_ARGUMENT, "null argument");
     t->proj_groups = p->fwd_groups;
     t->proj_rows = p->fwd_rows;
-    t->proj_layout = p->fwd_pairs ? 2 : 1;
+    t->proj_layout = p->fwd_pairs ? 2 : p->fwd_staged ? 3 : 1;
+    t->proj_slots = p->fwd_slots;
     t->back_mz = p->back_mz;
     t->back_mz_tf = p->back_mz_tf;
     t->pd_mz = p->pd_mz;
@@ -881,11 +898,26 @@ extern "C" ctsim_status ctsim_plan_set_tuning(ctsim_plan *p, const ctsim_tuning 
         (t->back_mz_tf && (!mz_valid(t->back_mz_tf) || !back_mz_fits(p, t->back_mz_tf))))
         return fail(CTSIM_ERR_ARGUMENT, "back_mz must be 1, 2, 4 or 8 and fit the row buffer");
     if (t->pd_mz && !mz_valid(t->pd_mz)) return fail(CTSIM_ERR_ARGUMENT, "pd_mz must be 1, 2, 4 or 8");
-    if (t->proj_layout && t->proj_layout != 1 && !(t->proj_layout == 2 && p->xs_holds_pairs))
-        return fail(CTSIM_ERR_ARGUMENT, "proj_layout must be 1 (sums), or 2 (pairs) on a plan whose volume fits them");
+    if (t->proj_layout && t->proj_layout != 1 && t->proj_layout != 3 && !(t->proj_layout == 2 && p->xs_holds_pairs))
+        return fail(CTSIM_ERR_ARGUMENT,
+                    "proj_layout must be 1 (sums), 2 (pairs, on a plan whose volume fits them) or 3 (staged sums)");
+    {
+        const bool staged = t->proj_layout ? t->proj_layout == 3 : (p->fwd_staged && !p->fwd_pairs);
+        const int G = t->proj_groups ? t->proj_groups : p->fwd_groups;
+        const int R = t->proj_rows ? t->proj_rows : p->fwd_rows;
+        const int S = t->proj_slots ? t->proj_slots : p->fwd_slots;
+        if (t->proj_slots && !proj_slots_valid(p->g.xstride, t->proj_slots))
+            return fail(CTSIM_ERR_ARGUMENT, "proj_slots must be 1 .. 64 with slots * column bytes < 1 MiB");
+        if (staged && proj_staged_smem_bytes(p->geom.nv, p->geom.nx, p->geom.ny, p->g.xstride, G, R, S) > 200 * 1024)
+            return fail(CTSIM_ERR_ARGUMENT, "the staged forward projector's shared memory exceeds 200 KiB: fewer slots");
+    }
     if (t->proj_groups) p->fwd_groups = t->proj_groups;
     if (t->proj_rows) p->fwd_rows = t->proj_rows;
-    if (t->proj_layout) p->fwd_pairs = t->proj_layout == 2;
+    if (t->proj_slots) p->fwd_slots = t->proj_slots;
+    if (t->proj_layout) {
+        p->fwd_pairs = t->proj_layout == 2;
+        p->fwd_staged = t->proj_layout == 3;
+    }
     if (t->back_mz) {
         p->back_mz = t->back_mz;
         p->back_qcap = back_qcap_for(p, t->back_mz);
@@ -922,16 +954,23 @@ static std::vector<ctsim_tuning> tuning_candidates(const ctsim_plan *p, int meth
         if (rmax > 32) rows.push_back(32);
         for (int R : rows) {
             for (int Gr : {1, 2, 4, 8})
-                if (proj_shape_valid(G.nv, Gr, R) && proj_smem_bytes(G.nv, G.nx, G.ny, Gr, R) <= 200 * 1024)
+                if (proj_shape_valid(G.nv, Gr, R) && proj_smem_bytes(G.nv, G.nx, G.ny, Gr, R) <= 200 * 1024) {
                     for (int lay = p->xs_holds_pairs ? 2 : 1; lay >= 1; lay--) {
-                        ctsim_tuning t = {Gr, 0, 0, 0, R, lay};
+                        ctsim_tuning t = {Gr, 0, 0, 0, R, lay, 0};
                         out.push_back(t);
                     }
+                    for (int S : {8, 16, 32})
+                        if (proj_slots_valid(p->g.xstride, S) &&
+                            proj_staged_smem_bytes(G.nv, G.nx, G.ny, p->g.xstride, Gr, R, S) <= 200 * 1024) {
+                            ctsim_tuning t = {Gr, 0, 0, 0, R, 3, S};
+                            out.push_back(t);
+                        }
+                }
         }
         return out;
     }
     for (int mz : {1, 2, 4, 8}) {
-        ctsim_tuning t = {0, 0, 0, 0, 0, 0};
+        ctsim_tuning t = {0, 0, 0, 0, 0, 0, 0};
         if (method == CTSIM_BACK_DD) { if (!back_mz_fits(p, mz)) continue; t.back_mz = mz; }
         else if (method == CTSIM_BACK_TF) { if (!back_mz_fits(p, mz)) continue; t.back_mz_tf = mz; }
         else t.pd_mz = mz;
@@ -951,7 +990,7 @@ extern "C" ctsim_status ctsim_plan_autotune(ctsim_plan *p, int method, int sampl
     const ctsim_geom &G = p->geom;
     const std::vector<int> key = {method, G.nx, G.ny, G.nz, G.nu, G.nv, G.detector_type};
     bool have = false;
-    ctsim_tuning best = {0, 0, 0, 0, 0, 0};
+    ctsim_tuning best = {0, 0, 0, 0, 0, 0, 0};
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tuned.find(key);
@@ -1059,15 +1098,18 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
     // column prefix sums of every image (each plan's own scratch)
     for (int i = 0; i < n; i++) {
         const ctsim_plan *p = items[i].plan;
-        if ((e = launch_prefix(items[i].in, items[i].in_dtype, p->d_xs, p->g.nx * p->g.ny, p->g.nz, p->fwd_pairs,
+        if ((e = launch_prefix(items[i].in, items[i].in_dtype, p->d_xs, p->g.nx * p->g.ny, p->g.nz, p->fwd_pairs, p->g.xstride,
                                st)) != cudaSuccess)
             return cuda_fail(e, "prefix kernel");
     }
-    // one persistent launch per launch-shape class (row threads, candidate groups)
-    std::map<std::vector<int>, std::vector<int>> classes;  // (row threads, groups, prefix layout, FP32 out)
+    // one persistent launch per launch-shape class (row threads, candidate groups, prefix
+    // layout: 0 plain, 1 pairs, 2 staged, with the staged slots)
+    std::map<std::vector<int>, std::vector<int>> classes;  // (row threads, groups, layout, FP32 out, slots)
     for (int i = 0; i < n; i++) {
         const ctsim_plan *p = items[i].plan;
-        classes[{p->fwd_rows, p->fwd_groups, p->fwd_pairs ? 1 : 0, items[i].out_dtype == CTSIM_F32 ? 0 : 1}].push_back(i);
+        const bool staged = p->fwd_staged && !p->fwd_pairs;
+        classes[{p->fwd_rows, p->fwd_groups, p->fwd_pairs ? 1 : staged ? 2 : 0,
+                 items[i].out_dtype == CTSIM_F32 ? 0 : 1, staged ? p->fwd_slots : 0}].push_back(i);
     }
     for (auto &cl : classes) {
         const std::vector<int> &idx = cl.second;
@@ -1092,12 +1134,20 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
                 T.gx = (p->g.nu + proj_group_width() - 1) / proj_group_width();
                 T.first = b.total;
                 T.margin = p->margin;
+                T.err = p->d_err;
                 b.total += proj_task_blocks(p->g, it.view_count);
-                smem = std::max(smem, proj_smem_bytes(p->g.nv, p->g.nx, p->g.ny, p->fwd_groups, p->fwd_rows));
+                smem = std::max(smem, cl.first[2] == 2 ? proj_staged_smem_bytes(p->g.nv, p->g.nx, p->g.ny, p->g.xstride,
+                                                                                p->fwd_groups, p->fwd_rows,
+                                                                                p->fwd_slots)
+                                                       : proj_smem_bytes(p->g.nv, p->g.nx, p->g.ny, p->fwd_groups,
+                                                                         p->fwd_rows));
             }
-            if ((e = launch_proj_batch(method == CTSIM_PROJ_DD ? kDD : kTF, cl.first[1], cl.first[0], cl.first[2] != 0,
-                                       cl.first[3] != 0, smem, b, st)) != cudaSuccess)
-                return cuda_fail(e, "batched forward projection");
+            const int m = method == CTSIM_PROJ_DD ? kDD : kTF;
+            e = cl.first[2] == 2 ? launch_proj_staged_batch(m, cl.first[1], cl.first[0], cl.first[4], cl.first[3] != 0,
+                                                            smem, b, st)
+                                 : launch_proj_batch(m, cl.first[1], cl.first[0], cl.first[2] == 1, cl.first[3] != 0,
+                                                     smem, b, st);
+            if (e != cudaSuccess) return cuda_fail(e, "batched forward projection");
         }
     }
     return CTSIM_OK;

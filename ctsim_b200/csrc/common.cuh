@@ -53,7 +53,13 @@ struct Geom {
     float v_clamp_lo, v_clamp_hi; // hpd clamps 0.5 and nv - 1.5 as floats (cbct_back.c:110-111)
     float rdv;                    // RN(1/dv) for the correctly rounded division by dv, 0 = use IEEE division
     float add, sad_add;           // arc detector: radius ADD, sad / add (geom/cbct/cbct_proj3.c:337-355)
+    int xstride;                  // column stride (floats) of the plain prefix-sum layout: prefix_stride(nz)
 };
+
+// Column stride of the plain prefix-sum layout: X[0..nz] and at least one copy of X[nz]
+// above it, rounded up to 4 floats so that every column starts on a 16-byte boundary
+// (the bulk copies of the staged forward projector need that).
+__host__ __device__ inline int prefix_stride(int nz) { return (nz + 2 + 3) & ~3; }
 
 // Per-view constants, geom/cbct/cbct_proj.c:256-265 and cbct_back.c:50-52.
 struct View {

@@ -257,18 +257,19 @@ __global__ void prescale_kernel(const void *__restrict__ proj, int in_dtype, con
 // * PAIRS: xc[col][k] = (X[k], X[k+1] - X[k]) as float2, with the top pair (X[nz], 0), so
 //   X(s) = X[k] + (s - k) * slope is one aligned 8-byte load and one FMA for 0 <= s <= nz;
 // * single: xc[col][k] = X[k] as float (half the bytes: better when the volume's prefix
-//   does not stay cache-resident; measured on B200 at 512^2 x 256).
+//   does not stay cache-resident; measured on B200 at 512^2 x 256), columns xstride =
+//   prefix_stride(nz) floats apart, with X[nz] repeated above X[nz] up to the stride.
 // 32 columns per block; a 32x32 tile is transposed through shared memory so that the
 // image reads and the prefix writes are coalesced.
 // ---------------------------------------------------------------------------
 template <bool PAIRS>
 __global__ void __launch_bounds__(256) prefix_kernel(const void *__restrict__ image, int in_dtype,
-                                                     float *__restrict__ xs, int nxy, int nz) {
+                                                     float *__restrict__ xs, int nxy, int nz, int xstride) {
     __shared__ float tile[32][33];
     __shared__ float carry[32];
     const int c0 = blockIdx.x * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
-    const size_t stride = (size_t)nz + 1;
+    const size_t stride = PAIRS ? (size_t)nz + 1 : (size_t)xstride;
     if (threadIdx.x < 32) carry[threadIdx.x] = 0.0f;
     for (int z0 = 0; z0 < nz; z0 += 32) {
         __syncthreads();
@@ -302,8 +303,12 @@ __global__ void __launch_bounds__(256) prefix_kernel(const void *__restrict__ im
     __syncthreads();
     if (threadIdx.x < 32 && c0 + threadIdx.x < nxy) {
         const size_t c = c0 + threadIdx.x;
-        if (PAIRS) reinterpret_cast<float2 *>(xs)[c * stride + nz] = make_float2(carry[threadIdx.x], 0.0f);
-        else xs[c * stride] = 0.0f;
+        if (PAIRS) {
+            reinterpret_cast<float2 *>(xs)[c * stride + nz] = make_float2(carry[threadIdx.x], 0.0f);
+        } else {
+            xs[c * stride] = 0.0f;
+            for (size_t k = nz + 1; k < stride; k++) xs[c * stride + k] = carry[threadIdx.x];
+        }
     }
 }
 
@@ -510,7 +515,7 @@ __device__ __forceinline__ void proj_block(const Geom g, const View *__restrict_
             if (jj < 0) continue;
             const int rlo = s_rlo[s], rhi = s_rhi[s];
             const float b0 = s_b0[s], izc = s_iz[s];
-            const float *x = xs + (size_t)s_col[s] * (g.nz + 1) * (PAIRS ? 2 : 1);
+            const float *x = xs + (size_t)s_col[s] * (PAIRS ? 2 * (g.nz + 1) : g.xstride);
             const int jlo = jj & 0xff, jhi = jj >> 8;
             // groups of one warp own all their accumulator rows, so the warp walks the
             // candidate's own rows from rlo (128 per pass); wider groups own fixed bands
@@ -565,10 +570,390 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
                                                                const float *__restrict__ ampv,
                                                                const uint8_t *__restrict__ map,
                                                                void *__restrict__ proj, int out_dtype,
-                                                               int view_begin, int view_stride, float margin) {
+                                                               int view_begin, int view_stride, float margin,
+                                                               int vgroup) {
     extern __shared__ float4 acc4_smem[];
+    // blocks in launch order: the vgroup views of a view group for one detector-column
+    // group, then the next column group (neighbouring views share candidate columns in L2)
     proj_block<METHOD, GROUPS, PAIRS>(g, views, xs, ampv, map, proj, out_dtype, view_begin, view_stride, margin,
-                                      acc4_smem, blockIdx.x, blockIdx.y);
+                                      acc4_smem, blockIdx.x / vgroup, blockIdx.y * vgroup + blockIdx.x % vgroup);
+}
+
+// ---------------------------------------------------------------------------
+// A with the candidates' prefix columns staged in shared memory by bulk copies.
+//
+// Same decomposition and arithmetic as proj_block: one block per (group of kTU
+// detector columns, view), candidate columns from the monotone projected centres of
+// the volume lines, exact footprints per candidate, rows accumulated as
+// w_u * ampu * zinc * (X(iv+1) - X(iv)) by the thread that owns them.  What changes is
+// where X comes from: the valid candidates of a chunk are packed into a list, and
+// their whole prefix columns (g.xstride floats, X[nz] repeated at the top) are copied
+// from global memory into shared memory by the copy engine (cp.async.bulk, completion
+// counted in bytes on an mbarrier), `slots` columns at a time into one of two buffers,
+// so that the copies of the next slots overlap the row loop over the current ones.  The
+// row loop then reads X from shared memory (32-bit addresses, no global gathers).
+// ---------------------------------------------------------------------------
+constexpr int kMbarPolls = 1 << 22;  // bound of every mbarrier wait (a copy normally lands in microseconds)
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// Makes the initialised barriers visible to the copy engine (async proxy).
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// One arrival that also announces `bytes` of copies to complete on this phase.
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// Global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16), its
+// bytes counted on `bar`.  No multicast: the destination is this block's own memory.
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+// Waits for the phase of the given parity to complete; false after kMbarPolls polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    const uint32_t a = smem_addr(bar);
+    for (int i = 0; i < kMbarPolls; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// X(s) of a staged column, s clamped to [0, nz] (X[nz + 1] = X[nz] is part of the copy).
+// xadj: the column's shared-memory address minus 4 * 0x4B000000 (mod 2^32), so that the
+// address of X[floor(s)] is xadj + 4 * bits(s + 2^23 rounded down).
+__device__ __forceinline__ float staged_integral(uint32_t xadj, float s, float fnz) {
+    s = fminf(fmaxf(s, 0.0f), fnz);
+    const float t = __fadd_rd(s, kTwo23);
+    const uint32_t a = xadj + (__float_as_uint(t) << 2);
+    float x0, x1;
+    asm volatile("ld.shared.f32 %0, [%2];\n\tld.shared.f32 %1, [%2+4];" : "=f"(x0), "=f"(x1) : "r"(a));
+    return fmaf(s - (t - kTwo23), x1 - x0, x0);
+}
+// acc += w * (r0, r1, r2, r3) on the float4 at shared address a.
+__device__ __forceinline__ void acc_add4(uint32_t a, float w, float r0, float r1, float r2, float r3) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    v.x = fmaf(w, r0, v.x); v.y = fmaf(w, r1, v.y); v.z = fmaf(w, r2, v.z); v.w = fmaf(w, r3, v.w);
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(a), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w)
+                 : "memory");
+}
+
+// Dynamic shared-memory layout of the staged forward projector: two mbarriers (first, so
+// that a persistent block keeps them across work items of different shapes), the
+// accumulators, the two stage buffers, the candidate table and its packed index, the
+// line tables.
+struct StagedSmem {
+    int nq, nt, nlines, groups, slots, xstride;
+    __host__ __device__ size_t acc_bytes() const { return (size_t)groups * kTU * nq * 16; }
+    __host__ __device__ size_t stage_floats() const { return (size_t)slots * xstride; }  // one buffer
+    __host__ __device__ size_t bytes() const {
+        return 16 + acc_bytes() + 2 * stage_floats() * 4 + (size_t)nt * (6 + kTU) * 4 +
+               (size_t)(2 * nlines + 1 + 32) * 4;
+    }
+};
+
+// Error flag bit of a stage wait that ran out (ctsim_plan_check reports the flag).
+constexpr int kErrStageWait = 4;
+
+// Candidate intervals of the lines for detector columns [iu0, iu0 + kTU) of view v:
+// line_start[L], and line_off[L] the exclusive scan of the counts (line_off[nlines] =
+// the total).  All threads of the block call it; ends with a block barrier.
+__device__ __forceinline__ int candidate_lines(const Geom &g, const View &v, int iu0, float margin, bool rows,
+                                               int *line_start, int *line_off, int *s_warp_tot) {
+    const int NT = blockDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int nlines = rows ? g.ny : g.nx;
+    const int npos = rows ? g.nx : g.ny;
+    const float ulo = (float)iu0 - margin, uhi = (float)(iu0 + kTU) + margin;
+    auto centre_u = [&](int ix, int iy) -> float {
+        const float xcf = ((float)ix + g.wx) * g.dx;
+        const float ycf = ((float)iy + g.wy) * g.dy;
+        const float tp = xcf * v.cos_a - ycf * v.sin_a;
+        const float ds = g.sad + xcf * v.sin_a + ycf * v.cos_a;
+        const float r = __fdividef(tp, ds);
+        float u;
+        if (g.det == 1) {
+            u = g.sdd_du * r;
+        } else if (g.det == 0) {
+            u = g.sdd_du * atanf(r);
+        } else {  // arc (candidate search only; the footprints are exact)
+            const float gam = atanf(r);
+            u = (gam + asinf(g.sad_add * sinf(gam))) * g.add / g.du;
+        }
+        return u - g.wu + 0.5f;
+    };
+    for (int L = t; L < nlines; L += NT) {
+        auto f = [&](int p) { return rows ? centre_u(p, L) : centre_u(L, p); };
+        const bool inc = f(npos - 1) >= f(0);
+        int lo = 0, hi = npos;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            const float fm = f(mid);
+            if (inc ? (fm < ulo) : (fm > uhi)) lo = mid + 1; else hi = mid;
+        }
+        const int first = lo;
+        hi = npos;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            const float fm = f(mid);
+            if (inc ? (fm > uhi) : (fm < ulo)) hi = mid; else lo = mid + 1;
+        }
+        line_start[L] = first;
+        line_off[L] = lo - first;
+    }
+    __syncthreads();
+    const int per = (nlines + NT - 1) / NT;
+    const int b = t * per, e = min(b + per, nlines);
+    int sum = 0;
+    for (int L = b; L < e; L++) sum += line_off[L];
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int n = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += n;
+    }
+    if (lane == 31) s_warp_tot[warp] = incl;
+    __syncthreads();
+    int wbase = 0;
+    for (int w = 0; w < warp; w++) wbase += s_warp_tot[w];
+    int run = wbase + incl - sum;
+    __syncthreads();
+    for (int L = b; L < e; L++) {
+        const int c = line_off[L];
+        line_off[L] = run;
+        run += c;
+    }
+    if (t == NT - 1) line_off[nlines] = run;
+    __syncthreads();
+    return line_off[nlines];
+}
+
+// The work of one block.  bar: the block's two stage mbarriers (initialised once per
+// block); phase: their next-completion parities (bit b for buffer b), carried across
+// the items of a persistent block; acc4: the shared memory past the mbarriers.  Returns
+// false when a stage wait ran out (the block has then set kErrStageWait, waited for its
+// copies in flight and must stop).
+template <int METHOD, int GROUPS>
+__device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__restrict__ views,
+                                                  const float *__restrict__ xs, const float *__restrict__ ampv,
+                                                  const uint8_t *__restrict__ map, void *__restrict__ proj,
+                                                  int out_dtype, int view_begin, int view_stride, float margin,
+                                                  int slots, int *__restrict__ err, float4 *acc4, uint64_t *bar,
+                                                  unsigned &phase, int bx, int by) {
+    const int NT = blockDim.x;
+    const int R = NT / GROUPS;
+    const int nv = g.nv;
+    const int nq = (nv + 3) >> 2;
+    const int nlines0 = max(g.nx, g.ny);
+    const int xst = g.xstride;
+    StagedSmem L{nq, NT, nlines0, GROUPS, slots, xst};
+    float *stage = reinterpret_cast<float *>(acc4 + GROUPS * kTU * nq);  // [2][slots][xst]
+    int *c_col = reinterpret_cast<int *>(stage + 2 * L.stage_floats());
+    float *c_b0 = reinterpret_cast<float *>(c_col + NT);
+    float *c_iz = c_b0 + NT;
+    int *c_rr = reinterpret_cast<int *>(c_iz + NT);  // rlo | rhi << 16
+    int *c_jj = c_rr + NT;                            // jlo | jhi << 8
+    int *c_idx = c_jj + NT;                           // slots of the valid candidates, packed
+    float *c_w = reinterpret_cast<float *>(c_idx + NT);  // [NT][kTU]
+    int *line_start = reinterpret_cast<int *>(c_w + NT * kTU);
+    int *line_off = line_start + nlines0;
+    int *s_warp_tot = line_off + nlines0 + 1;  // [32]
+
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int grp = GROUPS == 1 ? 0 : t / R;
+    const int gwarp = GROUPS == 1 ? warp : (t - grp * R) >> 5;
+    const int iu0 = bx * kTU;
+    const View v = views[view_begin + by * view_stride];
+    for (int i = t; i < GROUPS * kTU * nq; i += NT) acc4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 *gacc = acc4 + grp * kTU * nq;
+    const bool rows = fabsf(v.cos_a) >= fabsf(v.sin_a);
+    const int nlines = rows ? g.ny : g.nx;
+    const int ncand = candidate_lines(g, v, iu0, margin, rows, line_start, line_off, s_warp_tot);
+    const float fnz = (float)g.nz;
+    const int rows_per_pass = 4 * R;
+    const unsigned col_bytes = (unsigned)xst * 4u;
+    int buf0 = 0;   // buffer of the next chunk's first slots
+    int vbase = 0;  // valid candidates of the earlier chunks
+
+    for (int c0 = 0; c0 < ncand; c0 += NT) {
+        // 1. exact footprint of candidate c0 + t into slot t; the valid slots are packed
+        // into the index list c_idx
+        bool valid = false;
+        {
+            const int c = c0 + t;
+            if (c < ncand) {
+                int a = 0, bnd = nlines - 1;  // last line with line_off <= c
+                while (a < bnd) {
+                    const int mid = (a + bnd + 1) >> 1;
+                    if (line_off[mid] <= c) a = mid; else bnd = mid - 1;
+                }
+                const int pos = line_start[a] + (c - line_off[a]);
+                const int ix = rows ? pos : a, iy = rows ? a : pos;
+                const int col = iy * g.nx + ix;
+                if (map[col]) {
+                    const ColumnFP fp = column_footprint<METHOD>(g, v, ix, iy);
+                    if (fp.hit && fp.iumax >= iu0 && fp.iumin <= iu0 + kTU - 1) {
+                        const int jlo = max(fp.iumin, iu0) - iu0, jhi = min(fp.iumax, iu0 + kTU - 1) - iu0;
+                        const float scl = fp.ampu * fp.zinc;
+#pragma unroll
+                        for (int j = 0; j < kTU; j++) {
+                            float w = 0.0f;
+                            if (j >= jlo && j <= jhi)
+                                w = u_weight<METHOD>(iu0 + j, fp.iumin, fp.iumax, fp.p0, fp.p1, fp.p2, fp.p3) * scl;
+                            c_w[t * kTU + j] = w;
+                        }
+                        const float b0 = fp.vstart + 0.5f;
+                        const float btop = fmaf(fnz, fp.zinc, b0);
+                        const int rlo = max((int)floorf(b0) - 1, 0);
+                        const int rhi = min((int)floorf(btop) + 1, nv - 1);
+                        if (rlo <= rhi) {
+                            valid = true;
+                            const float izc = 1.0f / fp.zinc;
+                            c_col[t] = col;
+                            c_b0[t] = -b0 * izc;  // s(iv) = iv / zinc - b0 / zinc
+                            c_iz[t] = izc;
+                            c_rr[t] = rlo | (rhi << 16);
+                            c_jj[t] = jlo | (jhi << 8);
+                        }
+                    }
+                }
+            }
+        }
+        const unsigned bal = __ballot_sync(kFull, valid);
+        if (lane == 0) s_warp_tot[warp] = __popc(bal);
+        __syncthreads();
+        int base = 0, nval = 0;
+        for (int w = 0; w < (NT >> 5); w++) {
+            const int n = s_warp_tot[w];
+            base += w < warp ? n : 0;
+            nval += n;
+        }
+        if (valid) c_idx[base + __popc(bal & ((1u << lane) - 1u))] = t;
+        __syncthreads();
+
+        // 2. the packed candidates, `slots` at a time: warp 0 issues the copies of the next
+        // slots into the other buffer while every warp runs the rows of the current ones
+        const int nsub = (nval + slots - 1) / slots;
+        auto issue = [&](int sub, int buf) {
+            const int p0 = sub * slots, n = min(slots, nval - p0);
+            if (lane == 0) mbar_arrive_expect(&bar[buf], (unsigned)n * col_bytes);
+            __syncwarp();
+            float *dst = stage + (size_t)buf * L.stage_floats();
+            for (int i = lane; i < n; i += 32)
+                bulk_copy_g2s(dst + (size_t)i * xst, xs + (size_t)c_col[c_idx[p0 + i]] * xst, col_bytes, &bar[buf]);
+        };
+        if (nsub > 0 && warp == 0) issue(0, buf0);
+        for (int sub = 0; sub < nsub; sub++) {
+            const int buf = (buf0 + sub) & 1;
+            if (sub + 1 < nsub && warp == 0) issue(sub + 1, buf ^ 1);
+            const bool ok = mbar_wait(&bar[buf], (phase >> buf) & 1u);
+            phase ^= 1u << buf;
+            const uint32_t sb = smem_addr(stage + (size_t)buf * L.stage_floats()) - (0x4B000000u << 2);
+            const int p0 = sub * slots, p1 = min(nval, p0 + slots);
+            // group g takes the valid candidates whose position in the block's whole sequence of
+            // valid candidates (vbase + p) is g mod GROUPS, in order: the same split and order
+            // whatever the chunk, row-thread or slot counts
+            const int pstart0 = p0 + (((grp - vbase - p0) % GROUPS) + GROUPS) % GROUPS;
+            for (int p = pstart0; p < p1; p += GROUPS) {
+                const int q = c_idx[p];
+                const int rr = c_rr[q];
+                const int prlo = rr & 0xffff, prhi = rr >> 16;
+                const float psa = c_b0[q], piz = c_iz[q];
+                const int jj = c_jj[q];
+                const int pjlo = jj & 0xff, pjhi = jj >> 8;
+                const uint32_t xadj = sb + (uint32_t)((p - p0) * xst) * 4u;
+                const float *wq = c_w + q * kTU + pjlo;
+                const bool walk = R == 32;
+                const int pstart = walk ? (prlo & ~3) : 0, pend = walk ? prhi + 1 : nv;
+                for (int pbase = pstart; pbase < pend; pbase += rows_per_pass) {
+                    const int wrow = pbase + 128 * gwarp;
+                    if (wrow > prhi || wrow + 127 < prlo) continue;  // warp-uniform
+                    // boundary iv sits at s = iv / zinc - b0 / zinc, one rounding from iv alone, so
+                    // a row's value does not depend on which lane or warp evaluates it
+                    const int iv0 = wrow + 4 * lane;
+                    const float f0 = small_int_to_float(iv0);
+                    const float X0 = staged_integral(xadj, fmaf(f0, piz, psa), fnz);
+                    const float X1 = staged_integral(xadj, fmaf(f0 + 1.0f, piz, psa), fnz);
+                    const float X2 = staged_integral(xadj, fmaf(f0 + 2.0f, piz, psa), fnz);
+                    const float X3 = staged_integral(xadj, fmaf(f0 + 3.0f, piz, psa), fnz);
+                    float X4 = __shfl_down_sync(kFull, X0, 1);
+                    if (lane == 31) X4 = staged_integral(xadj, fmaf(f0 + 4.0f, piz, psa), fnz);
+                    if (iv0 <= prhi && iv0 + 3 >= prlo && iv0 < nv) {
+                        const float R0 = X1 - X0, R1 = X2 - X1, R2 = X3 - X2, R3 = X4 - X3;
+                        const uint32_t a = smem_addr(gacc + (iv0 >> 2) + pjlo * nq);
+                        const uint32_t step = (uint32_t)nq * 16u;
+                        acc_add4(a, wq[0], R0, R1, R2, R3);
+                        if (pjhi > pjlo) {
+                            acc_add4(a + step, wq[1], R0, R1, R2, R3);
+                            if (pjhi > pjlo + 1) {
+                                acc_add4(a + 2 * step, wq[2], R0, R1, R2, R3);
+                                for (int j = 3; j <= pjhi - pjlo; j++) acc_add4(a + j * step, wq[j], R0, R1, R2, R3);
+                            }
+                        }
+                    }
+                }
+            }
+            // every warp is done with buffer `buf` before the copies of slots sub + 2 reuse it
+            if (__syncthreads_or(!ok)) {
+                if (t == 0) atomicOr(err, kErrStageWait);
+                // let the copies in flight land before the block stops (bounded waits)
+                mbar_wait(&bar[buf], ((phase >> buf) & 1u) ^ 1u);
+                if (sub + 1 < nsub) mbar_wait(&bar[buf ^ 1], (phase >> (buf ^ 1)) & 1u);
+                return false;
+            }
+        }
+        buf0 = (buf0 + nsub) & 1;
+        vbase += nval;
+    }
+    if (ncand == 0) __syncthreads();
+    // 3. sum of the groups (in group order), axial amplitude and store
+    const size_t obase = (size_t)by * g.nu * nv;
+    const float *accf = reinterpret_cast<const float *>(acc4);
+    const int gstride = kTU * 4 * nq;
+    for (int j = 0; j < kTU; j++) {
+        const int iu = iu0 + j;
+        if (iu >= g.nu) break;
+        for (int iv = t; iv < nv; iv += NT) {
+            float a = accf[j * 4 * nq + iv];
+#pragma unroll
+            for (int q = 1; q < GROUPS; q++) a += accf[q * gstride + j * 4 * nq + iv];
+            store_from_float(proj, obase + (size_t)iu * nv + iv, a * ampv[(size_t)iu * nv + iv], out_dtype);
+        }
+    }
+    return true;
+}
+
+template <int METHOD, int GROUPS>
+__global__ void __launch_bounds__(kProjMaxThreads, 3) proj_staged_kernel(Geom g, const View *__restrict__ views,
+                                                                      const float *__restrict__ xs,
+                                                                      const float *__restrict__ ampv,
+                                                                      const uint8_t *__restrict__ map,
+                                                                      void *__restrict__ proj, int out_dtype,
+                                                                      int view_begin, int view_stride, float margin,
+                                                                      int slots, int *__restrict__ err, int vgroup) {
+    extern __shared__ float4 smem_staged[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_staged);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    unsigned phase = 0;
+    proj_staged_block<METHOD, GROUPS>(g, views, xs, ampv, map, proj, out_dtype, view_begin, view_stride, margin,
+                                      slots, err, smem_staged + 1, bar, phase, blockIdx.x / vgroup,
+                                      blockIdx.y * vgroup + blockIdx.x % vgroup);
 }
 
 // ---------------------------------------------------------------------------
@@ -768,10 +1153,11 @@ cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, co
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, bool pairs, cudaStream_t st) {
+cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, bool pairs, int xstride,
+                          cudaStream_t st) {
     const int blocks = (nxy + 31) / 32;
-    if (pairs) prefix_kernel<true><<<blocks, 256, 0, st>>>(image, in_dtype, xs, nxy, nz);
-    else prefix_kernel<false><<<blocks, 256, 0, st>>>(image, in_dtype, xs, nxy, nz);
+    if (pairs) prefix_kernel<true><<<blocks, 256, 0, st>>>(image, in_dtype, xs, nxy, nz, 0);
+    else prefix_kernel<false><<<blocks, 256, 0, st>>>(image, in_dtype, xs, nxy, nz, xstride);
     return cudaGetLastError();
 }
 
@@ -802,12 +1188,56 @@ size_t proj_smem_bytes(int nv, int nx, int ny, int groups) {
 int proj_group_width() { return kTU; }
 int proj_max_lines() { return kMaxLines; }
 
+// Views per group of the forward projector's launch order: the largest of 8 .. 1 that
+// divides the view count (every group full).
+int proj_view_group(int vc) {
+    for (int v = 8; v > 1; v--)
+        if (vc % v == 0) return v;
+    return 1;
+}
+
+size_t proj_staged_smem_bytes(int nv, int nx, int ny, int xstride, int groups, int rows, int slots) {
+    StagedSmem L{(nv + 3) / 4, rows * groups, std::max(nx, ny), groups, slots, xstride};
+    return L.bytes();
+}
+// Slots per stage buffer: 1 .. 64, and one buffer's bytes within an mbarrier phase's
+// transaction count (< 2^20).
+bool proj_slots_valid(int xstride, int slots) {
+    return slots >= 1 && slots <= 64 && (size_t)slots * xstride * 4 < (1u << 20);
+}
+
+cudaError_t launch_proj_staged(int method, int groups, int rows, int slots, const Geom &g, const View *views,
+                               const float *xs, const float *ampv, const uint8_t *map, void *proj, int out_dtype,
+                               int vb, int vs, int vc, float margin, int *err, cudaStream_t st) {
+    if (!proj_shape_valid(g.nv, groups, rows) || !proj_slots_valid(g.xstride, slots) ||
+        g.xstride % 4 != 0 || g.xstride < g.nz + 2 || reinterpret_cast<uintptr_t>(xs) % 16 != 0)
+        return cudaErrorInvalidValue;
+    const size_t sm = proj_staged_smem_bytes(g.nv, g.nx, g.ny, g.xstride, groups, rows, slots);
+    const int vg = proj_view_group(vc);
+    dim3 grid((g.nu + kTU - 1) / kTU * vg, vc / vg);
+    const int nt = rows * groups;
+#define CTSIM_PROJ_STAGED_CASE(M, GR)                                                                 \
+    if (method == M && groups == GR) {                                                                \
+        cudaError_t e = allow_dynamic_smem((const void *)proj_staged_kernel<M, GR>, sm);              \
+        if (e != cudaSuccess) return e;                                                               \
+        proj_staged_kernel<M, GR><<<grid, nt, sm, st>>>(g, views, xs, ampv, map, proj, out_dtype, vb, vs, margin, \
+                                                        slots, err, vg);                              \
+        return cudaGetLastError();                                                                    \
+    }
+    CTSIM_PROJ_STAGED_CASE(kDD, 1) CTSIM_PROJ_STAGED_CASE(kDD, 2) CTSIM_PROJ_STAGED_CASE(kDD, 4)
+    CTSIM_PROJ_STAGED_CASE(kDD, 8) CTSIM_PROJ_STAGED_CASE(kTF, 1) CTSIM_PROJ_STAGED_CASE(kTF, 2)
+    CTSIM_PROJ_STAGED_CASE(kTF, 4) CTSIM_PROJ_STAGED_CASE(kTF, 8)
+#undef CTSIM_PROJ_STAGED_CASE
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_proj(int method, int groups, int rows, bool pairs, const Geom &g, const View *views,
                         const float *xc, const float *ampv, const uint8_t *map, void *proj, int out_dtype, int vb,
                         int vs, int vc, float margin, cudaStream_t st) {
     if (!proj_shape_valid(g.nv, groups, rows)) return cudaErrorInvalidValue;
     const size_t sm = proj_smem_bytes(g.nv, g.nx, g.ny, groups, rows);
-    dim3 grid((g.nu + kTU - 1) / kTU, vc);
+    const int vg = proj_view_group(vc);
+    dim3 grid((g.nu + kTU - 1) / kTU * vg, vc / vg);
     // one thread per 4 detector rows (rows threads per group, more rows loop), groups
     // of those threads share the candidates
     const int nt = rows * groups;
@@ -815,7 +1245,7 @@ cudaError_t launch_proj(int method, int groups, int rows, bool pairs, const Geom
     if (method == M && groups == GR && pairs == P) {                                                  \
         cudaError_t e = allow_dynamic_smem((const void *)proj_kernel<M, GR, P>, sm);                  \
         if (e != cudaSuccess) return e;                                                               \
-        proj_kernel<M, GR, P><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin); \
+        proj_kernel<M, GR, P><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin, vg); \
         return cudaGetLastError();                                                                    \
     }
     CTSIM_PROJ_CASE(kDD, 1, false) CTSIM_PROJ_CASE(kDD, 2, false) CTSIM_PROJ_CASE(kDD, 4, false)
@@ -912,6 +1342,37 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_batch_kernel(const __gri
     }
 }
 
+// The staged forward projector over the flat blocks of many plans (same group count,
+// row threads and slots; each task its own geometry and scratch); the mbarriers and their
+// phases persist across the items of a block.
+template <int METHOD, int GROUPS, bool LOWP>
+__global__ void __launch_bounds__(kProjMaxThreads, 3) proj_staged_batch_kernel(const __grid_constant__ ProjBatch b,
+                                                                               int slots) {
+    extern __shared__ float4 smem_staged_batch[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_staged_batch);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    unsigned phase = 0;
+    for (int blk = blockIdx.x; blk < b.total; blk += gridDim.x) {
+        int lo = 0, hi = b.n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (b.t[mid].first <= blk) lo = mid; else hi = mid - 1;
+        }
+        const ProjTask &T = b.t[lo];
+        const int local = blk - T.first;
+        if (!proj_staged_block<METHOD, GROUPS>(T.g, T.views, T.xs, T.ampv, T.map, T.proj, LOWP ? T.out_dtype : kF32,
+                                               T.vb, T.vs, T.margin, slots, T.err, smem_staged_batch + 1, bar, phase,
+                                               local % T.gx, local / T.gx))
+            return;
+        __syncthreads();  // the next item reuses the shared accumulators and tables
+    }
+}
+
 template <int METHOD, int MZ, bool VEC, bool LOWP>
 __global__ void __launch_bounds__(256) back_batch_kernel(const __grid_constant__ BackBatch b) {
     extern __shared__ float smem_batch[];
@@ -959,6 +1420,24 @@ cudaError_t launch_proj_batch(int method, int groups, int row_threads, bool pair
     CTSIM_PB_CASE(kDD, 1) CTSIM_PB_CASE(kDD, 2) CTSIM_PB_CASE(kDD, 4) CTSIM_PB_CASE(kDD, 8)
     CTSIM_PB_CASE(kTF, 1) CTSIM_PB_CASE(kTF, 2) CTSIM_PB_CASE(kTF, 4) CTSIM_PB_CASE(kTF, 8)
 #undef CTSIM_PB_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_proj_staged_batch(int method, int groups, int row_threads, int slots, bool lowp, size_t smem,
+                                     const ProjBatch &b, cudaStream_t st) {
+    if (b.n < 1 || b.total < 1) return cudaSuccess;
+    const int nt = row_threads * groups;
+#define CTSIM_PSB_CASE(M, GR)                                                                         \
+    if (method == M && groups == GR) {                                                                \
+        auto k = lowp ? proj_staged_batch_kernel<M, GR, true> : proj_staged_batch_kernel<M, GR, false>; \
+        cudaError_t e = allow_dynamic_smem((const void *)k, smem);                                    \
+        if (e != cudaSuccess) return e;                                                               \
+        k<<<persistent_grid(k, nt, smem, b.total), nt, smem, st>>>(b, slots);                         \
+        return cudaGetLastError();                                                                    \
+    }
+    CTSIM_PSB_CASE(kDD, 1) CTSIM_PSB_CASE(kDD, 2) CTSIM_PSB_CASE(kDD, 4) CTSIM_PSB_CASE(kDD, 8)
+    CTSIM_PSB_CASE(kTF, 1) CTSIM_PSB_CASE(kTF, 2) CTSIM_PSB_CASE(kTF, 4) CTSIM_PSB_CASE(kTF, 8)
+#undef CTSIM_PSB_CASE
     return cudaErrorInvalidValue;
 }
 

@@ -24,7 +24,8 @@ cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const
                                  cudaStream_t st);
 
 // pairs: the (X, slope) layout of the column prefix sums (forward_pairs below)
-cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, bool pairs, cudaStream_t st);
+cudaError_t launch_prefix(const void *image, int in_dtype, float *xs, int nxy, int nz, bool pairs, int xstride,
+                          cudaStream_t st);
 
 cudaError_t launch_proj(int method, int groups, int rows, bool pairs, const Geom &g, const View *views,
                         const float *xs, const float *ampv, const uint8_t *map, void *proj, int out_dtype,
@@ -36,6 +37,16 @@ int proj_default_rows(int nv);
 bool proj_groups_valid(int nv, int groups);
 bool proj_shape_valid(int nv, int groups, int rows);
 size_t proj_smem_bytes(int nv, int nx, int ny, int groups, int rows);
+// The forward projector with each candidate's prefix column staged in shared memory by
+// bulk copies (plain layout, g.xstride a multiple of 4 and >= nz + 2, xs 16-byte aligned):
+// `slots` columns per stage buffer, two buffers.  A stage wait that runs out sets bit 4
+// of *err.
+cudaError_t launch_proj_staged(int method, int groups, int rows, int slots, const Geom &g, const View *views,
+                               const float *xs, const float *ampv, const uint8_t *map, void *proj, int out_dtype,
+                               int view_begin, int view_stride, int view_count, float margin, int *err,
+                               cudaStream_t st);
+size_t proj_staged_smem_bytes(int nv, int nx, int ny, int xstride, int groups, int rows, int slots);
+bool proj_slots_valid(int xstride, int slots);
 
 // voxel-driven bilinear modes: back,pd (v outside the detector skipped), back,hpd (v
 // clamped), back,var (geom/cbct/cbct_back_var.c)
@@ -61,6 +72,7 @@ struct ProjTask {
     int out_dtype;
     int vb, vs, gx, first;  // view selection, blocks along u, first flat block of the task
     float margin;
+    int *err;               // the plan's error flag (staged projector: a stage wait that ran out)
 };
 struct ProjBatch {
     int n, total;  // tasks, flat blocks of all tasks
@@ -92,6 +104,9 @@ cudaError_t launch_proj_batch(int method, int groups, int row_threads, bool pair
                               const ProjBatch &b, cudaStream_t st);
 cudaError_t launch_back_batch(int method, int mz, bool vec, bool lowp, size_t smem, const BackBatch &b,
                               cudaStream_t st);
+// The staged forward projector (launch_proj_staged) over a batch of plain-layout plans.
+cudaError_t launch_proj_staged_batch(int method, int groups, int row_threads, int slots, bool lowp, size_t smem,
+                                     const ProjBatch &b, cudaStream_t st);
 
 // Raises (never lowers) a kernel's dynamic shared-memory limit on the current device.
 cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes);

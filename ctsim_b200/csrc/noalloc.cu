@@ -124,6 +124,7 @@ extern "C" ctsim_status ctsim_back_dd_noalloc(const ctsim_geom *geom, const doub
     g.wv = centre(G.nv, G.offset_v);
     g.sdd_du = G.sdd / G.du;
     g.dz_dv = G.dz / G.dv;
+    g.xstride = prefix_stride(G.nz);
     double rmax = 0.0;
     for (int cx = 0; cx < 2; cx++)
         for (int cy = 0; cy < 2; cy++) {

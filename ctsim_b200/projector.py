@@ -127,6 +127,11 @@ def _mex_call(projType, geom: CTGeometry, data):
 # ---------------------------------------------------------------------------
 # Device plans
 # ---------------------------------------------------------------------------
+def _tuning_dict(t) -> dict:
+    return {"proj_groups": t.proj_groups, "proj_rows": t.proj_rows, "proj_layout": t.proj_layout,
+            "proj_slots": t.proj_slots, "back_mz": t.back_mz, "back_mz_tf": t.back_mz_tf, "pd_mz": t.pd_mz}
+
+
 class Plan:
     """Device-resident projector plan for one geometry (all of its views).
 
@@ -166,13 +171,12 @@ class Plan:
         """Launch shapes: forward candidate groups, A^T and FDK z-pass depths."""
         t = _lib.CtsimTuning()
         _lib.check(self._L.ctsim_plan_get_tuning(self._h, C.byref(t)), "ctsim_plan_get_tuning")
-        return {"proj_groups": t.proj_groups, "proj_rows": t.proj_rows, "proj_layout": t.proj_layout,
-                "back_mz": t.back_mz, "back_mz_tf": t.back_mz_tf, "pd_mz": t.pd_mz}
+        return _tuning_dict(t)
 
     def set_tuning(self, proj_groups: int = 0, back_mz: int = 0, pd_mz: int = 0, back_mz_tf: int = 0,
-                   proj_rows: int = 0, proj_layout: int = 0):
+                   proj_rows: int = 0, proj_layout: int = 0, proj_slots: int = 0):
         t = _lib.CtsimTuning(int(proj_groups), int(back_mz), int(pd_mz), int(back_mz_tf), int(proj_rows),
-                             int(proj_layout))
+                             int(proj_layout), int(proj_slots))
         _lib.check(self._L.ctsim_plan_set_tuning(self._h, C.byref(t)), "ctsim_plan_set_tuning")
 
     def autotune(self, method: str, sample_views: int = 0) -> dict:
@@ -186,8 +190,7 @@ class Plan:
         with torch.cuda.device(self.device):
             _lib.check(self._L.ctsim_plan_autotune(self._h, m, int(sample_views), st, C.byref(t)),
                        "ctsim_plan_autotune")
-        return {"proj_groups": t.proj_groups, "proj_rows": t.proj_rows, "proj_layout": t.proj_layout,
-                "back_mz": t.back_mz, "back_mz_tf": t.back_mz_tf, "pd_mz": t.pd_mz}
+        return _tuning_dict(t)
 
     @property
     def device_bytes(self) -> int:

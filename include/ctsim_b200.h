@@ -191,7 +191,9 @@ typedef struct {
                        of each candidate's shadow */
     int proj_layout; /* column prefix sums: 1 plain sums, 2 (sum, slope) pairs (one 8-byte load
                         per evaluation; twice the bytes; plans whose pairs take at most 160 MB
-                        start with 2 and may switch) */
+                        start with 2 and may switch), 3 plain sums with each candidate column
+                        copied into shared memory by the copy engine before its rows are summed */
+    int proj_slots;  /* layout 3: prefix columns per stage buffer (two buffers), 1 .. 64 */
 } ctsim_tuning;
 ctsim_status ctsim_plan_get_tuning(const ctsim_plan *plan, ctsim_tuning *tuning);
 ctsim_status ctsim_plan_set_tuning(ctsim_plan *plan, const ctsim_tuning *tuning);

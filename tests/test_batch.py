@@ -16,11 +16,16 @@ def _plans():
     return [(cases[n], Plan(cases[n])) for n in names]
 
 
+@pytest.mark.parametrize("staged", [False, True])
 @pytest.mark.parametrize("method", ["dd", "tf"])
-def test_batched_launches_equal_per_plan_calls(method):
+def test_batched_launches_equal_per_plan_calls(method, staged):
     import torch
     from ctsim_b200.projector import batch_backproject, batch_project
     gp = _plans()
+    if staged:  # forward projections staged through shared memory: two slot counts and the plans' defaults mixed
+        for k, (g, p) in enumerate(gp):
+            if k % 3 != 2:
+                p.set_tuning(proj_layout=3, proj_slots=8 if k % 3 == 0 else 2)
     xs, ys = [], []
     for k, (g, p) in enumerate(gp):
         x, y = case_inputs(g, seed=20 + k)

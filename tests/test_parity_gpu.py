@@ -51,6 +51,24 @@ def test_cuda_matches_golden(name):
             assert np.array_equal(got, ref), f"{name} {k}: not bit-identical (max {np.abs(got - ref).max():.3e})"
 
 
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("slots", [1, 8])
+def test_staged_forward_projector_matches_golden(name, slots):
+    """The forward projector with the candidates' prefix columns staged in shared memory
+    (layout 3), whatever the plan's default, against the reference's outputs."""
+    import torch
+    g = CASES[name]
+    d = np.load(os.path.join(GOLDEN_DIR, f"{name}.npz"))
+    plan = Plan(g)
+    plan.set_tuning(proj_layout=3, proj_slots=slots)
+    xd = torch.from_numpy(np.ascontiguousarray(d["image_in"])).cuda()
+    for m in ("dd", "tf"):
+        got = plan.project(xd, m).cpu().numpy()
+        plan.check()
+        err = rel_l2(got, d[f"proj_{m}"])
+        assert err <= REL_L2, f"{name} proj,{m} (staged, {slots} slots): rel L2 {err:.3e}"
+
+
 @pytest.mark.parametrize("name", ["basic", "offsets_curved", "thick_slices", "ragged"])
 def test_device_plan_matches_oracle_and_is_adjoint(name):
     import torch
@@ -232,11 +250,12 @@ def test_launch_shapes_keep_parity_and_autotune():
     plan = Plan(g)
     hpd0 = plan.backproject(yd, "hpd").cpu().numpy()
     for G in (1, 2, 4, 8):
-        for layout in (1, 2):  # plain prefix sums / (sum, slope) pairs
+        # plain prefix sums / (sum, slope) pairs / plain sums staged in shared memory (1 or 8 slots)
+        for layout, slots in ((1, 0), (2, 0), (3, 1), (3, 8)):
             same = None
             for R in (64, 32):  # fewer row threads than rows: passes; 32: walks each candidate's rows
                 try:
-                    plan.set_tuning(proj_groups=G, proj_rows=R, proj_layout=layout)
+                    plan.set_tuning(proj_groups=G, proj_rows=R, proj_layout=layout, proj_slots=slots)
                 except CtsimError:
                     continue
                 for m in ("dd", "tf"):
