@@ -641,6 +641,21 @@ __device__ __forceinline__ float staged_integral(uint32_t xadj, float s, float f
     asm volatile("ld.shared.f32 %0, [%2];\n\tld.shared.f32 %1, [%2+4];" : "=f"(x0), "=f"(x1) : "r"(a));
     return fmaf(s - (t - kTwo23), x1 - x0, x0);
 }
+__device__ __forceinline__ float lds_f32(uint32_t a) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ int lds_s32(uint32_t a) {
+    int v;
+    asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ float4 lds_f32x4(uint32_t a) {
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
 // acc += w * (r0, r1, r2, r3) on the float4 at shared address a.
 __device__ __forceinline__ void acc_add4(uint32_t a, float w, float r0, float r1, float r2, float r3) {
     float4 v;
@@ -759,12 +774,10 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
     const int xst = g.xstride;
     StagedSmem L{nq, NT, nlines0, GROUPS, slots, xst};
     float *stage = reinterpret_cast<float *>(acc4 + GROUPS * kTU * nq);  // [2][slots][xst]
-    int *c_col = reinterpret_cast<int *>(stage + 2 * L.stage_floats());
-    float *c_b0 = reinterpret_cast<float *>(c_col + NT);
-    float *c_iz = c_b0 + NT;
-    int *c_rr = reinterpret_cast<int *>(c_iz + NT);  // rlo | rhi << 16
-    int *c_jj = c_rr + NT;                            // jlo | jhi << 8
-    int *c_idx = c_jj + NT;                           // slots of the valid candidates, packed
+    // per candidate slot: {-b0 / zinc, 1 / zinc, rlo | rhi << 16, jlo | jhi << 8} (one 16-byte load)
+    float4 *c_prm = reinterpret_cast<float4 *>(stage + 2 * L.stage_floats());
+    int *c_col = reinterpret_cast<int *>(c_prm + NT);
+    int *c_idx = c_col + NT;                          // slots of the valid candidates, packed
     float *c_w = reinterpret_cast<float *>(c_idx + NT);  // [NT][kTU]
     int *line_start = reinterpret_cast<int *>(c_w + NT * kTU);
     int *line_off = line_start + nlines0;
@@ -777,6 +790,9 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
     const View v = views[view_begin + by * view_stride];
     for (int i = t; i < GROUPS * kTU * nq; i += NT) acc4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     float4 *gacc = acc4 + grp * kTU * nq;
+    // 32-bit shared addresses of the row loop's tables
+    const uint32_t acc_u32 = smem_addr(gacc), nq16 = 16u * (uint32_t)nq;
+    const uint32_t idx_u32 = smem_addr(c_idx), prm_u32 = smem_addr(c_prm), w_u32 = smem_addr(c_w);
     const bool rows = fabsf(v.cos_a) >= fabsf(v.sin_a);
     const int nlines = rows ? g.ny : g.nx;
     const int ncand = candidate_lines(g, v, iu0, margin, rows, line_start, line_off, s_warp_tot);
@@ -821,10 +837,9 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
                             valid = true;
                             const float izc = 1.0f / fp.zinc;
                             c_col[t] = col;
-                            c_b0[t] = -b0 * izc;  // s(iv) = iv / zinc - b0 / zinc
-                            c_iz[t] = izc;
-                            c_rr[t] = rlo | (rhi << 16);
-                            c_jj[t] = jlo | (jhi << 8);
+                            // s(iv) = iv / zinc - b0 / zinc
+                            c_prm[t] = make_float4(-b0 * izc, izc, __int_as_float(rlo | (rhi << 16)),
+                                                   __int_as_float(jlo | (jhi << 8)));
                         }
                     }
                 }
@@ -866,14 +881,15 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
             // whatever the chunk, row-thread or slot counts
             const int pstart0 = p0 + (((grp - vbase - p0) % GROUPS) + GROUPS) % GROUPS;
             for (int p = pstart0; p < p1; p += GROUPS) {
-                const int q = c_idx[p];
-                const int rr = c_rr[q];
+                const int q = lds_s32(idx_u32 + 4u * (uint32_t)p);
+                const float4 prm = lds_f32x4(prm_u32 + 16u * (uint32_t)q);
+                const int rr = __float_as_int(prm.z), jj = __float_as_int(prm.w);
                 const int prlo = rr & 0xffff, prhi = rr >> 16;
-                const float psa = c_b0[q], piz = c_iz[q];
-                const int jj = c_jj[q];
-                const int pjlo = jj & 0xff, pjhi = jj >> 8;
+                const float psa = prm.x, piz = prm.y;
+                const int pjlo = jj & 0xff, pjn = (jj >> 8) - pjlo;  // columns jlo .. jlo + pjn
                 const uint32_t xadj = sb + (uint32_t)((p - p0) * xst) * 4u;
-                const float *wq = c_w + q * kTU + pjlo;
+                const uint32_t wq = w_u32 + 4u * (uint32_t)(q * kTU + pjlo);
+                const uint32_t aq = acc_u32 + nq16 * (uint32_t)pjlo;
                 const bool walk = R == 32;
                 const int pstart = walk ? (prlo & ~3) : 0, pend = walk ? prhi + 1 : nv;
                 for (int pbase = pstart; pbase < pend; pbase += rows_per_pass) {
@@ -887,18 +903,19 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
                     const float X1 = staged_integral(xadj, fmaf(f0 + 1.0f, piz, psa), fnz);
                     const float X2 = staged_integral(xadj, fmaf(f0 + 2.0f, piz, psa), fnz);
                     const float X3 = staged_integral(xadj, fmaf(f0 + 3.0f, piz, psa), fnz);
-                    float X4 = __shfl_down_sync(kFull, X0, 1);
-                    if (lane == 31) X4 = staged_integral(xadj, fmaf(f0 + 4.0f, piz, psa), fnz);
-                    if (iv0 <= prhi && iv0 + 3 >= prlo && iv0 < nv) {
+                    const float X4 = staged_integral(xadj, fmaf(f0 + 4.0f, piz, psa), fnz);
+                    // rows outside the column's shadow [rlo, rhi] have both edges clamped to the same
+                    // end of the column, so their R is exactly 0: no per-lane shadow test
+                    if (iv0 < nv) {
                         const float R0 = X1 - X0, R1 = X2 - X1, R2 = X3 - X2, R3 = X4 - X3;
-                        const uint32_t a = smem_addr(gacc + (iv0 >> 2) + pjlo * nq);
-                        const uint32_t step = (uint32_t)nq * 16u;
-                        acc_add4(a, wq[0], R0, R1, R2, R3);
-                        if (pjhi > pjlo) {
-                            acc_add4(a + step, wq[1], R0, R1, R2, R3);
-                            if (pjhi > pjlo + 1) {
-                                acc_add4(a + 2 * step, wq[2], R0, R1, R2, R3);
-                                for (int j = 3; j <= pjhi - pjlo; j++) acc_add4(a + j * step, wq[j], R0, R1, R2, R3);
+                        const uint32_t a = aq + 4u * (uint32_t)iv0;  // float4 of rows iv0 .. iv0 + 3
+                        acc_add4(a, lds_f32(wq), R0, R1, R2, R3);
+                        if (pjn > 0) {
+                            acc_add4(a + nq16, lds_f32(wq + 4u), R0, R1, R2, R3);
+                            if (pjn > 1) {
+                                acc_add4(a + 2u * nq16, lds_f32(wq + 8u), R0, R1, R2, R3);
+                                for (int j = 3; j <= pjn; j++)
+                                    acc_add4(a + (uint32_t)j * nq16, lds_f32(wq + 4u * j), R0, R1, R2, R3);
                             }
                         }
                     }
