@@ -314,7 +314,10 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
         stretch = (1.0 + k * cg / std::sqrt(1.0 - k * k * sg * sg)) / (1.0 + k) * ((double)G.sad + G.add) / G.sdd;
         stretch = std::max(stretch, 1.0);
     }
-    p->margin = (float)std::ceil(0.5 * diag * G.sdd / dmin / G.du * stretch) + 2.0f;
+    // candidate window of the forward projector: a voxel's u footprint lies within this many
+    // pixels of its projected centre (half the voxel diagonal at the largest magnification,
+    // times the detector's stretch), plus half a pixel for the float search
+    p->margin = (float)(0.5 * diag * G.sdd / dmin / G.du * stretch * 1.0001 + 0.5);
     if (p->zinc_max > 9.0f) {
         // the kernels integrate the axial footprint exactly; the reference truncates
         // footprints wider than 10 rows (cbct_proj.c:395), which they do not reproduce

@@ -793,10 +793,37 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
     // 32-bit shared addresses of the row loop's tables
     const uint32_t acc_u32 = smem_addr(gacc), nq16 = 16u * (uint32_t)nq;
     const uint32_t idx_u32 = smem_addr(c_idx), prm_u32 = smem_addr(c_prm), w_u32 = smem_addr(c_w);
+    const float fnz = (float)g.nz;
+    // rows iv0 .. iv0 + 3 (f0 = iv0 as float) of one candidate: X at the five row edges from
+    // the staged column (xadj), R = X(iv + 1) - X(iv), added with the weights at wq into the
+    // accumulator columns at aq (pjn + 1 of them).  Boundary iv sits at s = iv / zinc -
+    // b0 / zinc (psa, piz), one rounding from iv alone, so a row's value does not depend on
+    // which lane, warp or pass evaluates it; rows outside the column's shadow have both
+    // edges clamped to the same end of the column and add exactly 0 (no per-lane test).
+    auto staged_rows = [&](int iv0, float f0, float psa, float piz, uint32_t xadj, uint32_t wq, uint32_t aq,
+                           int pjn) {
+        const float X0 = staged_integral(xadj, fmaf(f0, piz, psa), fnz);
+        const float X1 = staged_integral(xadj, fmaf(f0 + 1.0f, piz, psa), fnz);
+        const float X2 = staged_integral(xadj, fmaf(f0 + 2.0f, piz, psa), fnz);
+        const float X3 = staged_integral(xadj, fmaf(f0 + 3.0f, piz, psa), fnz);
+        const float X4 = staged_integral(xadj, fmaf(f0 + 4.0f, piz, psa), fnz);
+        if (iv0 < nv) {
+            const float R0 = X1 - X0, R1 = X2 - X1, R2 = X3 - X2, R3 = X4 - X3;
+            const uint32_t a = aq + 4u * (uint32_t)iv0;  // float4 of rows iv0 .. iv0 + 3
+            acc_add4(a, lds_f32(wq), R0, R1, R2, R3);
+            if (pjn > 0) {
+                acc_add4(a + nq16, lds_f32(wq + 4u), R0, R1, R2, R3);
+                if (pjn > 1) {
+                    acc_add4(a + 2u * nq16, lds_f32(wq + 8u), R0, R1, R2, R3);
+                    for (int j = 3; j <= pjn; j++)
+                        acc_add4(a + (uint32_t)j * nq16, lds_f32(wq + 4u * j), R0, R1, R2, R3);
+                }
+            }
+        }
+    };
     const bool rows = fabsf(v.cos_a) >= fabsf(v.sin_a);
     const int nlines = rows ? g.ny : g.nx;
     const int ncand = candidate_lines(g, v, iu0, margin, rows, line_start, line_off, s_warp_tot);
-    const float fnz = (float)g.nz;
     const int rows_per_pass = 4 * R;
     const unsigned col_bytes = (unsigned)xst * 4u;
     int buf0 = 0;   // buffer of the next chunk's first slots
@@ -880,44 +907,35 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
             // valid candidates (vbase + p) is g mod GROUPS, in order: the same split and order
             // whatever the chunk, row-thread or slot counts
             const int pstart0 = p0 + (((grp - vbase - p0) % GROUPS) + GROUPS) % GROUPS;
-            for (int p = pstart0; p < p1; p += GROUPS) {
-                const int q = lds_s32(idx_u32 + 4u * (uint32_t)p);
-                const float4 prm = lds_f32x4(prm_u32 + 16u * (uint32_t)q);
-                const int rr = __float_as_int(prm.z), jj = __float_as_int(prm.w);
-                const int prlo = rr & 0xffff, prhi = rr >> 16;
-                const float psa = prm.x, piz = prm.y;
-                const int pjlo = jj & 0xff, pjn = (jj >> 8) - pjlo;  // columns jlo .. jlo + pjn
-                const uint32_t xadj = sb + (uint32_t)((p - p0) * xst) * 4u;
-                const uint32_t wq = w_u32 + 4u * (uint32_t)(q * kTU + pjlo);
-                const uint32_t aq = acc_u32 + nq16 * (uint32_t)pjlo;
-                const bool walk = R == 32;
-                const int pstart = walk ? (prlo & ~3) : 0, pend = walk ? prhi + 1 : nv;
-                for (int pbase = pstart; pbase < pend; pbase += rows_per_pass) {
+            if (R == 32) {
+                // one-warp groups walk each candidate's own rows (every row of the group is theirs)
+                for (int p = pstart0; p < p1; p += GROUPS) {
+                    const int q = lds_s32(idx_u32 + 4u * (uint32_t)p);
+                    const float4 prm = lds_f32x4(prm_u32 + 16u * (uint32_t)q);
+                    const int rr = __float_as_int(prm.z), jj = __float_as_int(prm.w);
+                    const int prlo = rr & 0xffff, prhi = rr >> 16;
+                    const int pjlo = jj & 0xff;
+                    const uint32_t xadj = sb + (uint32_t)((p - p0) * xst) * 4u;
+                    for (int wrow = prlo & ~3; wrow <= prhi; wrow += 128)
+                        staged_rows(wrow + 4 * lane, small_int_to_float(wrow + 4 * lane), prm.x, prm.y, xadj,
+                                    w_u32 + 4u * (uint32_t)(q * kTU + pjlo), acc_u32 + nq16 * (uint32_t)pjlo,
+                                    (jj >> 8) - pjlo);
+                }
+            } else {
+                // fixed bands: warp gwarp owns rows pbase + 128 gwarp .. + 127 of each pass
+                for (int pbase = 0; pbase < nv; pbase += rows_per_pass) {
                     const int wrow = pbase + 128 * gwarp;
-                    if (wrow > prhi || wrow + 127 < prlo) continue;  // warp-uniform
-                    // boundary iv sits at s = iv / zinc - b0 / zinc, one rounding from iv alone, so
-                    // a row's value does not depend on which lane or warp evaluates it
                     const int iv0 = wrow + 4 * lane;
                     const float f0 = small_int_to_float(iv0);
-                    const float X0 = staged_integral(xadj, fmaf(f0, piz, psa), fnz);
-                    const float X1 = staged_integral(xadj, fmaf(f0 + 1.0f, piz, psa), fnz);
-                    const float X2 = staged_integral(xadj, fmaf(f0 + 2.0f, piz, psa), fnz);
-                    const float X3 = staged_integral(xadj, fmaf(f0 + 3.0f, piz, psa), fnz);
-                    const float X4 = staged_integral(xadj, fmaf(f0 + 4.0f, piz, psa), fnz);
-                    // rows outside the column's shadow [rlo, rhi] have both edges clamped to the same
-                    // end of the column, so their R is exactly 0: no per-lane shadow test
-                    if (iv0 < nv) {
-                        const float R0 = X1 - X0, R1 = X2 - X1, R2 = X3 - X2, R3 = X4 - X3;
-                        const uint32_t a = aq + 4u * (uint32_t)iv0;  // float4 of rows iv0 .. iv0 + 3
-                        acc_add4(a, lds_f32(wq), R0, R1, R2, R3);
-                        if (pjn > 0) {
-                            acc_add4(a + nq16, lds_f32(wq + 4u), R0, R1, R2, R3);
-                            if (pjn > 1) {
-                                acc_add4(a + 2u * nq16, lds_f32(wq + 8u), R0, R1, R2, R3);
-                                for (int j = 3; j <= pjn; j++)
-                                    acc_add4(a + (uint32_t)j * nq16, lds_f32(wq + 4u * j), R0, R1, R2, R3);
-                            }
-                        }
+                    for (int p = pstart0; p < p1; p += GROUPS) {
+                        const int q = lds_s32(idx_u32 + 4u * (uint32_t)p);
+                        const float4 prm = lds_f32x4(prm_u32 + 16u * (uint32_t)q);
+                        const int rr = __float_as_int(prm.z), jj = __float_as_int(prm.w);
+                        if (wrow > (rr >> 16) || wrow + 127 < (rr & 0xffff)) continue;  // warp-uniform
+                        const int pjlo = jj & 0xff;
+                        staged_rows(iv0, f0, prm.x, prm.y, sb + (uint32_t)((p - p0) * xst) * 4u,
+                                    w_u32 + 4u * (uint32_t)(q * kTU + pjlo), acc_u32 + nq16 * (uint32_t)pjlo,
+                                    (jj >> 8) - pjlo);
                     }
                 }
             }
