@@ -15,7 +15,8 @@
  *   mex -I<repo>/include cbct_geom_mex_b200.c -L<repo>/ctsim_b200/_lib -lctsim_b200
  *
  * and call it from geom/shell/forwardProjectMex.m / backProjectMex.m in place of
- * cbct_geom_mex.
+ * cbct_geom_mex.  Called with no arguments and no outputs it prints its usage, as the
+ * reference gateway prints its help (geom/cbct/cbct_geom_mex.c:317-320).
  */
 #include <string.h>
 
@@ -31,9 +32,24 @@ static int known_type(const char *t)
     return 0;
 }
 
+static void usage(void)
+{
+    mexPrintf("\n"
+              "  sino = cbct_geom_mex_b200(type, int32([nx ny nz]), single([dx dy dz]), single([ox oy oz]),\n"
+              "             int32([nu nv]), single([du dv]), single([ou ov]), single(SAD), single(ADD),\n"
+              "             single(SDD), int32(noViews), double(betas), single(couchZ),\n"
+              "             int32(flatPanel), single(data), logical(map))\n"
+              "  type: proj,dd | proj,tf  (data: image [nx ny nz] -> sinogram [nv nu noViews])\n"
+              "        back,dd | back,tf | back,pd | back,hpd | back,var  (sinogram -> image)\n");
+}
+
 void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[])
 {
     char type[16];
+    if (!nlhs && !nrhs) {
+        usage();
+        return;
+    }
     if (nrhs != 16 || !mxIsChar(prhs[0]) || mxGetString(prhs[0], type, sizeof(type)))
         mexErrMsgTxt("The 1st argument is invalid! \n");
     if (!known_type(type)) mexErrMsgTxt("Error: unknown geom type. \n");

@@ -28,10 +28,24 @@ static int known_type(const char *t)
     return 0;
 }
 
+static void usage(void)
+{
+    mexPrintf("\n"
+              "  sino = fbct_geom_mex_b200(type, int32([nx ny]), single([dx dy]), single([ox oy]),\n"
+              "             int32(nu), single(du), single(ou), single(SAD), single(ADD), single(SDD),\n"
+              "             int32(noViews), double(betas), int32(flatPanel), single(data))\n"
+              "  type: proj,dd | proj,tf  (image [nx ny] -> sinogram [nu noViews])\n"
+              "        back,dd | back,tf  (sinogram -> image)\n");
+}
+
 void mexFunction(int nlhs, mxArray *plhs[], int nrhs, const mxArray *prhs[])
 {
     char type[16];
-    if (!mxIsChar(prhs[0]) || mxGetString(prhs[0], type, sizeof(type)))
+    if (!nlhs && !nrhs) {  /* usage, as with the cone-beam gateway */
+        usage();
+        return;
+    }
+    if (nrhs < 1 || !mxIsChar(prhs[0]) || mxGetString(prhs[0], type, sizeof(type)))
         mexErrMsgTxt("The 1st argument is invalid! \n");
     if (nrhs != 14 || nlhs != 1) mexErrMsgTxt("Error: incorrect number of arguments. \n");
     if (!known_type(type)) mexErrMsgTxt("Error: unknown geom type. \n");

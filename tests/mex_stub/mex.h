@@ -1,6 +1,6 @@
 /* Minimal stand-in for MATLAB's mex.h (test infrastructure): declares just what the
- * MEX gateway in ctsim_b200/mex/ uses, so that the gateway can be compile-checked
- * on a machine without MATLAB. */
+ * MEX gateways in ctsim_b200/mex/ use, so that they can be compiled, and linked with
+ * mex_fake.c and called, on a machine without MATLAB. */
 #ifndef CTSIM_TEST_MEX_STUB_H
 #define CTSIM_TEST_MEX_STUB_H
 #include <stdbool.h>
