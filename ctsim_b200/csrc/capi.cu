@@ -543,7 +543,11 @@ extern "C" ctsim_status ctsim_plan_backproject(ctsim_plan *p, int method, const 
 extern "C" ctsim_status ctsim_plan_check(ctsim_plan *p) {
     if (!p) return fail(CTSIM_ERR_ARGUMENT, "null plan");
     int h = 0;
-    cudaError_t e = cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    // stream-ordered plans: read the flag on the plan's own stream (a legacy-stream copy
+    // would wait for every other request's work on the device)
+    cudaError_t e = p->stream_ordered ? cudaMemcpyAsync(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, p->stream)
+                                      : cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && p->stream_ordered) e = cudaStreamSynchronize(p->stream);
     if (e != cudaSuccess) return cuda_fail(e, "error flag read");
     if (h) return fail(CTSIM_ERR_UNSUPPORTED, "a footprint exceeded the kernel's row buffer");
     return CTSIM_OK;

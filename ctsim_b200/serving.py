@@ -17,7 +17,12 @@ its own geometry.  The server
   and requests that arrive meanwhile are admitted as soon as slots and memory
   free up.  From the second iteration on, an OS-PWLS iteration is one replay of
   a CUDA graph captured from the first;
-* records per-request latency (completion - arrival) for p50/p99.
+* records per-request latency (completion - arrival) for p50/p99;
+* isolates failures: a request whose set-up or work raises, or whose plan reports a
+  device-side error at retirement, ends as ``status == "failed"`` with the error text,
+  and its slot and budget return to the server, while the other requests go on;
+  ``cancel(rid)`` withdraws a request (pending: at once; active: after the units
+  already on its stream).
 
 OS-PWLS requests run a fixed number of iterations (the reference's stopping test
 on the RMS change needs a host read per iteration).
@@ -54,6 +59,8 @@ class ReconRequest:
     result: "object" = None
     t_admit: float = float("nan")
     t_done: float = float("nan")
+    status: str = "pending"        # "done", "failed" or "cancelled" when the server is through with it
+    error: Optional[str] = None    # why it failed
 
     @property
     def latency(self) -> float:
@@ -97,8 +104,6 @@ class _Active:
     def __init__(self, req: ReconRequest, stream, device, graphs: bool = True, autotune: bool = False,
                  batched: bool = False):
         import torch
-        from .fdk import FDK
-        from .projector import Plan
         self.req = req
         self.stream = stream
         self.device = device
@@ -108,6 +113,26 @@ class _Active:
         self.solver = None
         self._graph = {}
         dt = _dtype(req.storage)
+        self.plan = self.fdk = self.sino = None
+        try:
+            self._setup(req, stream, device, dt, autotune)
+        except BaseException:
+            self.release()  # what the set-up made so far (stream-ordered)
+            raise
+        # batched OS-PWLS: the server steps the request's sub-iterations together with the
+        # other active requests' on its batch stream, after this set-up on the slot stream
+        self.batched = batched and req.kind == "pwls"
+        if self.batched:
+            self.units = req.iterations * req.subsets
+            self.sub = 0
+            self.joined = False
+            self.ready = torch.cuda.Event()
+            self.ready.record(stream)
+
+    def _setup(self, req, stream, device, dt, autotune):
+        import torch
+        from .fdk import FDK
+        from .projector import Plan
         with torch.cuda.device(device), torch.cuda.stream(stream):
             self.plan = Plan(req.geom, device, stream=stream)
             self.fdk = FDK(req.geom, req.window, 1.0, device, plan=self.plan)
@@ -124,15 +149,6 @@ class _Active:
                 self.fdk.close()
                 self.fdk = None
                 self.units = req.iterations
-        # batched OS-PWLS: the server steps the request's sub-iterations together with the
-        # other active requests' on its batch stream, after this set-up on the slot stream
-        self.batched = batched and req.kind == "pwls"
-        if self.batched:
-            self.units = req.iterations * req.subsets
-            self.sub = 0
-            self.joined = False
-            self.ready = torch.cuda.Event()
-            self.ready.record(stream)
 
     def in_flight(self) -> int:
         while self.events and self.events[0].query():
@@ -212,6 +228,11 @@ class _Active:
     def complete(self) -> bool:
         return self.issued == self.units and self.in_flight() == 0
 
+    def check(self):
+        """Raise if a kernel of this request set the plan's error flag (reads it on the
+        request's stream, whose work is complete when this is called)."""
+        self.plan.check()
+
     def release(self):
         """Free the request's device state (stream-ordered, no synchronisation)."""
         import torch
@@ -219,9 +240,11 @@ class _Active:
             self._graph.clear()
             if self.fdk is not None:
                 self.fdk.close()
+                self.fdk = None
             self.solver = None
             self.sino = None
-            self.plan.close()
+            if self.plan is not None:
+                self.plan.close()
 
 
 def _to_device(a, device):
@@ -256,6 +279,8 @@ class ReconServer:
         self.used = 0
         self.peak_used = 0
         self.done = []
+        self.failed = []      # requests that failed or were cancelled, in the order they ended
+        self._cancel = set()  # rids to withdraw when their set-up finishes
         self.t0 = 0.0
         self._clock = clock or time.perf_counter
         if activate is None:
@@ -300,7 +325,12 @@ class ReconServer:
             self.used += need
             self.peak_used = max(self.peak_used, self.used)
             if self._pool is None:
-                self._start(self._activate(req, slot), slot)
+                try:
+                    a = self._activate(req, slot)
+                except Exception as exc:  # this request only: its slot and budget return
+                    self._end(req, slot, "failed", exc)
+                    continue
+                self._start(a, slot)
             else:
                 self.starting.append((self._pool.submit(self._activate_in_worker, req, slot), req, slot))
 
@@ -313,26 +343,81 @@ class ReconServer:
         self._slot_of[id(a)] = slot
         self.active.append(a)
 
+    def _end(self, req, slot, status, exc=None):
+        """A request the server is through with other than by success: its slot and its
+        share of the budget return."""
+        req.status = status
+        req.error = None if exc is None else f"{type(exc).__name__}: {exc}"
+        req.t_done = self.now()
+        req.result = None
+        self.used -= hbm_footprint(req)
+        self._free_slots.append(slot)
+        self._cancel.discard(req.rid)
+        self.failed.append(req)
+
     def _collect_started(self):
         keep = []
         for fut, req, slot in self.starting:
-            if fut.done():
-                self._start(fut.result(), slot)  # re-raises a set-up error here
-            else:
+            if not fut.done():
                 keep.append((fut, req, slot))
+                continue
+            try:
+                a = fut.result()
+            except Exception as exc:  # a set-up error ends this request only
+                self._end(req, slot, "failed", exc)
+                continue
+            if req.rid in self._cancel:
+                a.release()
+                self._end(req, slot, "cancelled")
+            else:
+                self._start(a, slot)
         self.starting = keep
+
+    def cancel(self, rid: int) -> bool:
+        """Withdraw request ``rid``: a pending one at once, one being set up when its set-up
+        finishes, an active one once the units already on its stream are done (no more
+        are issued).  False if the server does not hold it (unknown or finished)."""
+        for i, r in enumerate(self.pending):
+            if r.rid == rid:
+                del self.pending[i]  # by position: requests hold arrays, so no equality test
+                r.status, r.t_done = "cancelled", self.now()
+                self.failed.append(r)
+                return True
+        if any(req.rid == rid for _, req, _ in self.starting):
+            self._cancel.add(rid)
+            return True
+        for a in self.active:
+            if a.req.rid == rid:
+                a.cancelled = True
+                return True
+        return False
 
     def _retire(self):
         keep = []
         for a in self.active:
-            if a.complete():
-                a.req.t_done = self.now()
-                a.release()
-                self.used -= hbm_footprint(a.req)
-                self._free_slots.append(self._slot_of.pop(id(a)))
-                self.done.append(a.req)
-            else:
+            failed = getattr(a, "failed", None)
+            cancelled = getattr(a, "cancelled", False)
+            if failed is None and not (cancelled and a.in_flight() == 0) and not a.complete():
                 keep.append(a)
+                continue
+            slot = self._slot_of.pop(id(a))
+            if failed is None and not cancelled:
+                try:
+                    a.check()  # the plan's device-side error flag
+                except Exception as exc:
+                    failed = exc
+            try:
+                a.release()
+            except Exception as exc:
+                failed = failed or exc
+            if failed is not None or cancelled:
+                self._end(a.req, slot, "failed" if failed is not None else "cancelled", failed)
+            else:
+                a.req.t_done = self.now()
+                a.req.status = "done"
+                self.used -= hbm_footprint(a.req)
+                self._free_slots.append(slot)
+                self.done.append(a.req)
         self.active = keep
 
     def tick(self):
@@ -340,8 +425,13 @@ class ReconServer:
         if self.starting:
             self._collect_started()
         for a in self.active:
+            if getattr(a, "cancelled", False) or getattr(a, "failed", None) is not None:
+                continue
             if not getattr(a, "batched", False) and a.issued < a.units and a.in_flight() < self.depth:
-                a.issue(self.to_host)
+                try:
+                    a.issue(self.to_host)
+                except Exception as exc:  # retired (and released) as failed below
+                    a.failed = exc
         if self.batch_pwls:
             self._batched_tick()
         self._retire()
@@ -355,7 +445,8 @@ class ReconServer:
             self._tick_events.popleft()
         if len(self._tick_events) >= self.depth:
             return
-        pw = [a for a in self.active if getattr(a, "batched", False) and a.issued < a.units]
+        pw = [a for a in self.active if getattr(a, "batched", False) and a.issued < a.units and
+              not getattr(a, "cancelled", False) and getattr(a, "failed", None) is None]
         if not pw:
             return
         bs = self.batch_stream
@@ -364,9 +455,14 @@ class ReconServer:
                 if not a.joined:
                     bs.wait_event(a.ready)
                     a.joined = True
-            batched_subset_steps([a.batch_pair() for a in pw])
-            for a in pw:
-                a.batch_advance(self.to_host, bs)
+            try:
+                batched_subset_steps([a.batch_pair() for a in pw])
+                for a in pw:
+                    a.batch_advance(self.to_host, bs)
+            except Exception as exc:  # the requests of this batched step fail together
+                for a in pw:
+                    a.failed = exc
+                return
             ev = torch.cuda.Event()
             ev.record(bs)
             self._tick_events.append(ev)
@@ -377,8 +473,8 @@ class ReconServer:
             self._pool = None
 
     def run(self, requests, time_limit: Optional[float] = None, idle_sleep: float = 2e-4):
-        """Serve requests (by arrival time) until all are done; returns the finished ones
-        in completion order."""
+        """Serve requests (by arrival time) until each is done, failed or cancelled; returns
+        the ones that succeeded, in completion order (``failed`` holds the others)."""
         for r in sorted(requests, key=lambda r: r.arrival):
             self.submit(r)
         self.t0 = self._clock()

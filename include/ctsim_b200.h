@@ -252,8 +252,10 @@ ctsim_status ctsim_plan_backproject_ex(ctsim_plan *plan, int method, const void 
                                        void *d_image, int image_dtype, int view_begin, int view_stride,
                                        int view_count, float scale, void *stream);
 
-/* Synchronous: waits for the device and reports whether any kernel on this plan met a
- * footprint larger than its buffers (a device-side flag; never expected for a valid plan). */
+/* Synchronous: reports whether any kernel on this plan met a footprint larger than its
+ * buffers, or a staged forward projection whose copy wait ran out (a device-side flag;
+ * never expected for a valid plan).  Waits for the device, or for a stream-ordered plan
+ * (ctsim_plan_create_async) for the plan's own stream only. */
 ctsim_status ctsim_plan_check(ctsim_plan *plan);
 
 /* ---------------------------------------------------------------------------

@@ -40,6 +40,9 @@ class _FakeActive:
         self.released = True
         self.log.append(("release", self.req.rid, self.slot))
 
+    def check(self):
+        pass
+
 
 class _Clock:
     def __init__(self):
@@ -201,3 +204,125 @@ def test_served_footprint_bounds_device_memory():
         a.release()
         torch.cuda.synchronize()
         assert used <= hbm_footprint(r), (r.kind, used, hbm_footprint(r))
+
+
+# ---------------------------------------------------------------------------
+# Failure isolation (host-side injection only: no GPU fault is made)
+# ---------------------------------------------------------------------------
+class _FailingIssue(_FakeActive):
+    def issue(self, to_host=False):
+        if self.issued == 1:
+            raise RuntimeError("injected failure of the second unit")
+        super().issue(to_host)
+
+
+def _serve_with_faults(admit_workers):
+    reqs = _requests()
+    log = []
+
+    def activate(r, s):
+        if r.rid == 2:
+            raise MemoryError("injected set-up failure")
+        if r.rid == 6:
+            return _FailingIssue(r, s, log)  # a PWLS request (3 units) that fails at its second
+        return _FakeActive(r, s, log)
+
+    srv = ReconServer(hbm_budget=1 << 40, max_active=3, activate=activate, clock=_Clock(),
+                      admit_workers=admit_workers)
+    for r in sorted(reqs, key=lambda r: r.arrival):
+        srv.submit(r)
+    srv.t0 = srv._clock()
+    cancelled = set()
+    ticks = 0
+    while srv.pending or srv.active or srv.starting:
+        srv.tick()
+        ticks += 1
+        if ticks == 3:  # one request still pending, one active mid-run
+            assert srv.cancel(13) and srv.pending[-1].rid != 13
+            act = [a.req.rid for a in srv.active if a.issued > 0 and a.req.kind == "pwls" and a.req.rid != 6]
+            if act:
+                assert srv.cancel(act[0])
+                cancelled.add(act[0])
+            cancelled.add(13)
+        assert srv.used >= 0 and len(srv._free_slots) + len(srv.active) + len(srv.starting) == 3
+    srv.close()
+    return reqs, srv, cancelled, log
+
+
+@pytest.mark.parametrize("admit_workers", [0, 2])
+def test_failures_and_cancellations_stay_with_their_requests(admit_workers):
+    reqs, srv, cancelled, log = _serve_with_faults(admit_workers)
+    assert len(cancelled) == 2  # one pending, one active mid-run
+    by = {r.rid: r for r in reqs}
+    assert by[2].status == "failed" and "MemoryError" in by[2].error and by[2].result is None
+    assert by[6].status == "failed" and "second unit" in by[6].error
+    for rid in cancelled:
+        assert by[rid].status == "cancelled"
+    assert srv.cancel(13) is False  # no longer held
+    others = [r for r in reqs if r.rid not in cancelled | {2, 6}]
+    assert all(r.status == "done" for r in others)
+    assert sorted(r.rid for r in srv.done) == sorted(r.rid for r in others)
+    assert sorted(r.rid for r in srv.failed) == sorted(cancelled | {2, 6})
+    # every slot and byte of budget came back; no work was issued for a withdrawn request after it ended
+    assert srv.used == 0 and len(srv._free_slots) == 3
+    assert all(e[1] not in (2, 13) for e in log if e[0] == "issue")
+    # the released device state of a request that failed mid-run
+    assert ("release", 6) in {(e[0], e[1]) for e in log}
+
+
+def test_a_request_whose_plan_reports_an_error_fails_at_retirement():
+    log = []
+
+    class _Flagged(_FakeActive):
+        def check(self):
+            raise RuntimeError("a footprint exceeded the kernel's row buffer")
+
+    srv = ReconServer(hbm_budget=1 << 40, max_active=2, clock=_Clock(),
+                      activate=lambda r, s: (_Flagged if r.rid == 1 else _FakeActive)(r, s, log))
+    reqs = _requests()[:4]
+    done = srv.run(reqs)
+    assert sorted(r.rid for r in done) == [0, 2, 3]
+    assert reqs[1].status == "failed" and "row buffer" in reqs[1].error and srv.used == 0
+
+
+@pytest.mark.gpu
+def test_served_failure_and_cancellation_leave_other_results_unchanged():
+    """On the device: one request's set-up raises (injected on the host, before any device
+    work of its own), another is cancelled after its first unit; the rest finish with
+    images bit-identical to their solo runs, and the budget is whole again."""
+    reqs = _device_requests()
+    solo = []
+    for r in reqs:
+        alone = copy.deepcopy(r)
+        ReconServer(max_active=1).run([alone])
+        solo.append(_result(alone))
+    mixed = copy.deepcopy(reqs)
+    fail_rid = mixed[1].rid
+    cancel_rid = mixed[3].rid  # an OS-PWLS request (3 iterations)
+    srv = ReconServer(max_active=3, admit_workers=2, to_host=True)
+    default = srv._activate
+
+    def activate(r, slot):
+        if r.rid == fail_rid:
+            raise MemoryError("injected set-up failure")
+        return default(r, slot)
+
+    srv._activate = activate
+    for r in mixed:
+        srv.submit(r)
+    srv.t0 = srv._clock()
+    cancelled = False
+    while srv.pending or srv.active or srv.starting:
+        srv.tick()
+        if not cancelled and any(a.req.rid == cancel_rid and a.issued >= 1 for a in srv.active):
+            cancelled = srv.cancel(cancel_rid)
+    srv.close()
+    assert cancelled
+    by = {r.rid: r for r in mixed}
+    assert by[fail_rid].status == "failed" and "MemoryError" in by[fail_rid].error
+    assert by[cancel_rid].status == "cancelled" and by[cancel_rid].result is None
+    assert srv.used == 0
+    for i, r in enumerate(mixed):
+        if r.rid in (fail_rid, cancel_rid):
+            continue
+        assert r.status == "done" and np.array_equal(_result(r), solo[i]), (i, r.kind)
