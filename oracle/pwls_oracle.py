@@ -124,6 +124,8 @@ def recon_pwls_se_sqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0, fp64=F
         rmsd = float(np.sqrt(np.mean((x.astype(np.float64) - xold) ** 2)))
         phis.append(phi)
         rmsds.append(rmsd)
+        if history is not None:
+            history.append(x.copy())
         if itn > 5 and rmsd < 1e-5:
             break
     return x, np.array(phis), np.array(rmsds)
@@ -195,9 +197,10 @@ def _matlab_round(v):
     return int(np.floor(abs(v) + 0.5)) * (1 if v >= 0 else -1)
 
 
-def recon_pwls_nesterov_sqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0, img_opt=None):
+def recon_pwls_nesterov_sqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0, img_opt=None, history=None):
     """reconPwlsSeNesterovSqs.m in single precision (MATLAB: a double scalar times a single
-    array is computed in single); returns (x, phis, rmsds)."""
+    array is computed in single); returns (x, phis, rmsds).  ``history``, if a list,
+    receives a copy of x after every outer iteration."""
     if pfun == "huber":
         R = lambda x: huber_penalty(x, 0, delta)
         S = lambda x: huber_penalty(x, 1, delta)
@@ -252,6 +255,8 @@ def recon_pwls_nesterov_sqs(y, w, geom, beta, pfun, itnlim, delta, numos, img0, 
             rmsd = float(np.sqrt(np.mean((x[k].astype(np.float64) - np.asarray(img_opt, np.float64)[k]) ** 2)))
         phis.append(phi)
         rmsds.append(rmsd)
+        if history is not None:
+            history.append(x.copy())
         if itn > 5 and rmsd < stop_crt:
             break
         if itn % nrestart == 0:

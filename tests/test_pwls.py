@@ -122,3 +122,54 @@ def test_device_nesterov_rmsd_against_converged_image():
     xo, _, rmsdo = pwls_oracle.recon_pwls_nesterov_sqs(y, w, g, 2.0, "huber", 4, 0.01, 3, x0, img_opt=x_opt)
     assert np.allclose(rmsds, rmsdo, rtol=1e-3)
     assert rmsds[-1] < rmsds[0]  # approaching the converged image
+
+
+def config1_pwls_case(views=60):
+    """Config-1 shapes (128^2 x 64 at 1 mm, flat 256 x 96 detector at 1.6 mm, SAD 1000, SDD
+    1500) with ``views`` views over the turn: the seeded 12-ellipsoid phantom, Poisson counts
+    at I0 = 1e5 (counts clamped at 10 in the log) and w = counts; a uniform start image."""
+    from ctsim_b200.phantom import config1, to_projector_units
+    from oracle.bindings import oracle_cbct
+    g, x_mm = config1(n_views=views, seed=1)
+    p = oracle_cbct("proj,tf", g, to_projector_units(x_mm))
+    rng = np.random.default_rng(21)
+    counts = rng.poisson(1e5 * np.exp(-p.astype(np.float64))).astype(np.float32)
+    y = np.log(1e5 / np.maximum(counts, 10)).astype(np.float32)
+    w = pwls_oracle.compute_weights_pwls(counts)
+    x0 = np.full(g.image_shape, 0.15, np.float32)
+    return g, y, w, x0
+
+
+# relative L2 of the image after each outer iteration, device against the restatement: the
+# FP32 projectors of the two sides differ in summation order (about 1e-6 per projection),
+# and each SQS step divides two such sums
+PER_ITERATION_REL_L2 = 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pfun", ["huber", "quad"])
+@pytest.mark.parametrize("nesterov", [False, True], ids=["sqs", "nesterov"])
+def test_config1_os_pwls_each_iteration_matches_oracle(pfun, nesterov):
+    """reconPwlsSeSqs / reconPwlsSeNesterovSqs at config-1 shapes, 60 views, 4 ordered
+    subsets, 2 outer iterations (statsrecon/pwls/reconPwlsSeSqs.m:51-78,
+    reconPwlsSeNesterovSqs.m:60-113): the image after every iteration, phi and rmsd."""
+    import torch
+    from ctsim_b200.pwls import PwlsNesterovSolver, PwlsSolver
+    g, y, w, x0 = config1_pwls_case()
+    beta, delta, M, its = 1e3, 0.01, 4, 2
+    cls = PwlsNesterovSolver if nesterov else PwlsSolver
+    s = cls(torch.from_numpy(y).cuda(), torch.from_numpy(w).cuda(), g, beta, pfun, delta, M,
+            torch.from_numpy(x0).cuda())
+    got, phis, rmsds = [], [], []
+    for _ in range(its):
+        phi, rmsd = s.step()
+        got.append(s.x.cpu().numpy())
+        phis.append(phi)
+        rmsds.append(rmsd)
+    hist = []
+    run = pwls_oracle.recon_pwls_nesterov_sqs if nesterov else pwls_oracle.recon_pwls_se_sqs
+    _, phio, rmsdo = run(y, w, g, beta, pfun, its, delta, M, x0, history=hist)
+    errs = [float(np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(b)) for a, b in zip(got, hist)]
+    assert max(errs) <= PER_ITERATION_REL_L2, errs
+    assert np.allclose(phis, phio, rtol=1e-5), (phis, phio)
+    assert np.allclose(rmsds, rmsdo, rtol=1e-3), (rmsds, rmsdo)
