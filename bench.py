@@ -683,6 +683,46 @@ def run_reference_gpu(args):
             fdk["vs_reference_cpu_2_views"] = {"ours_bit_identical": bool(np.array_equal(ours_pd2, cpu_pd)),
                                                "ours": rel(ours_pd2, cpu_pd),
                                                "reference_gpu": rel(refgpu_cbct("back,hpd", g2, y2), cpu_pd)}
+    # SF pair: the reference's cbct_proj_tf_gpu / cbct_back_tf_gpu against the drop-in
+    # ctsim_proj_tf / ctsim_back_tf (host pointers, synchronous)
+    sf = None
+    from oracle.bindings import REFGPU_SF_SO
+    if os.path.exists(REFGPU_SF_SO):
+        refgpu_cbct("proj,tf", warm, x)
+        refgpu_cbct("back,tf", warm, y[:2])
+        s0 = time.perf_counter()
+        ref_sa = refgpu_cbct("proj,tf", g, x)
+        s1 = time.perf_counter()
+        ref_sat = refgpu_cbct("back,tf", g, y)
+        s2 = time.perf_counter()
+        ours_sa = np.empty(g.sino_shape, np.float32)
+        ours_sat = np.empty(g.image_shape, np.float32)
+
+        def ours_sf():
+            ok = L.ctsim_proj_tf(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel, x.ctypes.data,
+                                 ours_sa.ctypes.data, mp.ctypes.data)
+            ok = ok and L.ctsim_back_tf(*sc, betas.ctypes.data, couch.ctypes.data, g.flatPanel,
+                                        ours_sat.ctypes.data, y.ctypes.data, mp.ctypes.data)
+            if not ok:
+                raise RuntimeError(_lib.last_error())
+
+        ours_sf()
+        s3 = time.perf_counter()
+        ours_sf()
+        s4 = time.perf_counter()
+        sf = {"reference_gpu_ms": {"A": (s1 - s0) * 1e3, "A^T": (s2 - s1) * 1e3},
+              "ours_host_pointer_ms": (s4 - s3) * 1e3, "speedup": (s2 - s0) / (s4 - s3),
+              "rel_l2_reference_gpu_vs_ours": {"A": rel(ref_sa, ours_sa), "A^T": rel(ref_sat, ours_sat)}}
+        if ref_available():
+            cpu_sa = ref_cbct("proj,tf", g2, x, nthreads=2)
+            cpu_sat = ref_cbct("back,tf", g2, y2, nthreads=2)
+            ours_sat2 = np.empty(g2.image_shape, np.float32)
+            if not L.ctsim_back_tf(*g2.scalars(), b2.ctypes.data, c2.ctypes.data, g2.flatPanel,
+                                   ours_sat2.ctypes.data, y2.ctypes.data, mp.ctypes.data):
+                raise RuntimeError(_lib.last_error())
+            sf["vs_reference_cpu_2_views"] = {
+                "A": {"ours": rel(ours_sa[:2], cpu_sa), "reference_gpu": rel(ref_sa[:2], cpu_sa)},
+                "A^T": {"ours": rel(ours_sat2, cpu_sat), "reference_gpu": rel(refgpu_cbct("back,tf", g2, y2), cpu_sat)}}
     vv = float(g.nx * g.ny * g.nz * g.noViews)
     line = {"metric": METRIC, "impl": "reference-gpu", "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
             "value": 2 * vv / (t2 - t0) / 1e9, "dtype": "f32", "data": "synthetic",
@@ -693,7 +733,7 @@ def run_reference_gpu(args):
             "ours_host_pointer_value": 2 * vv / (t4 - t3) / 1e9,
             "speedup": (t2 - t0) / (t4 - t3),
             "rel_l2_reference_gpu_vs_ours": {"A": rel(ref_a, ours_a), "A^T": rel(ref_at, ours_at)},
-            "rel_l2_vs_reference_cpu": cpu_check, "fdk_back_hpd": fdk}
+            "rel_l2_vs_reference_cpu": cpu_check, "fdk_back_hpd": fdk, "sf_pair": sf}
     print(json.dumps(line), flush=True)
 
 

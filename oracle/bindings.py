@@ -5,8 +5,9 @@
                       (single-threaded, or over view chunks with ``nthreads``)
 * ``ref3_cbct``    -> the reference's arc-detector DD pair (geom/cbct/cbct_proj3.c,
                       cbct_back3.c), ``_ref/libcbct_ref3.so``
-* ``refgpu_cbct``  -> the reference's CUDA DD pair (geom/dd_cuda), ``_ref/librefgpu_dd.so``:
-                      a timing baseline on the GPU, not a parity target
+* ``refgpu_cbct``  -> the reference's CUDA DD pair (geom/dd_cuda), SF pair (geom/sf_cuda) and
+                      FDK backprojection (geom/fdk_cuda), ``_ref/librefgpu_{dd,sf,pd}.so``:
+                      timing baselines on the GPU, not parity targets
 
 Both take and return numpy arrays in the package conventions
 (image ``[nz, ny, nx]``, sino ``[noViews, nu, nv]``, float32).
@@ -26,6 +27,7 @@ REF_SO = os.path.join(HERE, "_ref", "libcbct_ref.so")
 REF3_SO = os.path.join(HERE, "_ref", "libcbct_ref3.so")
 REFGPU_SO = os.path.join(HERE, "_ref", "librefgpu_dd.so")
 REFGPU_PD_SO = os.path.join(HERE, "_ref", "librefgpu_pd.so")
+REFGPU_SF_SO = os.path.join(HERE, "_ref", "librefgpu_sf.so")
 
 KINDS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3,
          "back,pd": 4, "back,hpd": 5, "back,var": 6}
@@ -67,6 +69,10 @@ def _load(path):
         elif path == REFGPU_PD_SO:
             lib.refgpu_back_pd.argtypes = _GEOM_ARGS + [C.c_bool]
             lib.refgpu_back_pd.restype = C.c_bool
+        elif path == REFGPU_SF_SO:
+            for fn in (lib.refgpu_proj_tf, lib.refgpu_back_tf):
+                fn.argtypes = _GEOM_ARGS
+                fn.restype = C.c_bool
         else:
             lib.ref_cbct_call.argtypes = [_i] + _GEOM_ARGS
             lib.ref_cbct_call.restype = _i
@@ -182,19 +188,24 @@ def refgpu_available() -> bool:
 
 def refgpu_cbct(kind: str, geom, data) -> np.ndarray:
     """The reference's own GPU drivers cbct_proj_dd_gpu / cbct_back_dd_gpu
-    (geom/dd_cuda/cbct_dd_proj.c:407, cbct_dd_back.c:299) and cbct_back_pd_gpu
-    (geom/fdk_cuda/cbct_back_pd.c:230) on the current CUDA device: host arrays in and
-    out, synchronous."""
-    if kind not in ("proj,dd", "back,dd", "back,pd", "back,hpd"):
-        raise ValueError("the reference GPU builds cover proj,dd, back,dd, back,pd and back,hpd")
+    (geom/dd_cuda/cbct_dd_proj.c:407, cbct_dd_back.c:299), cbct_proj_tf_gpu /
+    cbct_back_tf_gpu (geom/sf_cuda/cbct_sf_proj.c:443, cbct_sf_back.c:334) and
+    cbct_back_pd_gpu (geom/fdk_cuda/cbct_back_pd.c:230) on the current CUDA device:
+    host arrays in and out, synchronous."""
+    if kind not in ("proj,dd", "back,dd", "proj,tf", "back,tf", "back,pd", "back,hpd"):
+        raise ValueError("the reference GPU builds cover proj,dd, back,dd, proj,tf, back,tf, back,pd and back,hpd")
     data, out, args, keep = _prep(kind, geom, data)
     a = list(args)
-    if kind != "proj,dd":  # the back drivers take (image, proj): the output image first
+    if not kind.startswith("proj"):  # the back drivers take (image, proj): the output image first
         a[-3], a[-2] = a[-2], a[-3]
     if kind == "proj,dd":
         ok = _load(REFGPU_SO).refgpu_proj_dd(*a)
     elif kind == "back,dd":
         ok = _load(REFGPU_SO).refgpu_back_dd(*a)
+    elif kind == "proj,tf":
+        ok = _load(REFGPU_SF_SO).refgpu_proj_tf(*a)
+    elif kind == "back,tf":
+        ok = _load(REFGPU_SF_SO).refgpu_back_tf(*a)
     else:
         ok = _load(REFGPU_PD_SO).refgpu_back_pd(*a, kind == "back,pd")
     if not ok:
