@@ -19,13 +19,14 @@ STATUS = {0: "OK", 1: "ERR_ARGUMENT", 2: "ERR_CUDA", 3: "ERR_ALLOC", 4: "ERR_UNS
 METHODS = {"proj,dd": 0, "proj,tf": 1, "back,dd": 2, "back,tf": 3, "back,pd": 4, "back,hpd": 5}
 
 # symbols declared in include/ctsim_b200.h
+INPUT_SCALED = 0x100  # CTSIM_INPUT_SCALED
 EXPORTED = ["ctsim_last_error", "ctsim_version", "ctsim_proj_dd", "ctsim_back_dd", "ctsim_proj_tf", "ctsim_back_tf",
             "ctsim_back_pd", "ctsim_cbct_geom", "ctsim_plan_create", "ctsim_plan_destroy", "ctsim_plan_device_bytes",
             "ctsim_plan_project", "ctsim_plan_backproject", "ctsim_plan_check", "ctsim_back_dd_noalloc",
             "ctsim_fdk_create", "ctsim_fdk_destroy", "ctsim_fdk_filter", "ctsim_fdk_run", "ctsim_fdk_dbeta",
             "ctsim_fdk_design_filter", "ctsim_pwls_weights", "ctsim_pwls_residual", "ctsim_sqdiff",
             "ctsim_penalty", "ctsim_sqs_update", "ctsim_plan_project_ex", "ctsim_plan_backproject_ex",
-            "ctsim_pwls_residual_ex", "ctsim_fdk_filter_ex", "ctsim_fdk_run_ex",
+            "ctsim_pwls_residual_ex", "ctsim_pwls_residual_scaled", "ctsim_fdk_filter_ex", "ctsim_fdk_run_ex",
             "ctsim_plan_create_async", "ctsim_pool_trim", "ctsim_nesterov_update",
             "ctsim_simulate_counts", "ctsim_log_attenuation", "ctsim_fbct_geom", "ctsim_fan_plan_create",
             "ctsim_fan_plan_destroy", "ctsim_fan_project", "ctsim_fan_backproject",
@@ -173,6 +174,8 @@ def load():
     L.ctsim_pwls_residual.restype = _i
     L.ctsim_pwls_residual_ex.argtypes = [_p, _p, _p, _i, _f, _p, _sz, _p, _p]
     L.ctsim_pwls_residual_ex.restype = _i
+    L.ctsim_pwls_residual_scaled.argtypes = [_p, _p, _p, _p, _i, _f, _p, _i, _p, _p]
+    L.ctsim_pwls_residual_scaled.restype = _i
     L.ctsim_sqdiff.argtypes = [_p, _p, _sz, _p, _p]
     L.ctsim_sqdiff.restype = _i
     L.ctsim_penalty.argtypes = [_i, _i, _f, _i, _i, _i, _p, _p, _p, _p]

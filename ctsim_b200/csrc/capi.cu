@@ -86,6 +86,7 @@ struct ctsim_plan {
 // Plan internals for other translation units (fdk.cu).
 const double *ctsim_plan_betas(const ctsim_plan *p) { return p->betas.data(); }
 const ctsim_geom *ctsim_plan_geom(const ctsim_plan *p) { return &p->geom; }
+const float *ctsim_plan_ampv(const ctsim_plan *p) { return p->d_ampv; }
 
 extern "C" const char *ctsim_last_error(void) { return g_last_error.c_str(); }
 
@@ -369,7 +370,9 @@ static ctsim_status create_plan(const ctsim_geom *geom, const double *betas, con
                         200 * 1024;
     if (p->fwd_ok)
         CTSIM_ALLOC(p->d_xs, sizeof(float) * (size_t)nxy * (p->xs_holds_pairs ? 2 * (G.nz + 1) : g.xstride));
-    CTSIM_ALLOC(p->d_ps, sizeof(float) * (size_t)G.nu * G.nv * G.noviews);
+    // the backprojection scratch (an FP32 copy of the sinogram times ampv) is allocated on
+    // first use (ensure_scratch): BF16/FP16 sinograms and CTSIM_INPUT_SCALED residuals are
+    // read as they are and never need it
 #undef CTSIM_ALLOC
     p->bytes = bytes;
     if ((e = ctsim_plan_upload(p, p->d_views, views.data(), sizeof(View) * G.noviews)) != cudaSuccess ||
@@ -413,6 +416,31 @@ extern "C" ctsim_status ctsim_plan_project_ex(ctsim_plan *p, int method, const v
                         stream, true);
 }
 
+// The backprojection scratch d_ps ([noviews][nu][nv] FP32), allocated with the plan's own
+// allocation mode at the first call that needs it: a DD/SF A^T of an unscaled FP32 sinogram
+// (the sinogram times ampv goes there first).  Not during stream capture: a plan that
+// will be captured makes one such call before.
+static ctsim_status ensure_scratch(ctsim_plan *p, cudaStream_t st) {
+    if (p->d_ps) return CTSIM_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (st && cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+        return fail(CTSIM_ERR_ARGUMENT,
+                    "the plan's first unscaled FP32 backprojection allocates its scratch: make one before stream "
+                    "capture (or pass BF16/FP16 or CTSIM_INPUT_SCALED data)");
+    const size_t n = sizeof(float) * (size_t)p->geom.nu * p->geom.nv * p->geom.noviews;
+    void *ptr = nullptr;
+    cudaError_t e = ctsim_plan_alloc(p, &ptr, n);
+    if (e != cudaSuccess) return fail(CTSIM_ERR_ALLOC, std::string("backprojection scratch: ") + cudaGetErrorString(e));
+    // a stream-ordered allocation is usable on the plan's stream; order `st` after it
+    if (p->stream_ordered && st != p->stream && (e = cudaStreamSynchronize(p->stream)) != cudaSuccess) {
+        ctsim_plan_release(p, ptr);
+        return cuda_fail(e, "backprojection scratch");
+    }
+    p->d_ps = static_cast<float *>(ptr);
+    p->bytes += n;
+    return CTSIM_OK;
+}
+
 // prefix = false reuses the column prefix sums of the previous call on the same image
 // (the host-pointer path projects one image in view chunks).
 static ctsim_status plan_project(ctsim_plan *p, int method, const void *d_image, int image_dtype, void *d_proj,
@@ -453,6 +481,10 @@ extern "C" ctsim_status ctsim_plan_backproject_ex(ctsim_plan *p, int method, con
                                                   int view_count, float scale, void *stream) {
     if (!p || !d_image || !d_proj) return fail(CTSIM_ERR_ARGUMENT, "null argument");
     if (!dtype_ok(image_dtype) || !dtype_ok(proj_dtype)) return fail(CTSIM_ERR_ARGUMENT, "unknown storage type");
+    const bool scaled_in = (method & CTSIM_INPUT_SCALED) != 0;
+    method &= ~CTSIM_INPUT_SCALED;
+    if (scaled_in && ((method != CTSIM_BACK_DD && method != CTSIM_BACK_TF) || proj_dtype != CTSIM_F32))
+        return fail(CTSIM_ERR_ARGUMENT, "CTSIM_INPUT_SCALED takes an FP32 sinogram for back,dd / back,tf");
     if (p->g.det == 2 && method != CTSIM_BACK_DD) return fail(CTSIM_ERR_UNSUPPORTED, kArcOnlyDD);
     ctsim_status s = check_views(p, view_begin, view_stride, view_count);
     if (s != CTSIM_OK) return s;
@@ -463,26 +495,29 @@ extern "C" ctsim_status ctsim_plan_backproject_ex(ctsim_plan *p, int method, con
     case CTSIM_BACK_DD:
     case CTSIM_BACK_TF: {
         if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
-        e = launch_prescale(d_proj, proj_dtype, p->d_ampv, p->d_ps, nuv, nuv * view_count, st);
-        if (e != cudaSuccess) return cuda_fail(e, "prescale kernel");
+        // BF16/FP16 sinograms and scaled FP32 residuals are read as they are; an unscaled
+        // FP32 sinogram is multiplied by ampv into the scratch first
+        const void *src = d_proj;
+        int kind = proj_dtype == CTSIM_BF16 ? kSrcBF16 : proj_dtype == CTSIM_F16 ? kSrcF16 : kSrcScaled;
+        if (proj_dtype == CTSIM_F32 && !scaled_in) {
+            if ((s = ensure_scratch(p, st)) != CTSIM_OK) return s;
+            e = launch_prescale(d_proj, proj_dtype, p->d_ampv, p->d_ps, nuv, nuv * view_count, st);
+            if (e != cudaSuccess) return cuda_fail(e, "prescale kernel");
+            src = p->d_ps;
+        }
         const bool dd = method == CTSIM_BACK_DD;
-        e = launch_back(dd ? kDD : kTF, dd ? p->back_mz : p->back_mz_tf, p->g, p->d_views, p->d_ps, p->d_map,
-                        d_image, image_dtype, view_begin, view_stride, view_count, scale,
-                        dd ? p->back_qcap : p->back_qcap_tf, p->d_err, st);
+        e = launch_back(dd ? kDD : kTF, dd ? p->back_mz : p->back_mz_tf, p->g, p->d_views, src, p->d_map, d_image,
+                        image_dtype, view_begin, view_stride, view_count, scale, dd ? p->back_qcap : p->back_qcap_tf,
+                        p->d_err, st, false, 0, -1, kind, p->d_ampv);
         break;
     }
     case CTSIM_BACK_PD:
     case CTSIM_BACK_HPD:
     case CTSIM_BACK_VAR: {
-        const float *src = static_cast<const float *>(d_proj);
-        if (proj_dtype != CTSIM_F32) {  // FP32 copy of the views in scratch
-            e = launch_prescale(d_proj, proj_dtype, nullptr, p->d_ps, nuv, nuv * view_count, st);
-            if (e != cudaSuccess) return cuda_fail(e, "conversion kernel");
-            src = p->d_ps;
-        }
+        // the sinogram is read in its storage type (no FP32 copy)
         const int mode = method == CTSIM_BACK_PD ? kPdOff : method == CTSIM_BACK_HPD ? kPdClamp : kPdVar;
-        e = launch_pd(mode, p->pd_mz, p->g, p->d_views, src, p->d_map, d_image, image_dtype, view_begin, view_stride,
-                      view_count, scale, st);
+        e = launch_pd(mode, p->pd_mz, p->g, p->d_views, d_proj, p->d_map, d_image, image_dtype, view_begin,
+                      view_stride, view_count, scale, st, false, proj_dtype);
         break;
     }
     default:
@@ -519,6 +554,7 @@ static ctsim_status plan_back_views(ctsim_plan *p, int method, const float *d_pr
         return e == cudaSuccess ? CTSIM_OK : cuda_fail(e, "backprojection kernel");
     }
     if (!p->fwd_ok) return fail(CTSIM_ERR_UNSUPPORTED, p->fwd_reason);
+    if ((s = ensure_scratch(p, st)) != CTSIM_OK) return s;
     const size_t nuv = (size_t)p->g.nu * p->g.nv;
     cudaError_t e;
     if (prescale && (e = launch_prescale(d_proj, CTSIM_F32, p->d_ampv, p->d_ps, nuv, nuv * vc, st)) != cudaSuccess)
@@ -1161,17 +1197,31 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
 }
 
 extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_item *items, int n, void *stream) {
+    const bool scaled_in = (method & CTSIM_INPUT_SCALED) != 0;
+    method &= ~CTSIM_INPUT_SCALED;
     ctsim_status s = batch_check(method, items, n, false);
     if (s != CTSIM_OK || n == 0) return s;
     cudaStream_t st = (cudaStream_t)stream;
     const bool dd = method == CTSIM_BACK_DD;
     cudaError_t e;
-    for (int i = 0; i < n; i++) {  // sinograms times ampv into each plan's scratch
-        const ctsim_plan *p = items[i].plan;
-        const size_t nuv = (size_t)p->g.nu * p->g.nv;
-        if ((e = launch_prescale(items[i].in, items[i].in_dtype, p->d_ampv, p->d_ps, nuv, nuv * items[i].view_count,
-                                 st)) != cudaSuccess)
-            return cuda_fail(e, "prescale kernel");
+    // each item's source: BF16/FP16 and scaled FP32 sinograms as they are, unscaled FP32
+    // ones times ampv into the plan's scratch
+    std::vector<const void *> src(n);
+    std::vector<int> kind(n);
+    for (int i = 0; i < n; i++) {
+        ctsim_plan *p = items[i].plan;
+        const int dt = items[i].in_dtype;
+        if (scaled_in && dt != CTSIM_F32) return fail(CTSIM_ERR_ARGUMENT, "CTSIM_INPUT_SCALED takes FP32 sinograms");
+        src[i] = items[i].in;
+        kind[i] = dt == CTSIM_BF16 ? kSrcBF16 : dt == CTSIM_F16 ? kSrcF16 : kSrcScaled;
+        if (dt == CTSIM_F32 && !scaled_in) {
+            if ((s = ensure_scratch(p, st)) != CTSIM_OK) return s;
+            const size_t nuv = (size_t)p->g.nu * p->g.nv;
+            if ((e = launch_prescale(items[i].in, dt, p->d_ampv, p->d_ps, nuv, nuv * items[i].view_count, st)) !=
+                cudaSuccess)
+                return cuda_fail(e, "prescale kernel");
+            src[i] = p->d_ps;
+        }
     }
     // An item of at least four waves of the single-plan kernel gains nothing from sharing a
     // launch and runs on that kernel (64 registers, four blocks per SM, against up to 128
@@ -1180,19 +1230,22 @@ extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_it
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, items[0].plan->device);
     const int large = 4 * 4 * sms;
-    std::map<std::vector<int>, std::vector<int>> classes;  // (z blocks per lane, float4 rows, FP32 out)
+    // classes: (z blocks per lane, float4 rows, FP32 out, source form)
+    std::map<std::vector<int>, std::vector<int>> classes;
     for (int i = 0; i < n; i++) {
         const ctsim_batch_item &it = items[i];
         const ctsim_plan *p = it.plan;
         if (back_task_blocks(p->g) >= large) {
-            if ((e = launch_back(dd ? kDD : kTF, dd ? p->back_mz : p->back_mz_tf, p->g, p->d_views, p->d_ps, p->d_map,
+            if ((e = launch_back(dd ? kDD : kTF, dd ? p->back_mz : p->back_mz_tf, p->g, p->d_views, src[i], p->d_map,
                                  it.out, it.out_dtype, it.view_begin, it.view_stride, it.view_count, it.scale,
-                                 dd ? p->back_qcap : p->back_qcap_tf, p->d_err, st)) != cudaSuccess)
+                                 dd ? p->back_qcap : p->back_qcap_tf, p->d_err, st, false, 0, -1, kind[i],
+                                 p->d_ampv)) != cudaSuccess)
                 return cuda_fail(e, "backprojection kernel");
             continue;
         }
-        const bool vec = (p->g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(p->d_ps) % 16) == 0;
-        classes[{dd ? p->back_mz : p->back_mz_tf, vec ? 1 : 0, it.out_dtype == CTSIM_F32 ? 0 : 1}].push_back(i);
+        const size_t align = kind[i] == kSrcScaled ? 16 : 8;
+        const bool vec = (p->g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(src[i]) % align) == 0;
+        classes[{dd ? p->back_mz : p->back_mz_tf, vec ? 1 : 0, it.out_dtype == CTSIM_F32 ? 0 : 1, kind[i]}].push_back(i);
     }
     for (auto &cl : classes) {
         const std::vector<int> &idx = cl.second;
@@ -1207,7 +1260,8 @@ extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_it
                 BackTask &T = b.t[b.n++];
                 T.g = p->g;
                 T.views = p->d_views;
-                T.ps = p->d_ps;
+                T.ps = src[idx[c]];
+                T.ampv = p->d_ampv;
                 T.map = p->d_map;
                 T.image = it.out;
                 T.out_dtype = it.out_dtype;
@@ -1222,7 +1276,7 @@ extern "C" ctsim_status ctsim_batch_backproject(int method, const ctsim_batch_it
                 qcap = std::max(qcap, T.qcap);
             }
             if ((e = launch_back_batch(dd ? kDD : kTF, cl.first[0], cl.first[1] != 0, cl.first[2] != 0,
-                                       back_smem_bytes(qcap), b, st)) != cudaSuccess)
+                                       back_smem_bytes(qcap), b, st, cl.first[3])) != cudaSuccess)
                 return cuda_fail(e, "batched backprojection");
         }
     }

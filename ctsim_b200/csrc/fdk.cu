@@ -127,7 +127,7 @@ double parker_s(double b) {
 // frequency from natural order, read back bit-reversed.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) fdk_filter_kernel(const void *__restrict__ sino, int in_dtype,
-                                                         float *__restrict__ out,
+                                                         void *__restrict__ out, int out_dtype,
                                                          const float *__restrict__ wcos,
                                                          const float *__restrict__ parker,
                                                          const float *__restrict__ H, const float2 *__restrict__ tw,
@@ -137,7 +137,6 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(const void *__restrict_
     const int iv0 = blockIdx.x * kFiltRows;
     const size_t nuv = (size_t)nu * nv;
     const size_t vbase = (size_t)k * nuv;
-    float *ov = out + (size_t)k * nuv;
     const int t = threadIdx.x;
     const int sh = 32 - log2L;
     // load, weight, scatter to bit-reversed positions (zero padding beyond nu)
@@ -200,7 +199,7 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(const void *__restrict_
         if (iv0 + r >= nv) continue;
         const int pos = __brev(iu) >> sh;
         const float2 v = buf[(size_t)(r >> 1) * L + pos];
-        ov[(size_t)iu * nv + iv0 + r] = ((r & 1) ? v.y : v.x) * inv;
+        store_from_float(out, vbase + (size_t)iu * nv + iv0 + r, ((r & 1) ? v.y : v.x) * inv, out_dtype);
     }
 }
 
@@ -210,7 +209,9 @@ struct ctsim_fdk {
     ctsim_plan *plan = nullptr;
     int nu = 0, nv = 0, nviews = 0, L = 0, log2L = 0;
     float dbeta = 0.f;
-    float *d_H = nullptr, *d_wcos = nullptr, *d_parker = nullptr, *d_filtered = nullptr;
+    float *d_H = nullptr, *d_wcos = nullptr, *d_parker = nullptr;
+    void *d_filtered = nullptr;  // the filtered sinogram of ctsim_fdk_run_ex, in the input's storage type
+    size_t filtered_bytes = 0;
     float2 *d_tw = nullptr;
 };
 
@@ -304,12 +305,10 @@ extern "C" ctsim_status ctsim_fdk_create(ctsim_plan *plan, const char *window, f
     f->dbeta = (float)dbeta;
 
     cudaError_t e;
-    const size_t nsino = (size_t)G.nu * G.nv * G.noviews;
     const ctsim_plan *p = plan;
     if ((e = ctsim_plan_alloc(p, (void **)&f->d_H, sizeof(float) * f->L)) != cudaSuccess ||
         (e = ctsim_plan_alloc(p, (void **)&f->d_wcos, sizeof(float) * wcos.size())) != cudaSuccess ||
         (e = ctsim_plan_alloc(p, (void **)&f->d_tw, sizeof(float2) * tw.size())) != cudaSuccess ||
-        (e = ctsim_plan_alloc(p, (void **)&f->d_filtered, sizeof(float) * nsino)) != cudaSuccess ||
         (short_scan && (e = ctsim_plan_alloc(p, (void **)&f->d_parker, sizeof(float) * parker.size())) != cudaSuccess)) {
         free_fdk(f);
         return ctsim_set_last_error(CTSIM_ERR_ALLOC, cudaGetErrorString(e));
@@ -330,19 +329,26 @@ extern "C" ctsim_status ctsim_fdk_destroy(ctsim_fdk *f) {
     return CTSIM_OK;
 }
 
-extern "C" ctsim_status ctsim_fdk_filter_ex(ctsim_fdk *f, const void *d_sino, int sino_dtype, float *d_filtered,
-                                            void *stream) {
-    if (!f || !d_sino || !d_filtered) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
-    if (sino_dtype < kF32 || sino_dtype > kF16) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "unknown storage type");
+// The row filter of sino (sino_dtype) into out (out_dtype); FP32 arithmetic.
+static ctsim_status fdk_filter(ctsim_fdk *f, const void *d_sino, int sino_dtype, void *out, int out_dtype,
+                               void *stream) {
     const size_t sm = sizeof(float2) * 4 * f->L;
     if (sm > 200 * 1024) return ctsim_set_last_error(CTSIM_ERR_UNSUPPORTED, "detector too wide for the row filter");
     cudaError_t e = allow_dynamic_smem((const void *)fdk_filter_kernel, sm);
     if (e != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
     dim3 grid((f->nv + kFiltRows - 1) / kFiltRows, f->nviews);
-    fdk_filter_kernel<<<grid, 256, sm, (cudaStream_t)stream>>>(d_sino, sino_dtype, d_filtered, f->d_wcos, f->d_parker, f->d_H,
-                                                                f->d_tw, f->nu, f->nv, f->L, f->log2L);
+    fdk_filter_kernel<<<grid, 256, sm, (cudaStream_t)stream>>>(d_sino, sino_dtype, out, out_dtype, f->d_wcos,
+                                                                f->d_parker, f->d_H, f->d_tw, f->nu, f->nv, f->L,
+                                                                f->log2L);
     if ((e = cudaGetLastError()) != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
     return CTSIM_OK;
+}
+
+extern "C" ctsim_status ctsim_fdk_filter_ex(ctsim_fdk *f, const void *d_sino, int sino_dtype, float *d_filtered,
+                                            void *stream) {
+    if (!f || !d_sino || !d_filtered) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    if (sino_dtype < kF32 || sino_dtype > kF16) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "unknown storage type");
+    return fdk_filter(f, d_sino, sino_dtype, d_filtered, kF32, stream);
 }
 
 extern "C" ctsim_status ctsim_fdk_filter(ctsim_fdk *f, const float *d_sino, float *d_filtered, void *stream) {
@@ -351,11 +357,24 @@ extern "C" ctsim_status ctsim_fdk_filter(ctsim_fdk *f, const float *d_sino, floa
 
 extern "C" ctsim_status ctsim_fdk_run_ex(ctsim_fdk *f, const void *d_sino, int sino_dtype, float *d_image,
                                          void *stream) {
-    if (!f) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
-    ctsim_status s = ctsim_fdk_filter_ex(f, d_sino, sino_dtype, f->d_filtered, stream);
+    if (!f || !d_sino || !d_image) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    if (sino_dtype < kF32 || sino_dtype > kF16) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "unknown storage type");
+    // the filtered sinogram is kept in the input's storage type (a BF16/FP16 request holds
+    // no FP32 sinogram-sized buffer), allocated at the first run that needs its size
+    const size_t need = (size_t)f->nu * f->nv * f->nviews * (sino_dtype == kF32 ? 4 : 2);
+    if (f->filtered_bytes < need) {
+        ctsim_plan_release(f->plan, f->d_filtered);
+        f->d_filtered = nullptr;
+        f->filtered_bytes = 0;
+        cudaError_t e = ctsim_plan_alloc(f->plan, &f->d_filtered, need);
+        if (e != cudaSuccess) return ctsim_set_last_error(CTSIM_ERR_ALLOC, cudaGetErrorString(e));
+        f->filtered_bytes = need;
+    }
+    ctsim_status s = fdk_filter(f, d_sino, sino_dtype, f->d_filtered, sino_dtype, stream);
     if (s != CTSIM_OK) return s;
     // img = backProjectMex(sino, geom, 1, 0, 'back,hpd') * dbeta * 10  (reconFDK.m:84)
-    s = ctsim_plan_backproject(f->plan, CTSIM_BACK_HPD, f->d_filtered, d_image, 0, 1, f->nviews, f->dbeta, stream);
+    s = ctsim_plan_backproject_ex(f->plan, CTSIM_BACK_HPD, f->d_filtered, sino_dtype, d_image, kF32, 0, 1, f->nviews,
+                                  f->dbeta, stream);
     if (s != CTSIM_OK) return s;
     const ctsim_geom &G = *ctsim_plan_geom(f->plan);
     cudaError_t e = launch_scale(d_image, (size_t)G.nx * G.ny * G.nz, 10.0f, (cudaStream_t)stream);

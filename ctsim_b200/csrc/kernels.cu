@@ -17,10 +17,61 @@ namespace ctsim {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// Rows r0 .. r0+3 of one detector column of a sinogram source (element offset off of row
+// r0), times ampv at the same element for the unscaled sources.  VEC: nv a multiple of 4
+// and the source aligned (one 16-byte FP32 or 8-byte 16-bit load); otherwise rows at or
+// past nv read as 0.
+template <int SRC, bool VEC>
+__device__ __forceinline__ float4 load_rows4(const void *__restrict__ src, const float *__restrict__ ampv, size_t off,
+                                             size_t aoff, int r0, int nv) {
+    float4 p;
+    if (SRC == kSrcScaled || SRC == kSrcF32) {
+        const float *pr = static_cast<const float *>(src) + off;
+        if (VEC) {
+            p = __ldg(reinterpret_cast<const float4 *>(pr));
+        } else {
+            p.x = __ldg(pr);
+            p.y = r0 + 1 < nv ? __ldg(pr + 1) : 0.f;
+            p.z = r0 + 2 < nv ? __ldg(pr + 2) : 0.f;
+            p.w = r0 + 3 < nv ? __ldg(pr + 3) : 0.f;
+        }
+    } else {
+        const unsigned short *pr = static_cast<const unsigned short *>(src) + off;
+        unsigned short h[4];
+        if (VEC) {
+            const uint2 u = __ldg(reinterpret_cast<const uint2 *>(pr));
+            h[0] = (unsigned short)(u.x & 0xffffu); h[1] = (unsigned short)(u.x >> 16);
+            h[2] = (unsigned short)(u.y & 0xffffu); h[3] = (unsigned short)(u.y >> 16);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; i++) h[i] = r0 + i < nv ? __ldg(pr + i) : (unsigned short)0;
+        }
+        float f[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            f[i] = SRC == kSrcBF16 ? __uint_as_float((unsigned)h[i] << 16) : __half2float(__ushort_as_half(h[i]));
+        p = make_float4(f[0], f[1], f[2], f[3]);
+    }
+    if (SRC != kSrcScaled) {  // axial amplitude applied here instead of in a scratch copy
+        const float *ar = ampv + aoff;
+        float4 a;
+        if (VEC) {
+            a = __ldg(reinterpret_cast<const float4 *>(ar));
+        } else {
+            a.x = __ldg(ar);
+            a.y = r0 + 1 < nv ? __ldg(ar + 1) : 0.f;
+            a.z = r0 + 2 < nv ? __ldg(ar + 2) : 0.f;
+            a.w = r0 + 3 < nv ? __ldg(ar + 3) : 0.f;
+        }
+        p.x *= a.x; p.y *= a.y; p.z *= a.z; p.w *= a.w;
+    }
+    return p;
+}
+
 // ---------------------------------------------------------------------------
 // A^T: one warp per voxel column, lanes along z; 8 columns (consecutive ix) per block.
 // For each view the warp forms, in shared memory, the u-weighted detector column
-//     q[iv] = sum_iu w_u(iu) * ps[iu][iv]        (ps = proj * ampv, pre-scaled)
+//     q[iv] = sum_iu w_u(iu) * ps[iu][iv]        (ps = proj * ampv)
 // over the rows the column's voxels can touch (4 rows per lane, float4 loads).  Each
 // voxel then sums q over the rows its axial extent covers with the distance-driven
 // row weights of geom/cbct/cbct_back.c:318-357, its edges vmin/vmax computed with the
@@ -32,8 +83,8 @@ constexpr unsigned kFull = 0xffffffffu;
 // ---------------------------------------------------------------------------
 // The work of one block (8 columns of one row iy), as a device function: the plain
 // kernel runs it for blockIdx.x, the batched kernel for each of its work items.
-template <int METHOD, int MZ, bool VEC, bool PRESCALED, bool SUM = false>
-__device__ __forceinline__ void back_block(const Geom g, const View *__restrict__ views, const float *__restrict__ ps,
+template <int METHOD, int MZ, bool VEC, int SRC, bool SUM = false>
+__device__ __forceinline__ void back_block(const Geom g, const View *__restrict__ views, const void *__restrict__ ps,
                                            const uint8_t *__restrict__ map, void *__restrict__ image, int out_dtype,
                                            int view_begin, int view_stride, int view_count, float scale, int qcap,
                                            int *__restrict__ err, const float *__restrict__ ampv, float *smem,
@@ -108,30 +159,16 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                     // [r_lo, r_hi] only)
                     const int nb = iumax - iumin + 1;
                     const float *wj = wtab + j * kWS;
-                    const float *pv = ps + (size_t)(k0 + j) * nuv + (size_t)iumin * g.nv;
+                    const size_t pv = (size_t)(k0 + j) * nuv + (size_t)iumin * g.nv;  // element offsets
+                    const size_t av = (size_t)iumin * g.nv;
                     for (int c = rbase; c <= r_hi; c += 128) {
                         const int r0 = c + 4 * lane;
                         float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f;
                         if (r0 <= r_hi) {
                             for (int b = 0; b < nb; b++) {
                                 const float w = wj[b];
-                                const float *pr = pv + (size_t)b * g.nv + r0;
-                                float4 p;
-                                if (VEC) {
-                                    p = __ldg(reinterpret_cast<const float4 *>(pr));
-                                } else {
-                                    p.x = __ldg(pr);
-                                    p.y = r0 + 1 < g.nv ? __ldg(pr + 1) : 0.f;
-                                    p.z = r0 + 2 < g.nv ? __ldg(pr + 2) : 0.f;
-                                    p.w = r0 + 3 < g.nv ? __ldg(pr + 3) : 0.f;
-                                }
-                                if (!PRESCALED) {  // axial amplitude applied here instead of in a scratch copy
-                                    const float *ar = ampv + (size_t)(iumin + b) * g.nv + r0;
-                                    p.x *= __ldg(ar);
-                                    p.y *= r0 + 1 < g.nv ? __ldg(ar + 1) : 0.f;
-                                    p.z *= r0 + 2 < g.nv ? __ldg(ar + 2) : 0.f;
-                                    p.w *= r0 + 3 < g.nv ? __ldg(ar + 3) : 0.f;
-                                }
+                                const float4 p = load_rows4<SRC, VEC>(ps, ampv, pv + (size_t)b * g.nv + r0,
+                                                                      av + (size_t)b * g.nv + r0, r0, g.nv);
                                 q0 = fmaf(w, p.x, q0); q1 = fmaf(w, p.y, q1);
                                 q2 = fmaf(w, p.z, q2); q3 = fmaf(w, p.w, q3);
                             }
@@ -233,15 +270,15 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
 // view in place, geom/cbct/cbct_back.c:196-214), into scratch.
 // Four resident blocks per SM (registers capped at 64): measured on B200 at config 2,
 // DD 110 -> 100 ms and SF 143 -> 104 ms against the uncapped 80-118 registers.
-template <int METHOD, int MZ, bool VEC, bool PRESCALED = true, bool SUM = false>
+template <int METHOD, int MZ, bool VEC, int SRC = kSrcScaled, bool SUM = false>
 __global__ void __launch_bounds__(256, 4) back_kernel(Geom g, const View *__restrict__ views,
-                                                   const float *__restrict__ ps, const uint8_t *__restrict__ map,
+                                                   const void *__restrict__ ps, const uint8_t *__restrict__ map,
                                                    void *__restrict__ image, int out_dtype, int view_begin,
                                                    int view_stride, int view_count, float scale, int qcap,
                                                    int *__restrict__ err, const float *__restrict__ ampv,
                                                    int block_base) {
     extern __shared__ float smem[];
-    back_block<METHOD, MZ, VEC, PRESCALED, SUM>(g, views, ps, map, image, out_dtype, view_begin, view_stride,
+    back_block<METHOD, MZ, VEC, SRC, SUM>(g, views, ps, map, image, out_dtype, view_begin, view_stride,
                                                 view_count, scale, qcap, err, ampv, smem, block_base + blockIdx.x);
 }
 
@@ -999,9 +1036,19 @@ __global__ void __launch_bounds__(kProjMaxThreads, 3) proj_staged_kernel(Geom g,
 // ---------------------------------------------------------------------------
 // SUM: the FP32 image holds the view sum of earlier view chunks (scale 1), which the
 // kernel continues in the same view order (separate instantiations).
-template <int MODE, int MZ, bool SUM = false>
+// One sinogram sample of storage type DT (kF32, kBF16, kF16) as float (exact widening).
+template <int DT>
+__device__ __forceinline__ float ld_sino(const void *__restrict__ base, size_t i) {
+    if (DT == kBF16) return __uint_as_float((unsigned)__ldg(static_cast<const unsigned short *>(base) + i) << 16);
+    if (DT == kF16) return __half2float(__ushort_as_half(__ldg(static_cast<const unsigned short *>(base) + i)));
+    return __ldg(static_cast<const float *>(base) + i);
+}
+
+// DT: the sinogram's storage type, read as it is (widening to FP32 is exact, so the
+// result equals that of an FP32 copy bit for bit).
+template <int MODE, int MZ, bool SUM = false, int DT = kF32>
 __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict__ views,
-                                                 const float *__restrict__ proj, const uint8_t *__restrict__ map,
+                                                 const void *__restrict__ proj, const uint8_t *__restrict__ map,
                                                  void *__restrict__ image, int out_dtype, int view_begin,
                                                  int view_stride, int view_count, float scale) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1063,7 +1110,7 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
                     const int iu = floor_pos(uj, &fiu);
                     const float wul = fsub(uj, fiu);
                     const float omu = fsub(1.0f, wul);
-                    const float *pv = proj + (size_t)(k0 + j) * nuv + (size_t)iu * g.nv;
+                    const size_t pv = (size_t)(k0 + j) * nuv + (size_t)iu * g.nv;  // element offset
 #pragma unroll
                     for (int m = 0; m < MZ; m++) {
                         if (lane + 32 * m < izn) {
@@ -1084,9 +1131,10 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
                                 const int iv = min(floor_pos(vv, &fiv), g.nv - 2);
                                 const float wvl = fsub(vv, fiv);
                                 const float omv = fsub(1.0f, wvl);
-                                const float *p = pv + iv;
-                                const float s0 = fadd(fmul(omv, __ldg(p)), fmul(wvl, __ldg(p + 1)));
-                                const float s1 = fadd(fmul(omv, __ldg(p + g.nv)), fmul(wvl, __ldg(p + g.nv + 1)));
+                                const size_t p = pv + iv;
+                                const float s0 = fadd(fmul(omv, ld_sino<DT>(proj, p)), fmul(wvl, ld_sino<DT>(proj, p + 1)));
+                                const float s1 = fadd(fmul(omv, ld_sino<DT>(proj, p + g.nv)),
+                                                      fmul(wvl, ld_sino<DT>(proj, p + g.nv + 1)));
                                 const float val = fadd(fmul(omu, s0), fmul(wul, s1));
                                 // w2s * (...) (cbct_back.c:120); w2s * w2s * (...) (cbct_back_var.c:116)
                                 acc[m] = fadd(acc[m], fmul(VAR ? fmul(w2sj, w2sj) : w2sj, val));
@@ -1137,18 +1185,18 @@ cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes) {
 // warp's buffer for the branch-free row reads
 size_t back_smem_bytes(int qcap) { return ((size_t)8 * (32 * 17 + qcap) + 4) * sizeof(float); }
 
-template <int METHOD, int MZ, bool VEC, bool SUM>
-static cudaError_t launch_back_mz(const Geom &g, const View *views, const float *ps, const uint8_t *map,
-                                  void *image, int out_dtype, int vb, int vs, int vc, float scale, int qcap,
-                                  int *err, int y_begin, int y_end, cudaStream_t st) {
+template <int METHOD, int MZ, bool VEC, int SRC, bool SUM>
+static cudaError_t launch_back_mz(const Geom &g, const View *views, const void *ps, const float *ampv,
+                                  const uint8_t *map, void *image, int out_dtype, int vb, int vs, int vc, float scale,
+                                  int qcap, int *err, int y_begin, int y_end, cudaStream_t st) {
     const int tiles_x = (g.nx + 7) / 8;
     const int blocks = (y_end - y_begin) * tiles_x;
     if (blocks <= 0) return cudaSuccess;
     const size_t sm = back_smem_bytes(qcap);
-    auto kfn = back_kernel<METHOD, MZ, VEC, true, SUM>;
+    auto kfn = back_kernel<METHOD, MZ, VEC, SRC, SUM>;
     cudaError_t e = allow_dynamic_smem((const void *)kfn, sm);
     if (e != cudaSuccess) return e;
-    kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap, err, nullptr,
+    kfn<<<blocks, 256, sm, st>>>(g, views, ps, map, image, out_dtype, vb, vs, vc, scale, qcap, err, ampv,
                                  y_begin * tiles_x);
     return cudaGetLastError();
 }
@@ -1161,30 +1209,38 @@ cudaError_t launch_prescale(const void *proj, int in_dtype, const float *ampv, f
     return cudaGetLastError();
 }
 
-cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *ps, const uint8_t *map,
+cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const void *ps, const uint8_t *map,
                         void *image, int out_dtype, int vb, int vs, int vc, float scale, int qcap, int *err,
-                        cudaStream_t st, bool accumulate, int y_begin, int y_end) {
-    if (accumulate && (out_dtype != kF32 || scale != 1.0f)) return cudaErrorInvalidValue;
+                        cudaStream_t st, bool accumulate, int y_begin, int y_end, int src, const float *ampv) {
+    if (accumulate && (out_dtype != kF32 || scale != 1.0f || src != kSrcScaled)) return cudaErrorInvalidValue;
+    if (src != kSrcScaled && src != kSrcBF16 && src != kSrcF16) return cudaErrorInvalidValue;
+    if (src != kSrcScaled && !ampv) return cudaErrorInvalidValue;
     if (y_end < 0) y_end = g.ny;
     if (y_begin < 0 || y_end > g.ny || y_begin > y_end) return cudaErrorInvalidValue;
-    const bool vec = (g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(ps) % 16) == 0;
+    const size_t align = src == kSrcScaled ? 16 : 8;  // one float4, or four 16-bit values, per load
+    const bool vec = (g.nv % 4) == 0 && (reinterpret_cast<uintptr_t>(ps) % align) == 0 &&
+                     (reinterpret_cast<uintptr_t>(ampv) % 16) == 0;
     // accumulate: the image holds the FP32 view sum of earlier views, which the kernel
     // continues (separate instantiations, so the plain kernel keeps its registers)
+#define CTSIM_BACK_ARGS g, views, ps, ampv, map, image, out_dtype, vb, vs, vc, scale, qcap, err, y_begin, y_end, st
 #define CTSIM_BACK_CASE(M, Z)                                                                            \
     if (method == M && mz == Z) {                                                                        \
         if (accumulate)                                                                                  \
-            return vec ? launch_back_mz<M, Z, true, true>(g, views, ps, map, image, out_dtype, vb, vs, vc, \
-                                                          scale, qcap, err, y_begin, y_end, st)          \
-                       : launch_back_mz<M, Z, false, true>(g, views, ps, map, image, out_dtype, vb, vs,  \
-                                                           vc, scale, qcap, err, y_begin, y_end, st);    \
-        return vec ? launch_back_mz<M, Z, true, false>(g, views, ps, map, image, out_dtype, vb, vs, vc,  \
-                                                       scale, qcap, err, y_begin, y_end, st)             \
-                   : launch_back_mz<M, Z, false, false>(g, views, ps, map, image, out_dtype, vb, vs, vc, \
-                                                        scale, qcap, err, y_begin, y_end, st);           \
+            return vec ? launch_back_mz<M, Z, true, kSrcScaled, true>(CTSIM_BACK_ARGS)                   \
+                       : launch_back_mz<M, Z, false, kSrcScaled, true>(CTSIM_BACK_ARGS);                 \
+        if (src == kSrcBF16)                                                                             \
+            return vec ? launch_back_mz<M, Z, true, kSrcBF16, false>(CTSIM_BACK_ARGS)                    \
+                       : launch_back_mz<M, Z, false, kSrcBF16, false>(CTSIM_BACK_ARGS);                  \
+        if (src == kSrcF16)                                                                              \
+            return vec ? launch_back_mz<M, Z, true, kSrcF16, false>(CTSIM_BACK_ARGS)                     \
+                       : launch_back_mz<M, Z, false, kSrcF16, false>(CTSIM_BACK_ARGS);                   \
+        return vec ? launch_back_mz<M, Z, true, kSrcScaled, false>(CTSIM_BACK_ARGS)                      \
+                   : launch_back_mz<M, Z, false, kSrcScaled, false>(CTSIM_BACK_ARGS);                    \
     }
     CTSIM_BACK_CASE(kDD, 1) CTSIM_BACK_CASE(kDD, 2) CTSIM_BACK_CASE(kDD, 4) CTSIM_BACK_CASE(kDD, 8)
     CTSIM_BACK_CASE(kTF, 1) CTSIM_BACK_CASE(kTF, 2) CTSIM_BACK_CASE(kTF, 4) CTSIM_BACK_CASE(kTF, 8)
 #undef CTSIM_BACK_CASE
+#undef CTSIM_BACK_ARGS
     return cudaErrorInvalidValue;
 }
 
@@ -1294,24 +1350,32 @@ cudaError_t launch_proj(int method, int groups, int rows, bool pairs, const Geom
 }
 
 template <int MODE, int MZ>
-static cudaError_t launch_pd_mz(const Geom &g, const View *views, const float *proj, const uint8_t *map,
+static cudaError_t launch_pd_mz(const Geom &g, const View *views, const void *proj, int in_dtype, const uint8_t *map,
                                 void *image, int out_dtype, int vb, int vs, int vc, float scale, bool accumulate,
                                 cudaStream_t st) {
     const int blocks = g.ny * ((g.nx + 7) / 8);
     if (accumulate)
         pd_kernel<MODE, MZ, true><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale);
+    else if (in_dtype == kBF16)
+        pd_kernel<MODE, MZ, false, kBF16><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc,
+                                                                  scale);
+    else if (in_dtype == kF16)
+        pd_kernel<MODE, MZ, false, kF16><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc,
+                                                                 scale);
     else
         pd_kernel<MODE, MZ><<<blocks, 256, 0, st>>>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale);
     return cudaGetLastError();
 }
 
-cudaError_t launch_pd(int mode, int mz, const Geom &g, const View *views, const float *proj, const uint8_t *map,
+cudaError_t launch_pd(int mode, int mz, const Geom &g, const View *views, const void *proj, const uint8_t *map,
                       void *image, int out_dtype, int vb, int vs, int vc, float scale, cudaStream_t st,
-                      bool accumulate) {
-    if (accumulate && (out_dtype != kF32 || scale != 1.0f)) return cudaErrorInvalidValue;
+                      bool accumulate, int in_dtype) {
+    if (accumulate && (out_dtype != kF32 || scale != 1.0f || in_dtype != kF32)) return cudaErrorInvalidValue;
+    if (in_dtype != kF32 && in_dtype != kBF16 && in_dtype != kF16) return cudaErrorInvalidValue;
 #define CTSIM_PD_CASE(O, Z)                                                                                    \
     if (mode == O && mz == Z)                                                                                  \
-        return launch_pd_mz<O, Z>(g, views, proj, map, image, out_dtype, vb, vs, vc, scale, accumulate, st);
+        return launch_pd_mz<O, Z>(g, views, proj, in_dtype, map, image, out_dtype, vb, vs, vc, scale, accumulate, \
+                                  st);
     CTSIM_PD_CASE(kPdOff, 1) CTSIM_PD_CASE(kPdOff, 2) CTSIM_PD_CASE(kPdOff, 4) CTSIM_PD_CASE(kPdOff, 8)
     CTSIM_PD_CASE(kPdClamp, 1) CTSIM_PD_CASE(kPdClamp, 2) CTSIM_PD_CASE(kPdClamp, 4) CTSIM_PD_CASE(kPdClamp, 8)
     CTSIM_PD_CASE(kPdVar, 1) CTSIM_PD_CASE(kPdVar, 2) CTSIM_PD_CASE(kPdVar, 4) CTSIM_PD_CASE(kPdVar, 8)
@@ -1334,7 +1398,7 @@ static cudaError_t launch_back_unscaled_mz(const Geom &g, const View *views, con
                                            cudaStream_t st) {
     const int blocks = g.ny * ((g.nx + 7) / 8);
     const size_t sm = back_smem_bytes(qcap);
-    auto kfn = back_kernel<METHOD, MZ, false, false>;
+    auto kfn = back_kernel<METHOD, MZ, false, kSrcF32>;
     cudaError_t e = allow_dynamic_smem((const void *)kfn, sm);
     if (e != cudaSuccess) return e;
     kfn<<<blocks, 256, sm, st>>>(g, views, proj, map, image, kF32, 0, 1, vc, 1.0f, qcap, err, ampv, 0);
@@ -1408,7 +1472,7 @@ __global__ void __launch_bounds__(kProjMaxThreads, 3) proj_staged_batch_kernel(c
     }
 }
 
-template <int METHOD, int MZ, bool VEC, bool LOWP>
+template <int METHOD, int MZ, bool VEC, bool LOWP, int SRC>
 __global__ void __launch_bounds__(256) back_batch_kernel(const __grid_constant__ BackBatch b) {
     extern __shared__ float smem_batch[];
     for (int blk = blockIdx.x; blk < b.total; blk += gridDim.x) {
@@ -1418,8 +1482,8 @@ __global__ void __launch_bounds__(256) back_batch_kernel(const __grid_constant__
             if (b.t[mid].first <= blk) lo = mid; else hi = mid - 1;
         }
         const BackTask &T = b.t[lo];
-        back_block<METHOD, MZ, VEC, true>(T.g, T.views, T.ps, T.map, T.image, LOWP ? T.out_dtype : kF32, T.vb, T.vs,
-                                          T.vc, T.scale, T.qcap, T.err, nullptr, smem_batch, blk - T.first);
+        back_block<METHOD, MZ, VEC, SRC>(T.g, T.views, T.ps, T.map, T.image, LOWP ? T.out_dtype : kF32, T.vb, T.vs,
+                                         T.vc, T.scale, T.qcap, T.err, T.ampv, smem_batch, blk - T.first);
         // the per-warp row buffers are laid out with the task's own stride, so a warp may
         // not start the next item (possibly another task) while its neighbours still work
         __syncthreads();
@@ -1477,21 +1541,29 @@ cudaError_t launch_proj_staged_batch(int method, int groups, int row_threads, in
 }
 
 cudaError_t launch_back_batch(int method, int mz, bool vec, bool lowp, size_t smem, const BackBatch &b,
-                              cudaStream_t st) {
+                              cudaStream_t st, int src) {
     if (b.n < 1 || b.total < 1) return cudaSuccess;
-#define CTSIM_BB_CASE(M, Z, V)                                                                        \
-    if (method == M && mz == Z && vec == V) {                                                         \
-        auto k = lowp ? back_batch_kernel<M, Z, V, true> : back_batch_kernel<M, Z, V, false>;         \
+    if (src != kSrcScaled && src != kSrcBF16 && src != kSrcF16) return cudaErrorInvalidValue;
+#define CTSIM_BB_LAUNCH(M, Z, V, S)                                                                   \
+    {                                                                                                 \
+        auto k = lowp ? back_batch_kernel<M, Z, V, true, S> : back_batch_kernel<M, Z, V, false, S>;   \
         cudaError_t e = allow_dynamic_smem((const void *)k, smem);                                    \
         if (e != cudaSuccess) return e;                                                               \
         k<<<persistent_grid(k, 256, smem, b.total), 256, smem, st>>>(b);                              \
         return cudaGetLastError();                                                                    \
+    }
+#define CTSIM_BB_CASE(M, Z, V)                                                                        \
+    if (method == M && mz == Z && vec == V) {                                                         \
+        if (src == kSrcBF16) CTSIM_BB_LAUNCH(M, Z, V, kSrcBF16)                                       \
+        if (src == kSrcF16) CTSIM_BB_LAUNCH(M, Z, V, kSrcF16)                                         \
+        CTSIM_BB_LAUNCH(M, Z, V, kSrcScaled)                                                          \
     }
     CTSIM_BB_CASE(kDD, 1, true) CTSIM_BB_CASE(kDD, 2, true) CTSIM_BB_CASE(kDD, 4, true) CTSIM_BB_CASE(kDD, 8, true)
     CTSIM_BB_CASE(kDD, 1, false) CTSIM_BB_CASE(kDD, 2, false) CTSIM_BB_CASE(kDD, 4, false) CTSIM_BB_CASE(kDD, 8, false)
     CTSIM_BB_CASE(kTF, 1, true) CTSIM_BB_CASE(kTF, 2, true) CTSIM_BB_CASE(kTF, 4, true) CTSIM_BB_CASE(kTF, 8, true)
     CTSIM_BB_CASE(kTF, 1, false) CTSIM_BB_CASE(kTF, 2, false) CTSIM_BB_CASE(kTF, 4, false) CTSIM_BB_CASE(kTF, 8, false)
 #undef CTSIM_BB_CASE
+#undef CTSIM_BB_LAUNCH
     return cudaErrorInvalidValue;
 }
 

@@ -14,10 +14,15 @@ namespace ctsim {
 cudaError_t launch_prescale(const void *proj, int in_dtype, const float *ampv, float *ps, size_t nuv, size_t n,
                             cudaStream_t st);
 
-cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const float *ps, const uint8_t *map,
+// Sinogram sources of the backprojector: FP32 already multiplied by the axial amplitude
+// ampv (a pre-scaled copy, or a residual written that way), or the stored sinogram in
+// FP32, BF16 or FP16, multiplied by ampv as it is read.  launch_back and the batches take
+// kSrcScaled, kSrcBF16 and kSrcF16 (kSrcF32 serves the entry point without allocations).
+enum BackSrc { kSrcScaled = 0, kSrcF32 = 1, kSrcBF16 = 2, kSrcF16 = 3 };
+cudaError_t launch_back(int method, int mz, const Geom &g, const View *views, const void *ps, const uint8_t *map,
                         void *image, int out_dtype, int view_begin, int view_stride, int view_count, float scale,
                         int qcap, int *err, cudaStream_t st, bool accumulate = false, int y_begin = 0,
-                        int y_end = -1);
+                        int y_end = -1, int src = kSrcScaled, const float *ampv = nullptr);
 size_t back_smem_bytes(int qcap);
 cudaError_t launch_back_unscaled(int mz, const Geom &g, const View *views, const float *proj, const float *ampv,
                                  const uint8_t *map, float *image, int view_count, int qcap, int *err,
@@ -51,9 +56,10 @@ bool proj_slots_valid(int xstride, int slots);
 // voxel-driven bilinear modes: back,pd (v outside the detector skipped), back,hpd (v
 // clamped), back,var (geom/cbct/cbct_back_var.c)
 enum PdMode { kPdOff = 0, kPdClamp = 1, kPdVar = 2 };
-cudaError_t launch_pd(int mode, int mz, const Geom &g, const View *views, const float *proj,
+// proj in storage type in_dtype (kF32, kBF16, kF16), read as it is.
+cudaError_t launch_pd(int mode, int mz, const Geom &g, const View *views, const void *proj,
                       const uint8_t *map, void *image, int out_dtype, int view_begin, int view_stride,
-                      int view_count, float scale, cudaStream_t st, bool accumulate = false);
+                      int view_count, float scale, cudaStream_t st, bool accumulate = false, int in_dtype = kF32);
 
 cudaError_t launch_scale(float *y, size_t n, float s, cudaStream_t st);
 
@@ -82,7 +88,8 @@ struct ProjBatch {
 struct BackTask {
     Geom g;
     const View *views;
-    const float *ps;
+    const void *ps;         // the class's source form (BackSrc)
+    const float *ampv;      // the plan's axial amplitudes (unscaled sources)
     const uint8_t *map;
     void *image;
     int out_dtype;
@@ -103,7 +110,7 @@ int proj_row_threads_of(int nv);
 cudaError_t launch_proj_batch(int method, int groups, int row_threads, bool pairs, bool lowp, size_t smem,
                               const ProjBatch &b, cudaStream_t st);
 cudaError_t launch_back_batch(int method, int mz, bool vec, bool lowp, size_t smem, const BackBatch &b,
-                              cudaStream_t st);
+                              cudaStream_t st, int src = kSrcScaled);
 // The staged forward projector (launch_proj_staged) over a batch of plain-layout plans.
 cudaError_t launch_proj_staged_batch(int method, int groups, int row_threads, int slots, bool lowp, size_t smem,
                                      const ProjBatch &b, cudaStream_t st);

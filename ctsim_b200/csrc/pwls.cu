@@ -8,10 +8,15 @@
 //   sqdiff           sum((a - b)^2) for the iteration's rmsd      reconPwlsSeSqs.m:81
 //   nesterov_update  the Nesterov step of reconPwlsSeNesterovSqs.m:65-87
 // Image layout [nz][ny][nx] (MATLAB x(i,j,k) = img[k][j][i]).  Reductions in FP64.
+#include <algorithm>
 #include <cmath>
 
 #include "../../include/ctsim_b200.h"
 #include "kernels.cuh"
+
+// plan internals (capi.cu)
+extern const ctsim_geom *ctsim_plan_geom(const ctsim_plan *p);
+extern const float *ctsim_plan_ampv(const ctsim_plan *p);
 
 using namespace ctsim;
 
@@ -46,6 +51,28 @@ __global__ void residual_kernel(const float *__restrict__ ax, const void *__rest
         const float wi = load_as_float(w, i, dtype) * w_scale;
         wd[i] = wi * d;
         acc += (double)wi * (double)d * (double)d;
+    }
+    if (phi) block_add_double(acc, phi);
+}
+
+// The residual of view_count views written as (w d) * ampv per detector pixel (the
+// product A^T forms first, in the same order, so the backprojection of this output equals
+// that of the plain residual bit for bit).  Blocks run along the pixels of one view
+// (blockIdx.y), so the amplitude index needs no division.
+__global__ void residual_scaled_kernel(const float *__restrict__ ax, const void *__restrict__ y,
+                                       const void *__restrict__ w, int dtype, float w_scale,
+                                       const float *__restrict__ ampv, float *__restrict__ wd, int nuv, int views,
+                                       double *__restrict__ phi) {
+    double acc = 0.0;
+    for (int k = blockIdx.y; k < views; k += gridDim.y) {
+        const size_t base = (size_t)k * nuv;
+        for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nuv; p += gridDim.x * blockDim.x) {
+            const size_t i = base + p;
+            const float d = ax[i] - load_as_float(y, i, dtype);
+            const float wi = load_as_float(w, i, dtype) * w_scale;
+            wd[i] = (wi * d) * ampv[p];
+            acc += (double)wi * (double)d * (double)d;
+        }
     }
     if (phi) block_add_double(acc, phi);
 }
@@ -229,6 +256,25 @@ extern "C" ctsim_status ctsim_pwls_residual_ex(const float *d_ax, const void *d_
     if (dtype < kF32 || dtype > kF16) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "unknown storage type");
     if (n == 0) return CTSIM_OK;
     residual_kernel<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(d_ax, d_y, d_w, dtype, w_scale, d_wd, n, d_phi);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? CTSIM_OK : ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
+}
+
+extern "C" ctsim_status ctsim_pwls_residual_scaled(const ctsim_plan *plan, const float *d_ax, const void *d_y,
+                                                   const void *d_w, int dtype, float w_scale, float *d_wd,
+                                                   int view_count, double *d_phi, void *stream) {
+    if (!plan || !d_ax || !d_y || !d_w || !d_wd) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    if (dtype < kF32 || dtype > kF16) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "unknown storage type");
+    const ctsim_geom &G = *ctsim_plan_geom(plan);
+    if (view_count < 0 || view_count > G.noviews)
+        return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "view_count outside the plan's views");
+    if (view_count == 0) return CTSIM_OK;
+    const int nuv = G.nu * G.nv;
+    const int gx = std::max(1, std::min((nuv + 255) / 256, 148 * 16 / std::min(view_count, 65535)));
+    dim3 grid(gx, std::min(view_count, 65535));
+    residual_scaled_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(d_ax, d_y, d_w, dtype, w_scale,
+                                                                   ctsim_plan_ampv(plan), d_wd, nuv, view_count,
+                                                                   d_phi);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? CTSIM_OK : ctsim_set_last_error(CTSIM_ERR_CUDA, cudaGetErrorString(e));
 }

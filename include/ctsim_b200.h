@@ -61,6 +61,13 @@ typedef enum {
     CTSIM_BACK_VAR = 6  /* "back,var": variance backprojection, geom/cbct/cbct_back_var.c:1 */
 } ctsim_method;
 
+/* OR'ed into CTSIM_BACK_DD / CTSIM_BACK_TF in ctsim_plan_backproject_ex and
+ * ctsim_batch_backproject (no reference counterpart): the FP32 sinogram is already
+ * multiplied by the plan's axial amplitude table, the per-pixel factor that A^T applies
+ * first (geom/cbct/cbct_back.c:196-214), as ctsim_pwls_residual_scaled writes its
+ * residual.  The backprojection then reads it as it is: no scaled copy, no scratch. */
+#define CTSIM_INPUT_SCALED 0x100
+
 /* Storage types of volumes and sinograms in the plan API (arithmetic is always FP32). */
 typedef enum {
     CTSIM_F32 = 0,
@@ -279,7 +286,10 @@ ctsim_status ctsim_fdk_filter(ctsim_fdk *fdk, const float *d_sino, float *d_filt
 /* Full FDK: filter, back,hpd, times dbeta, times 10 (reconFDK.m:84).  Image overwritten. */
 ctsim_status ctsim_fdk_run(ctsim_fdk *fdk, const float *d_sino, float *d_image, void *stream);
 
-/* The same with the sinogram stored as sino_dtype (ctsim_dtype; widened to FP32 on load). */
+/* The same with the sinogram stored as sino_dtype (ctsim_dtype; widened to FP32 on load).
+ * ctsim_fdk_run_ex keeps the filtered sinogram in sino_dtype too (FP32 filter arithmetic,
+ * rounded once at its store; the backprojection reads it as it is), in a buffer of the
+ * FDK object allocated at the first run of each size. */
 ctsim_status ctsim_fdk_filter_ex(ctsim_fdk *fdk, const void *d_sino, int sino_dtype, float *d_filtered, void *stream);
 ctsim_status ctsim_fdk_run_ex(ctsim_fdk *fdk, const void *d_sino, int sino_dtype, float *d_image, void *stream);
 
@@ -309,6 +319,15 @@ ctsim_status ctsim_pwls_residual(const float *d_ax, const float *d_y, const floa
  * formed in FP32. */
 ctsim_status ctsim_pwls_residual_ex(const float *d_ax, const void *d_y, const void *d_w, int dtype, float w_scale,
                                     float *d_wd, size_t n, double *d_phi, void *stream);
+
+/* ctsim_pwls_residual_ex for view_count views of `plan`'s detector, with the weighted
+ * residual written already multiplied by the plan's axial amplitude table (wd = (w d) *
+ * ampv per pixel, the product A^T forms first), for ctsim_plan_backproject_ex with
+ * CTSIM_INPUT_SCALED; *d_phi accumulates sum(w d^2) as before (no reference counterpart:
+ * it fuses the residual with the first step of the backprojection). */
+ctsim_status ctsim_pwls_residual_scaled(const ctsim_plan *plan, const float *d_ax, const void *d_y, const void *d_w,
+                                        int dtype, float w_scale, float *d_wd, int view_count, double *d_phi,
+                                        void *stream);
 
 /* *d_acc += sum((a - b)^2) in FP64 (the iteration rmsd, reconPwlsSeSqs.m:81). */
 ctsim_status ctsim_sqdiff(const float *d_a, const float *d_b, size_t n, double *d_acc, void *stream);
