@@ -68,7 +68,7 @@ __global__ void residual_scaled_kernel(const float *__restrict__ ax, const void 
         const size_t base = (size_t)k * nuv;
         for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nuv; p += gridDim.x * blockDim.x) {
             const size_t i = base + p;
-            const float d = ax[i] - load_as_float(y, i, dtype);
+            const float d = y ? ax[i] - load_as_float(y, i, dtype) : ax[i];
             const float wi = load_as_float(w, i, dtype) * w_scale;
             wd[i] = (wi * d) * ampv[p];
             acc += (double)wi * (double)d * (double)d;
@@ -263,7 +263,7 @@ extern "C" ctsim_status ctsim_pwls_residual_ex(const float *d_ax, const void *d_
 extern "C" ctsim_status ctsim_pwls_residual_scaled(const ctsim_plan *plan, const float *d_ax, const void *d_y,
                                                    const void *d_w, int dtype, float w_scale, float *d_wd,
                                                    int view_count, double *d_phi, void *stream) {
-    if (!plan || !d_ax || !d_y || !d_w || !d_wd) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
+    if (!plan || !d_ax || !d_w || !d_wd) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "null argument");
     if (dtype < kF32 || dtype > kF16) return ctsim_set_last_error(CTSIM_ERR_ARGUMENT, "unknown storage type");
     const ctsim_geom &G = *ctsim_plan_geom(plan);
     if (view_count < 0 || view_count > G.noviews)

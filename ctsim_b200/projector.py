@@ -240,9 +240,10 @@ class Plan:
         return out
 
     def backproject(self, sino, method: str = "dd", view_begin: int = 0, view_stride: int = 1, view_count=None,
-                    scale: float = 1.0, out=None, out_dtype=None):
+                    scale: float = 1.0, out=None, out_dtype=None, scaled: bool = False):
         """scale * A^T y (or the FDK pd/hpd, or the variance backprojection) -> [nz, ny, nx] of ``out_dtype``
-        (default: the sinogram's storage type)."""
+        (default: the sinogram's storage type).  ``scaled``: the FP32 sinogram is already
+        multiplied by the plan's axial amplitudes (CTSIM_INPUT_SCALED, dd/tf)."""
         torch = _torch()
         vb, vs, vc = self._views(view_begin, view_stride, view_count)
         sino = self._check_tensor(sino, (vc, self.geom.nu, self.geom.nv), "sino")
@@ -251,7 +252,7 @@ class Plan:
         else:
             out = self._check_tensor(out, self.geom.image_shape, "out")
         m = {"dd": 2, "tf": 3, "pd": 4, "hpd": 5, "var": 6, "back,dd": 2, "back,tf": 3, "back,pd": 4, "back,hpd": 5,
-             "back,var": 6}[method]
+             "back,var": 6}[method] | (_lib.INPUT_SCALED if scaled else 0)
         st = torch.cuda.current_stream(self.device).cuda_stream
         _lib.check(self._L.ctsim_plan_backproject_ex(self._h, m, sino.data_ptr(), _DTYPES[sino.dtype],
                                                      out.data_ptr(), _DTYPES[out.dtype], vb, vs, vc, float(scale),
@@ -363,7 +364,8 @@ def batch_project(method: str, entries):
     _batch("ctsim_batch_project", {"dd": 0, "tf": 1}[method], [e + (1.0,) if len(e) == 6 else e for e in entries])
 
 
-def batch_backproject(method: str, entries):
+def batch_backproject(method: str, entries, scaled: bool = False):
     """scale * A^T of many plans: entries are (plan, sino, out_image, view_begin,
-    view_stride, view_count, scale) (ctsim_batch_backproject)."""
-    _batch("ctsim_batch_backproject", {"dd": 2, "tf": 3}[method], entries)
+    view_stride, view_count, scale) (ctsim_batch_backproject); ``scaled`` as in
+    Plan.backproject."""
+    _batch("ctsim_batch_backproject", {"dd": 2, "tf": 3}[method] | (_lib.INPUT_SCALED if scaled else 0), entries)

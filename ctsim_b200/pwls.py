@@ -111,27 +111,32 @@ class PwlsSolver:
         self.storage = storage or torch.float32
         from .projector import _DTYPES
         self.sdt = _DTYPES[self.storage]
-        y32 = y.to(self.dev, torch.float32).contiguous()
+        if img0 is None:
+            from .fdk import reconFDK
+            img0 = reconFDK(y.to(self.dev, torch.float32).contiguous(), geom)
         y = y.to(self.dev, self.storage).contiguous()
-        w32 = w.to(self.dev, torch.float32)
         # weights are photon counts (1e5 and more): FP16 stores them divided by a power of two
         self.w_scale = 1.0
         if self.storage == torch.float16:
+            w32 = w.to(self.dev, torch.float32)
             wmax = float(w32.max().item())
             if wmax > 16384.0:
                 self.w_scale = float(2.0 ** math.ceil(math.log2(wmax / 16384.0)))
-        w = (w32 / self.w_scale).to(self.storage).contiguous()
-        del w32
-        if img0 is None:
-            from .fdk import reconFDK
-            img0 = reconFDK(y32, geom)
-        del y32
+            w = (w32 / self.w_scale).to(self.storage).contiguous()
+            del w32
+        else:
+            w = w.to(self.dev, self.storage).contiguous()
         self.x = img0.to(self.dev, torch.float32).clone().contiguous()
         self.xn = torch.empty_like(self.x)
         self.xold = torch.empty_like(self.x)
-        # precompute (reconPwlsSeSqs.m:40-41): a = A(1), precom = At(w .* a)
+        # precompute (reconPwlsSeSqs.m:40-41): a = A(1), precom = At(w .* a); w .* a is written
+        # over a already times the axial amplitudes (the first product of At), so one FP32
+        # sinogram-sized buffer serves both
         a = self.plan.project(torch.ones_like(self.x), method)
-        self.precom = self.plan.backproject((w.float() * self.w_scale * a).contiguous(), method)
+        _lib.check(self.L.ctsim_pwls_residual_scaled(self.plan._h, a.data_ptr(), None, w.data_ptr(), self.sdt,
+                                                     self.w_scale, a.data_ptr(), geom.noViews, None,
+                                                     _stream(self.dev)), "ctsim_pwls_residual_scaled")
+        self.precom = self.plan.backproject(a, method, scaled=True)
         del a
         # subsets 1+mod(isub,M):M:end for isub = 1..M (0-based start isub % M)
         self.subsets = []
@@ -160,14 +165,20 @@ class PwlsSolver:
         ax = self.ax[:count]
         wd = self.wd[:count]
         self.plan.project(self.x, self.method, start, stride, count, out=ax)
-        _lib.check(self.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), self.sdt,
-                                                 self.w_scale, wd.data_ptr(), ax.numel(), acc, st),
-                   "ctsim_pwls_residual")
-        self.plan.backproject(wd, self.method, start, stride, count, scale=float(self.M), out=self.num)
+        self._residual(ax, ys, ws, wd, count, acc, st)
+        self.plan.backproject(wd, self.method, start, stride, count, scale=float(self.M), out=self.num, scaled=True)
         _lib.check(self.L.ctsim_sqs_update(self.kind, self.beta, self.delta, self.nx, self.ny, self.nz,
                                            self.x.data_ptr(), self.xn.data_ptr(), self.num.data_ptr(),
                                            self.precom.data_ptr(), st), "ctsim_sqs_update")
         self.x, self.xn = self.xn, self.x
+
+    def _residual(self, ax, ys, ws, wd, count, acc, st):
+        """wd = (w (A_s x - y_s)) * ampv per pixel (the weighted residual with the first
+        product of A^T applied: backprojected with scaled=True, no scaled copy), and the
+        data term sum(w d^2) into the FP64 accumulator at acc (reconPwlsSeSqs.m:57-74)."""
+        _lib.check(self.L.ctsim_pwls_residual_scaled(self.plan._h, ax.data_ptr(), ys.data_ptr(), ws.data_ptr(),
+                                                     self.sdt, self.w_scale, wd.data_ptr(), count, acc, st),
+                   "ctsim_pwls_residual_scaled")
 
     def end_iteration(self):
         """Penalty value and squared change of the iteration into the FP64 accumulators
@@ -238,10 +249,8 @@ class PwlsNesterovSolver(PwlsSolver):
         ax = self.ax[:count]
         wd = self.wd[:count]
         self.plan.project(self.z, self.method, start, stride, count, out=ax)        # Aos(z, isub)
-        _lib.check(self.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), self.sdt,
-                                                 self.w_scale, wd.data_ptr(), ax.numel(), acc, st),
-                   "ctsim_pwls_residual")
-        self.plan.backproject(wd, self.method, start, stride, count, scale=float(self.M), out=self.num)
+        self._residual(ax, ys, ws, wd, count, acc, st)
+        self.plan.backproject(wd, self.method, start, stride, count, scale=float(self.M), out=self.num, scaled=True)
         t_next = (1.0 + math.sqrt(1.0 + 4.0 * self.t * self.t)) / 2.0
         _lib.check(self.L.ctsim_nesterov_update(self.kind, self.beta, self.delta, self.nx, self.ny, self.nz,
                                                 self.z.data_ptr(), self.x.data_ptr(), self.s.data_ptr(),
@@ -320,11 +329,9 @@ def batched_subset_steps(pairs):
     for s, i in pairs:
         start, count, ys, ws = s.subsets[i]
         ax, wd = s.ax[:count], s.wd[:count]
-        _lib.check(s.L.ctsim_pwls_residual_ex(ax.data_ptr(), ys.data_ptr(), ws.data_ptr(), s.sdt, s.w_scale,
-                                              wd.data_ptr(), ax.numel(), s.acc.data_ptr(), _stream(s.dev)),
-                   "ctsim_pwls_residual")
+        s._residual(ax, ys, ws, wd, count, s.acc.data_ptr(), _stream(s.dev))
         back.append((s.plan, wd, s.num, start, 1 if s.M == 1 else s.M, count, float(s.M)))
-    batch_backproject(method, back)
+    batch_backproject(method, back, scaled=True)
     for s, i in pairs:
         _lib.check(s.L.ctsim_sqs_update(s.kind, s.beta, s.delta, s.nx, s.ny, s.nz, s.x.data_ptr(),
                                         s.xn.data_ptr(), s.num.data_ptr(), s.precom.data_ptr(), _stream(s.dev)),

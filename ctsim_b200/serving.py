@@ -77,7 +77,10 @@ def _dtype(name):
 
 def hbm_footprint(req: ReconRequest) -> int:
     """Upper bound of the device bytes a request holds while active: plan tables and
-    scratch, FDK buffers, the stored sinogram/weights and the FP32 solver state."""
+    prefix sums, FDK tables and filtered sinogram, the stored sinogram/weights and the FP32
+    solver state.  Sinogram-sized data is held in the request's storage type (s bytes per
+    pixel): the plan reads BF16/FP16 sinograms and pre-scaled residuals as they are, so
+    no FP32 sinogram-sized scratch is allocated for a served request."""
     g = req.geom
     vox = g.nx * g.ny * g.nz
     pix = g.nu * g.nv * g.noViews
@@ -85,17 +88,18 @@ def hbm_footprint(req: ReconRequest) -> int:
     L = 64
     while L < 2 * g.nu - 1:
         L *= 2
-    xs = 8 * g.nx * g.ny * (g.nz + 1)  # column prefix sums (paired layout at most)
-    plan = xs + 4 * pix + 4 * g.nu * g.nv + g.nx * g.ny + 64 * g.noViews + 4096
-    fdk = 4 * pix + 4 * g.nu * g.nv + 12 * L + 4 * g.nu * g.noViews + 4096
+    xs = 8 * g.nx * g.ny * (g.nz + 4)  # column prefix sums (paired layout at most, or the padded plain one)
+    plan = xs + 4 * g.nu * g.nv + g.nx * g.ny + 64 * g.noViews + 4096
+    fdk = s * pix + 4 * g.nu * g.nv + 12 * L + 4 * g.nu * g.noViews + 4096  # filtered sinogram + tables
     image = 4 * vox
     if req.kind == "fdk":
         return plan + fdk + s * pix + image
-    # y, w in storage and their per-subset copies; while the solver is set up: the
-    # FP32 y and w, A(1) and the temporaries of w .* A(1); x, x_new, x_old, precom,
-    # num (FP32); the per-subset ax and wd
+    # while the solver is set up: the stored y and w (FP16 weights: FP32 until scaled) with
+    # their per-subset copies, the FDK start image, one FP32 sinogram for A(1) and (w A(1))
+    # ampv, the images x, x_new, x_old, precom, num (FP32) and the per-subset ax and wd
+    w_in = 4 if req.storage == "float16" else s
     sub = 2 * 4 * g.nu * g.nv * math.ceil(g.noViews / req.subsets)
-    return plan + fdk + 4 * s * pix + 6 * 4 * pix + 5 * image + sub + 4096
+    return plan + fdk + (s + w_in + 2 * s + 4) * pix + 6 * image + sub + 4096
 
 
 class _Active:
@@ -136,14 +140,17 @@ class _Active:
         with torch.cuda.device(device), torch.cuda.stream(stream):
             self.plan = Plan(req.geom, device, stream=stream)
             self.fdk = FDK(req.geom, req.window, 1.0, device, plan=self.plan)
-            sino = _to_device(req.sino, device)
+            # the sinogram goes to the device in its storage type (converted on the host:
+            # half the copy for BF16/FP16, and no FP32 copy on the device)
+            sino = _to_device(req.sino, device, dt)
             if req.kind == "fdk":
-                self.sino = sino.to(dt).contiguous()
+                self.sino = sino
                 self.units = 1
             else:
                 from .pwls import PwlsSolver
-                w = _to_device(req.weights, device)
-                x0 = self.fdk(sino.float().contiguous())  # reconFDK start image
+                # FP16 weights stay FP32 until the solver scales them into FP16's range
+                w = _to_device(req.weights, device, torch.float32 if dt == torch.float16 else dt)
+                x0 = self.fdk(sino)  # reconFDK start image, from the stored sinogram
                 self.solver = PwlsSolver(sino, w, req.geom, req.beta, req.pfun, req.delta, req.subsets, x0,
                                          storage=dt, plan=self.plan, autotune=autotune)
                 self.fdk.close()
@@ -247,11 +254,15 @@ class _Active:
                 self.plan.close()
 
 
-def _to_device(a, device):
+def _to_device(a, device, dtype=None):
+    """A host array or tensor on the device, contiguous, converted to ``dtype`` (on the host
+    for host data, rounding to nearest even as the device conversion does)."""
     import torch
     if isinstance(a, torch.Tensor):
-        return a.to(device, non_blocking=True)
+        return a.to(device, dtype or a.dtype, non_blocking=True).contiguous()
     t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None and t.dtype != dtype:
+        t = t.to(dtype)
     if torch.cuda.is_available():
         t = t.pin_memory()
     return t.to(device, non_blocking=True)

@@ -324,7 +324,8 @@ ctsim_status ctsim_pwls_residual_ex(const float *d_ax, const void *d_y, const vo
  * residual written already multiplied by the plan's axial amplitude table (wd = (w d) *
  * ampv per pixel, the product A^T forms first), for ctsim_plan_backproject_ex with
  * CTSIM_INPUT_SCALED; *d_phi accumulates sum(w d^2) as before (no reference counterpart:
- * it fuses the residual with the first step of the backprojection). */
+ * it fuses the residual with the first step of the backprojection).  d_y may be NULL
+ * (d = ax: the (w A1) * ampv of the SQS denominator).  d_wd may be d_ax. */
 ctsim_status ctsim_pwls_residual_scaled(const ctsim_plan *plan, const float *d_ax, const void *d_y, const void *d_w,
                                         int dtype, float w_scale, float *d_wd, int view_count, double *d_phi,
                                         void *stream);
