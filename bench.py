@@ -382,6 +382,10 @@ def run_ours(args):
                 "cpu_baseline": cpu}
         if args.extras:
             line["extras"] = extras(plan, xd, yd, sino, img, vv)
+        if world == 1 and not args.no_serving:
+            del plan, xd, yd, sino, img
+            torch.cuda.empty_cache()
+            line["serving"] = serving_leg(args.seed)
         print(json.dumps(line), flush=True)
     if dist:
         td.destroy_process_group()
@@ -418,6 +422,76 @@ def extras(plan, xd, yd, sino, img, vv):
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / 3
         out[name] = {"ms": ms, "gvv_s": vv / (ms / 1e3) / 1e9}
+    return out
+
+
+def serving_leg(seed: int, unique: int = 40, total: int = 200, budget_s: float = 60.0):
+    """The served stream at config-1 sizes (128^2 x 64, 360 views, 256 x 96): a seeded 70/30
+    FDK / OS-PWLS (10 iterations x 12 subsets) mix of `total` requests (`unique` distinct
+    phantoms, cycled), BF16 storage with FP32 arithmetic through ReconServer, against the
+    plain single-instance FP32 path (reconFDK / reconPwlsSeSqs one request at a time, host
+    arrays in and out) on the same requests.  Closed loop for req/s; Poisson arrivals at
+    50% and 80% of the served capacity for p50/p99 latency.  Every arm runs the same
+    requests after one untimed pass over the distinct ones; the leg stops short of
+    `budget_s` seconds of serving (the arms it reached are reported)."""
+    import copy
+    import torch
+    from ctsim_b200.serving import ReconServer, latency_stats, make_requests, serve_sequential
+    t_start = time.perf_counter()
+    base = make_requests(unique, seed=seed, sizes="config1", iterations=10, subsets=12)
+    reqs = []
+    for i in range(total):
+        r = copy.copy(base[i % unique])
+        r.rid = i
+        reqs.append(r)
+
+    def fresh(rs, storage, arrivals=None):
+        out = []
+        for i, r in enumerate(rs):
+            c = copy.copy(r)
+            c.storage, c.result, c.status = storage, None, "pending"
+            c.arrival = 0.0 if arrivals is None else float(arrivals[i])
+            out.append(c)
+        return out
+
+    def served(rs):
+        srv = ReconServer(max_active=8, to_host=True, admit_workers=2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        done = srv.run(rs)
+        torch.cuda.synchronize()
+        return done, time.perf_counter() - t0
+
+    serve_sequential(fresh(base, "float32"))  # warm-up: plans, pools, pinned buffers
+    served(fresh(base, "bfloat16"))
+    out = {"workload": "config-1 geometry (128^2x64 @1mm, 360 views, 256x96 @1.6mm), 70/30 FDK/OS-PWLS "
+                       "(10 x 12 subsets), seeded ellipsoid phantoms, Poisson counts I0=1e5",
+           "requests": total, "distinct": unique, "fdk": sum(r.kind == "fdk" for r in reqs),
+           "pwls": sum(r.kind == "pwls" for r in reqs), "slots": 8}
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    plain = serve_sequential(fresh(reqs, "float32"))
+    t_plain = time.perf_counter() - t0
+    done16, t16 = served(fresh(reqs, "bfloat16"))
+    cap = len(done16) / t16
+    out.update({"plain_fp32_req_per_s": len(plain) / t_plain, "served_bf16_req_per_s": cap,
+                "speedup_served_bf16_vs_plain_fp32": cap / (len(plain) / t_plain),
+                "closed_loop": latency_stats(done16, t16)})
+    rng = np.random.default_rng(seed)
+    sweep = []
+    for frac in (0.5, 0.8):
+        if time.perf_counter() - t_start > budget_s:
+            break
+        rate = frac * cap
+        arr = np.cumsum(rng.exponential(1.0 / rate, size=total))
+        d, t = served(fresh(reqs, "bfloat16", arr))
+        st = latency_stats(d, t)
+        st.update({"offered_req_per_s": rate, "load_fraction": frac})
+        sweep.append(st)
+    out["open_loop"] = sweep
+    out["clocks"] = clocks.stop()
+    out["seconds"] = time.perf_counter() - t_start
     return out
 
 
@@ -818,6 +892,8 @@ def main():
     ap.add_argument("--views", type=int, default=0, help="keep only this many views (profiling captures)")
     ap.add_argument("--consecutive", action="store_true", help="with --views: the first views, not every n-th")
     ap.add_argument("--no-e2e", dest="no_e2e", action="store_true", help="skip the end-to-end host-buffer leg")
+    ap.add_argument("--no-serving", dest="no_serving", action="store_true",
+                    help="skip the bounded served-stream leg of the default run")
     ap.add_argument("--serving", action="store_true", help="served FDK/OS-PWLS request mix instead of A/A^T")
     ap.add_argument("--requests", type=int, default=24, help="requests of the serving run")
     ap.add_argument("--slots", type=int, default=8, help="concurrent requests of the serving run")
