@@ -521,7 +521,8 @@ def run_serving(args):
         return out
 
     def served(reqs, **kw):
-        srv = ReconServer(max_active=args.slots, to_host=True, admit_workers=2, batch_pwls=args.batch_pwls, **kw)
+        srv = ReconServer(hbm_budget=int(args.budget_gb * 2 ** 30), max_active=args.slots, to_host=True,
+                          admit_workers=2, batch_pwls=args.batch_pwls, **kw)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         done = srv.run(reqs)
@@ -542,9 +543,9 @@ def run_serving(args):
     for _ in range(2):  # the better of two timed passes per arm, arms interleaved
         plain = serve_sequential(fresh(reqs, "float32"))
         t_plain = min(t_plain, max(r.t_done for r in plain))
-        d32, t, _ = served(fresh(reqs, "float32"))
+        d32, t, srv = served(fresh(reqs, "float32"))
         if t < t32:
-            done32, t32 = d32, t
+            done32, t32, srv32 = d32, t, srv
         d16, t, srv = served(fresh(reqs, "bfloat16"), autotune=args.autotune)
         if t < t16:
             done16, t16, srv16 = d16, t, srv
@@ -575,6 +576,9 @@ def run_serving(args):
         "served_fp32_req_per_s": len(done32) / t32,
         "speedup_vs_plain_fp32": cap / plain_rps,
         "closed_loop": closed, "open_loop": sweep, "peak_hbm_admitted_bytes": srv16.peak_used,
+        "hbm_budget_bytes": int(args.budget_gb * 2 ** 30),
+        "concurrency": {"bf16_mean": srv16.mean_active, "bf16_peak": srv16.peak_active,
+                        "fp32_mean": srv32.mean_active, "fp32_peak": srv32.peak_active},
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -897,6 +901,8 @@ def main():
     ap.add_argument("--serving", action="store_true", help="served FDK/OS-PWLS request mix instead of A/A^T")
     ap.add_argument("--requests", type=int, default=24, help="requests of the serving run")
     ap.add_argument("--slots", type=int, default=8, help="concurrent requests of the serving run")
+    ap.add_argument("--budget-gb", dest="budget_gb", type=float, default=150.0,
+                    help="serving: HBM admission budget in GiB")
     ap.add_argument("--scale", type=float, default=1.0, help="size scale of the serving run's geometries")
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--autotune", action="store_true", help="serving/batched: autotune launch shapes")

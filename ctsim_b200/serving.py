@@ -289,6 +289,9 @@ class ReconServer:
             self._pool = ThreadPoolExecutor(admit_workers, thread_name_prefix="ctsim-admit")
         self.used = 0
         self.peak_used = 0
+        self.peak_active = 0       # the most requests set up or active at once
+        self._active_sum = 0       # sum over ticks of the requests set up or active (mean concurrency)
+        self._ticks = 0
         self.done = []
         self.failed = []      # requests that failed or were cancelled, in the order they ended
         self._cancel = set()  # rids to withdraw when their set-up finishes
@@ -431,10 +434,19 @@ class ReconServer:
                 self.done.append(a.req)
         self.active = keep
 
+    @property
+    def mean_active(self) -> float:
+        """Requests set up or active per scheduler tick, on average."""
+        return self._active_sum / self._ticks if self._ticks else 0.0
+
     def tick(self):
         self._admit()
         if self.starting:
             self._collect_started()
+        n = len(self.active) + len(self.starting)
+        self.peak_active = max(self.peak_active, n)
+        self._active_sum += n
+        self._ticks += 1
         for a in self.active:
             if getattr(a, "cancelled", False) or getattr(a, "failed", None) is not None:
                 continue
