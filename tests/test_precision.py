@@ -67,3 +67,29 @@ def test_pwls_storage_precision():
         assert errs[-1] <= 0.01, (name, errs)
         if name == "float32":
             assert errs[-1] <= 1e-4
+
+
+def test_fdk_storage_precision():
+    """reconFDK from a sinogram stored in FP32 / BF16 / FP16 (FP32 filter arithmetic; the
+    filtered sinogram kept in the input's storage type and backprojected as it is)
+    against FDK in FP64 (the filter in float64 and the double restatement of back,hpd)."""
+    import torch
+    from ctsim_b200.fdk import FDK
+    from oracle import fdk_oracle
+    g, x_mm = config1(n_views=120)
+    x = to_projector_units(x_mm)
+    rng = np.random.default_rng(13)
+    p = oracle_cbct("proj,dd", g, x)
+    counts = rng.poisson(1e5 * np.exp(-p)).astype(np.float32)
+    y = np.log(1e5 / np.maximum(counts, 10)).astype(np.float32)
+    filt = fdk_oracle.filtered_sinogram(y, g, "hann")
+    betas = np.asarray(g.betas, np.float64)
+    dbeta = abs(betas[-1] - betas[0]) / (betas.size - 1) / 2
+    img64 = oracle_cbct("back,hpd", g, filt, fp64=True) * dbeta * 10
+    f = FDK(g, "hann")
+    print("\nstorage   | FDK image rel L2 | max abs   (vs FDK in FP64)")
+    for name, dt in (("float32", torch.float32), ("bfloat16", torch.bfloat16), ("float16", torch.float16)):
+        img = f(torch.from_numpy(y).cuda().to(dt)).cpu().numpy()
+        e, m = _err(img, img64)
+        print(f"{name:9s} | {e:.3e}        | {m:.3e}")
+        assert e <= BOUNDS[name], (name, e)
