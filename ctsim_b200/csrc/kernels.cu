@@ -83,6 +83,13 @@ __device__ __forceinline__ float4 load_rows4(const void *__restrict__ src, const
 // ---------------------------------------------------------------------------
 // The work of one block (8 columns of one row iy), as a device function: the plain
 // kernel runs it for blockIdx.x, the batched kernel for each of its work items.
+// 32-bit shared load ordered after the warp's earlier shared stores (compiler barrier).
+__device__ __forceinline__ float lds_ordered(uint32_t a) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a) : "memory");
+    return v;
+}
+
 template <int METHOD, int MZ, bool VEC, int SRC, bool SUM = false>
 __device__ __forceinline__ void back_block(const Geom g, const View *__restrict__ views, const void *__restrict__ ps,
                                            const uint8_t *__restrict__ map, void *__restrict__ image, int out_dtype,
@@ -180,6 +187,9 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                     // (geom/cbct/cbct_back.c:318-357); rows [k_lo, k_hi] lie in [r_lo, r_hi]
                     // because the edges are monotone in iz.
                     const float *qb = Q - rbase;
+                    // shared address of row k is qadj + 4 * bits(k + 2^23) (mod 2^32)
+                    const uint32_t qadj = (uint32_t)__cvta_generic_to_shared(Q) - 4u * (uint32_t)rbase -
+                                          (0x4B000000u << 2);
                     // vmax - vmin is zinc within 1.5 float ulps of nv (< 2^-10 for nv <= 8192), so
                     // away from zinc = 1 and 2 by a margin every voxel of the view covers the same
                     // number of rows give or take one: n = k_hi - k_lo is 0 or 1 (zinc < 1) or 1 or
@@ -197,8 +207,8 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                             const float vmin = fadd(vpre, 0.5f);
                             const float vmax = fadd(fadd(vpre, zinc), 0.5f);
                             const float tlo = __fadd_rd(vmin, kTwo23), thi = __fadd_rd(vmax, kTwo23);
-                            const float *qk = qb + (__float_as_int(tlo) - 0x4B000000);
-                            const float q0 = qk[0], q1 = qk[1];
+                            const uint32_t qa = qadj + (__float_as_uint(tlo) << 2);
+                            const float q0 = lds_ordered(qa), q1 = lds_ordered(qa + 4u);
                             // one row: (vmax - vmin) q0; two: (k_lo + 1 - vmin) q0 + (vmax - k_hi) q1
                             const float one = fsub(vmax, vmin) * q0;
                             const float two = fmaf(fsub(vmax, fsub(thi, kTwo23)), q1,
@@ -213,8 +223,8 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                             const float vmin = fadd(vpre, 0.5f);
                             const float vmax = fadd(fadd(vpre, zinc), 0.5f);
                             const float tlo = __fadd_rd(vmin, kTwo23), thi = __fadd_rd(vmax, kTwo23);
-                            const float *qk = qb + (__float_as_int(tlo) - 0x4B000000);
-                            const float q0 = qk[0], q1 = qk[1], q2 = qk[2];
+                            const uint32_t qa = qadj + (__float_as_uint(tlo) << 2);
+                            const float q0 = lds_ordered(qa), q1 = lds_ordered(qa + 4u), q2 = lds_ordered(qa + 8u);
                             const bool three = fsub(thi, tlo) == 2.0f;
                             const float wl = fsub(vmax, fsub(thi, kTwo23));
                             // two rows: w0 q0 + wl q1; three: w0 q0 + q1 + wl q2 (the reference's row order)
@@ -644,6 +654,10 @@ __device__ __forceinline__ void mbar_arrive_expect(uint64_t *bar, unsigned bytes
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
                  : "memory");
 }
+// One plain arrival (release: the arriving thread's earlier shared-memory reads are done).
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 // Global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16), its
 // bytes counted on `bar`.  No multicast: the destination is this block's own memory.
 __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
@@ -702,7 +716,7 @@ __device__ __forceinline__ void acc_add4(uint32_t a, float w, float r0, float r1
                  : "memory");
 }
 
-// Dynamic shared-memory layout of the staged forward projector: two mbarriers (first, so
+// Dynamic shared-memory layout of the staged forward projector: four mbarriers (first, so
 // that a persistent block keeps them across work items of different shapes), the
 // accumulators, the two stage buffers, the candidate table and its packed index, the
 // line tables.
@@ -711,13 +725,32 @@ struct StagedSmem {
     __host__ __device__ size_t acc_bytes() const { return (size_t)groups * kTU * nq * 16; }
     __host__ __device__ size_t stage_floats() const { return (size_t)slots * xstride; }  // one buffer
     __host__ __device__ size_t bytes() const {
-        return 16 + acc_bytes() + 2 * stage_floats() * 4 + (size_t)nt * (6 + kTU) * 4 +
+        return 32 + acc_bytes() + 2 * stage_floats() * 4 + (size_t)nt * (6 + kTU) * 4 +
                (size_t)(2 * nlines + 1 + 32) * 4;
     }
 };
 
 // Error flag bit of a stage wait that ran out (ctsim_plan_check reports the flag).
 constexpr int kErrStageWait = 4;
+
+// The stage buffers form a two-deep full/empty pipeline: bar[b] ("full", one arrival plus
+// the copies' bytes) completes when buffer b holds its slots, bar[2 + b] ("empty", one
+// arrival per warp) when every warp has finished reading it.  A thread's `phase` holds the
+// parity of the next completion it waits for: bit b for full[b], bit 2 + b for empty[b].
+// The empty bits start at 1, the parity of the phase before a fresh barrier's first,
+// which counts as complete, so the first copies into each buffer do not wait.
+constexpr unsigned kStagedPhase0 = 0xCu;
+
+__device__ __forceinline__ void staged_bars_init(uint64_t *bar) {
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init(&bar[2], blockDim.x >> 5);
+        mbar_init(&bar[3], blockDim.x >> 5);
+        mbar_init_fence();
+    }
+    __syncthreads();
+}
 
 // Candidate intervals of the lines for detector columns [iu0, iu0 + kTU) of view v:
 // line_start[L], and line_off[L] the exclusive scan of the counts (line_off[nlines] =
@@ -791,11 +824,11 @@ __device__ __forceinline__ int candidate_lines(const Geom &g, const View &v, int
     return line_off[nlines];
 }
 
-// The work of one block.  bar: the block's two stage mbarriers (initialised once per
-// block); phase: their next-completion parities (bit b for buffer b), carried across
-// the items of a persistent block; acc4: the shared memory past the mbarriers.  Returns
-// false when a stage wait ran out (the block has then set kErrStageWait, waited for its
-// copies in flight and must stop).
+// The work of one block.  bar: the block's four stage mbarriers (initialised once per
+// block by staged_bars_init); phase: their next-completion parities, carried across the
+// items of a persistent block (kStagedPhase0 at the start); acc4: the shared memory past
+// the mbarriers.  Returns false when a stage wait ran out (the block has then set
+// kErrStageWait, waited for its copies in flight and must stop).
 template <int METHOD, int GROUPS>
 __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__restrict__ views,
                                                   const float *__restrict__ xs, const float *__restrict__ ampv,
@@ -922,12 +955,20 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
         __syncthreads();
 
         // 2. the packed candidates, `slots` at a time: warp 0 issues the copies of the next
-        // slots into the other buffer while every warp runs the rows of the current ones
+        // slots into the other buffer once every warp has released it, while the warps run
+        // the rows of the current ones; each warp releases a buffer when it is done with it
         const int nsub = (nval + slots - 1) / slots;
+        bool failed = false;
         auto issue = [&](int sub, int buf) {
             const int p0 = sub * slots, n = min(slots, nval - p0);
-            if (lane == 0) mbar_arrive_expect(&bar[buf], (unsigned)n * col_bytes);
+            const bool free = mbar_wait(&bar[2 + buf], (phase >> (2 + buf)) & 1u);
+            phase ^= 4u << buf;
+            failed |= !free;
+            // a buffer that was not released gets no copies: its full phase completes empty
+            // and the block stops at the end of the chunk
+            if (lane == 0) mbar_arrive_expect(&bar[buf], free ? (unsigned)n * col_bytes : 0u);
             __syncwarp();
+            if (!free) return;
             float *dst = stage + (size_t)buf * L.stage_floats();
             for (int i = lane; i < n; i += 32)
                 bulk_copy_g2s(dst + (size_t)i * xst, xs + (size_t)c_col[c_idx[p0 + i]] * xst, col_bytes, &bar[buf]);
@@ -936,7 +977,7 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
         for (int sub = 0; sub < nsub; sub++) {
             const int buf = (buf0 + sub) & 1;
             if (sub + 1 < nsub && warp == 0) issue(sub + 1, buf ^ 1);
-            const bool ok = mbar_wait(&bar[buf], (phase >> buf) & 1u);
+            failed |= !mbar_wait(&bar[buf], (phase >> buf) & 1u);
             phase ^= 1u << buf;
             const uint32_t sb = smem_addr(stage + (size_t)buf * L.stage_floats()) - (0x4B000000u << 2);
             const int p0 = sub * slots, p1 = min(nval, p0 + slots);
@@ -976,14 +1017,19 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
                     }
                 }
             }
-            // every warp is done with buffer `buf` before the copies of slots sub + 2 reuse it
-            if (__syncthreads_or(!ok)) {
-                if (t == 0) atomicOr(err, kErrStageWait);
-                // let the copies in flight land before the block stops (bounded waits)
-                mbar_wait(&bar[buf], ((phase >> buf) & 1u) ^ 1u);
-                if (sub + 1 < nsub) mbar_wait(&bar[buf ^ 1], (phase >> (buf ^ 1)) & 1u);
-                return false;
-            }
+            // this warp is done with buffer `buf`
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar[2 + buf]);
+        }
+        // every warp is done with this chunk's candidate tables before the next chunk
+        // rewrites them
+        if (__syncthreads_or(failed)) {
+            if (t == 0) atomicOr(err, kErrStageWait);
+            // let copies still in flight land before the block stops (bounded waits: a
+            // phase that completed, or never began, returns at once)
+            mbar_wait(&bar[0], (phase & 1u) ^ 1u);
+            mbar_wait(&bar[1], ((phase >> 1) & 1u) ^ 1u);
+            return false;
         }
         buf0 = (buf0 + nsub) & 1;
         vbase += nval;
@@ -1016,15 +1062,10 @@ __global__ void __launch_bounds__(kProjMaxThreads, 3) proj_staged_kernel(Geom g,
                                                                       int slots, int *__restrict__ err, int vgroup) {
     extern __shared__ float4 smem_staged[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_staged);
-    if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        mbar_init_fence();
-    }
-    __syncthreads();
-    unsigned phase = 0;
+    staged_bars_init(bar);
+    unsigned phase = kStagedPhase0;
     proj_staged_block<METHOD, GROUPS>(g, views, xs, ampv, map, proj, out_dtype, view_begin, view_stride, margin,
-                                      slots, err, smem_staged + 1, bar, phase, blockIdx.x / vgroup,
+                                      slots, err, smem_staged + 2, bar, phase, blockIdx.x / vgroup,
                                       blockIdx.y * vgroup + blockIdx.x % vgroup);
 }
 
@@ -1449,13 +1490,8 @@ __global__ void __launch_bounds__(kProjMaxThreads, 3) proj_staged_batch_kernel(c
                                                                                int slots) {
     extern __shared__ float4 smem_staged_batch[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_staged_batch);
-    if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        mbar_init_fence();
-    }
-    __syncthreads();
-    unsigned phase = 0;
+    staged_bars_init(bar);
+    unsigned phase = kStagedPhase0;
     for (int blk = blockIdx.x; blk < b.total; blk += gridDim.x) {
         int lo = 0, hi = b.n - 1;
         while (lo < hi) {
@@ -1465,7 +1501,7 @@ __global__ void __launch_bounds__(kProjMaxThreads, 3) proj_staged_batch_kernel(c
         const ProjTask &T = b.t[lo];
         const int local = blk - T.first;
         if (!proj_staged_block<METHOD, GROUPS>(T.g, T.views, T.xs, T.ampv, T.map, T.proj, LOWP ? T.out_dtype : kF32,
-                                               T.vb, T.vs, T.margin, slots, T.err, smem_staged_batch + 1, bar, phase,
+                                               T.vb, T.vs, T.margin, slots, T.err, smem_staged_batch + 2, bar, phase,
                                                local % T.gx, local / T.gx))
             return;
         __syncthreads();  // the next item reuses the shared accumulators and tables
