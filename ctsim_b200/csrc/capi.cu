@@ -1174,6 +1174,7 @@ extern "C" ctsim_status ctsim_batch_project(int method, const ctsim_batch_item *
                 T.out_dtype = it.out_dtype;
                 T.vb = it.view_begin;
                 T.vs = it.view_stride;
+                T.vc = it.view_count;
                 T.gx = (p->g.nu + proj_group_width() - 1) / proj_group_width();
                 T.first = b.total;
                 T.margin = p->margin;

@@ -611,6 +611,21 @@ __device__ __forceinline__ void proj_block(const Geom g, const View *__restrict_
     }
 }
 
+// Views per group of the forward projector's launch order.
+constexpr int kViewGroup = 32;
+
+// Detector-column group bx and launch view by of the forward projector's linear block
+// L: the launch views in groups of kViewGroup consecutive ones (the last group may be
+// shorter), and within a group the blocks of one detector-column group over all its
+// views, then the next column group -- neighbouring views share candidate columns in L2.
+__device__ __forceinline__ void view_grouped_block(int L, int ngx, int vc, int &bx, int &by) {
+    const int per = ngx * kViewGroup;
+    const int G = L / per, r = L - G * per;
+    const int n = min(kViewGroup, vc - G * kViewGroup);  // views of this group
+    bx = r / n;
+    by = G * kViewGroup + (r - bx * n);
+}
+
 template <int METHOD, int GROUPS, bool PAIRS>
 __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const View *__restrict__ views,
                                                                const float *__restrict__ xs,
@@ -618,12 +633,12 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_kernel(Geom g, const Vie
                                                                const uint8_t *__restrict__ map,
                                                                void *__restrict__ proj, int out_dtype,
                                                                int view_begin, int view_stride, float margin,
-                                                               int vgroup) {
+                                                               int ngx, int vc) {
     extern __shared__ float4 acc4_smem[];
-    // blocks in launch order: the vgroup views of a view group for one detector-column
-    // group, then the next column group (neighbouring views share candidate columns in L2)
+    int bx, by;
+    view_grouped_block(blockIdx.x, ngx, vc, bx, by);
     proj_block<METHOD, GROUPS, PAIRS>(g, views, xs, ampv, map, proj, out_dtype, view_begin, view_stride, margin,
-                                      acc4_smem, blockIdx.x / vgroup, blockIdx.y * vgroup + blockIdx.x % vgroup);
+                                      acc4_smem, bx, by);
 }
 
 // ---------------------------------------------------------------------------
@@ -1059,14 +1074,16 @@ __global__ void __launch_bounds__(kProjMaxThreads, 3) proj_staged_kernel(Geom g,
                                                                       const uint8_t *__restrict__ map,
                                                                       void *__restrict__ proj, int out_dtype,
                                                                       int view_begin, int view_stride, float margin,
-                                                                      int slots, int *__restrict__ err, int vgroup) {
+                                                                      int slots, int *__restrict__ err, int ngx,
+                                                                      int vc) {
     extern __shared__ float4 smem_staged[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem_staged);
     staged_bars_init(bar);
     unsigned phase = kStagedPhase0;
+    int bx, by;
+    view_grouped_block(blockIdx.x, ngx, vc, bx, by);
     proj_staged_block<METHOD, GROUPS>(g, views, xs, ampv, map, proj, out_dtype, view_begin, view_stride, margin,
-                                      slots, err, smem_staged + 2, bar, phase, blockIdx.x / vgroup,
-                                      blockIdx.y * vgroup + blockIdx.x % vgroup);
+                                      slots, err, smem_staged + 2, bar, phase, bx, by);
 }
 
 // ---------------------------------------------------------------------------
@@ -1320,13 +1337,6 @@ size_t proj_smem_bytes(int nv, int nx, int ny, int groups) {
 int proj_group_width() { return kTU; }
 int proj_max_lines() { return kMaxLines; }
 
-// Views per group of the forward projector's launch order: the largest of 8 .. 1 that
-// divides the view count (every group full).
-int proj_view_group(int vc) {
-    for (int v = 8; v > 1; v--)
-        if (vc % v == 0) return v;
-    return 1;
-}
 
 size_t proj_staged_smem_bytes(int nv, int nx, int ny, int xstride, int groups, int rows, int slots) {
     StagedSmem L{(nv + 3) / 4, rows * groups, std::max(nx, ny), groups, slots, xstride};
@@ -1345,15 +1355,15 @@ cudaError_t launch_proj_staged(int method, int groups, int rows, int slots, cons
         g.xstride % 4 != 0 || g.xstride < g.nz + 2 || reinterpret_cast<uintptr_t>(xs) % 16 != 0)
         return cudaErrorInvalidValue;
     const size_t sm = proj_staged_smem_bytes(g.nv, g.nx, g.ny, g.xstride, groups, rows, slots);
-    const int vg = proj_view_group(vc);
-    dim3 grid((g.nu + kTU - 1) / kTU * vg, vc / vg);
+    const int ngx = (g.nu + kTU - 1) / kTU;
+    const int nblocks = ngx * vc;
     const int nt = rows * groups;
 #define CTSIM_PROJ_STAGED_CASE(M, GR)                                                                 \
     if (method == M && groups == GR) {                                                                \
         cudaError_t e = allow_dynamic_smem((const void *)proj_staged_kernel<M, GR>, sm);              \
         if (e != cudaSuccess) return e;                                                               \
-        proj_staged_kernel<M, GR><<<grid, nt, sm, st>>>(g, views, xs, ampv, map, proj, out_dtype, vb, vs, margin, \
-                                                        slots, err, vg);                              \
+        proj_staged_kernel<M, GR><<<nblocks, nt, sm, st>>>(g, views, xs, ampv, map, proj, out_dtype, vb, vs,    \
+                                                           margin, slots, err, ngx, vc);              \
         return cudaGetLastError();                                                                    \
     }
     CTSIM_PROJ_STAGED_CASE(kDD, 1) CTSIM_PROJ_STAGED_CASE(kDD, 2) CTSIM_PROJ_STAGED_CASE(kDD, 4)
@@ -1368,8 +1378,8 @@ cudaError_t launch_proj(int method, int groups, int rows, bool pairs, const Geom
                         int vs, int vc, float margin, cudaStream_t st) {
     if (!proj_shape_valid(g.nv, groups, rows)) return cudaErrorInvalidValue;
     const size_t sm = proj_smem_bytes(g.nv, g.nx, g.ny, groups, rows);
-    const int vg = proj_view_group(vc);
-    dim3 grid((g.nu + kTU - 1) / kTU * vg, vc / vg);
+    const int ngx = (g.nu + kTU - 1) / kTU;
+    const int nblocks = ngx * vc;
     // one thread per 4 detector rows (rows threads per group, more rows loop), groups
     // of those threads share the candidates
     const int nt = rows * groups;
@@ -1377,7 +1387,8 @@ cudaError_t launch_proj(int method, int groups, int rows, bool pairs, const Geom
     if (method == M && groups == GR && pairs == P) {                                                  \
         cudaError_t e = allow_dynamic_smem((const void *)proj_kernel<M, GR, P>, sm);                  \
         if (e != cudaSuccess) return e;                                                               \
-        proj_kernel<M, GR, P><<<grid, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin, vg); \
+        proj_kernel<M, GR, P><<<nblocks, nt, sm, st>>>(g, views, xc, ampv, map, proj, out_dtype, vb, vs, margin, \
+                                                       ngx, vc);                                      \
         return cudaGetLastError();                                                                    \
     }
     CTSIM_PROJ_CASE(kDD, 1, false) CTSIM_PROJ_CASE(kDD, 2, false) CTSIM_PROJ_CASE(kDD, 4, false)
@@ -1474,10 +1485,10 @@ __global__ void __launch_bounds__(kProjMaxThreads) proj_batch_kernel(const __gri
             if (b.t[mid].first <= blk) lo = mid; else hi = mid - 1;
         }
         const ProjTask &T = b.t[lo];
-        const int local = blk - T.first;
+        int bx, by;
+        view_grouped_block(blk - T.first, T.gx, T.vc, bx, by);
         proj_block<METHOD, GROUPS, PAIRS>(T.g, T.views, T.xs, T.ampv, T.map, T.proj, LOWP ? T.out_dtype : kF32, T.vb,
-                                          T.vs, T.margin,
-                                          acc4_batch, local % T.gx, local / T.gx);
+                                          T.vs, T.margin, acc4_batch, bx, by);
         __syncthreads();  // the next block reuses the shared accumulators
     }
 }
@@ -1499,10 +1510,11 @@ __global__ void __launch_bounds__(kProjMaxThreads, 3) proj_staged_batch_kernel(c
             if (b.t[mid].first <= blk) lo = mid; else hi = mid - 1;
         }
         const ProjTask &T = b.t[lo];
-        const int local = blk - T.first;
+        int bx, by;
+        view_grouped_block(blk - T.first, T.gx, T.vc, bx, by);
         if (!proj_staged_block<METHOD, GROUPS>(T.g, T.views, T.xs, T.ampv, T.map, T.proj, LOWP ? T.out_dtype : kF32,
                                                T.vb, T.vs, T.margin, slots, T.err, smem_staged_batch + 2, bar, phase,
-                                               local % T.gx, local / T.gx))
+                                               bx, by))
             return;
         __syncthreads();  // the next item reuses the shared accumulators and tables
     }

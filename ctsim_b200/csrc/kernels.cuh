@@ -76,7 +76,7 @@ struct ProjTask {
     const uint8_t *map;
     void *proj;
     int out_dtype;
-    int vb, vs, gx, first;  // view selection, blocks along u, first flat block of the task
+    int vb, vs, vc, gx, first;  // view selection, blocks along u, first flat block of the task
     float margin;
     int *err;               // the plan's error flag (staged projector: a stage wait that ran out)
 };
