@@ -425,6 +425,21 @@ def extras(plan, xd, yd, sino, img, vv):
     return out
 
 
+def served_accuracy(served, plain):
+    """Relative RMSE (||a - b|| / ||b||) of each served BF16-storage image against the plain
+    FP32 path's image of the same request, per request kind (max and median).  The FP32
+    path itself is within 2e-6 of the FP64 oracle on these shapes (tests/test_precision.py)."""
+    ref = {r.rid: r for r in plain}
+    errs = {"fdk": [], "pwls": []}
+    for r in served:
+        a = r.result
+        a = a.float().numpy() if hasattr(a, "float") else np.asarray(a, np.float32)
+        b = np.asarray(ref[r.rid].result, np.float64)
+        errs[r.kind].append(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)))
+    return {"against": "plain FP32 path, same requests", "metric": "relative RMSE",
+            **{k: {"max": max(v), "median": float(np.median(v)), "n": len(v)} for k, v in errs.items() if v}}
+
+
 def serving_leg(seed: int, unique: int = 40, total: int = 200, budget_s: float = 60.0):
     """The served stream at config-1 sizes (128^2 x 64, 360 views, 256 x 96): a seeded 70/30
     FDK / OS-PWLS (10 iterations x 12 subsets) mix of `total` requests (`unique` distinct
@@ -477,7 +492,8 @@ def serving_leg(seed: int, unique: int = 40, total: int = 200, budget_s: float =
     cap = len(done16) / t16
     out.update({"plain_fp32_req_per_s": len(plain) / t_plain, "served_bf16_req_per_s": cap,
                 "speedup_served_bf16_vs_plain_fp32": cap / (len(plain) / t_plain),
-                "closed_loop": latency_stats(done16, t16)})
+                "closed_loop": latency_stats(done16, t16),
+                "accuracy": served_accuracy(done16, plain)})
     rng = np.random.default_rng(seed)
     sweep = []
     for frac in (0.5, 0.8):
