@@ -3,12 +3,15 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ctsim_b200.h"
@@ -602,6 +605,103 @@ namespace {
 // in view chunks that overlap the kernels (forward results out, backprojection inputs in).
 // ---------------------------------------------------------------------------
 namespace {
+// Parts of a host-side job run on a small pool of threads plus the caller (the
+// pageable-memory staging below: one thread's memcpy moves about 15 GB/s, eight about 50,
+// while pageable cudaMemcpy moves 11 GB/s host to device on B200 hosts).  The pool is
+// created on first use and never destroyed; its threads stay parked on a condition
+// variable, so process exit does not wait for them.
+class HostPool {
+  public:
+    static HostPool &get() {
+        static HostPool *pool = new HostPool();
+        return *pool;
+    }
+    int width() const { return workers_ + 1; }
+    // fn(0) .. fn(n - 1), on the pool and the calling thread; returns when all are done.
+    void run(int n, const std::function<void(int)> &fn) {
+        std::lock_guard<std::mutex> one_job(job_m_);
+        if (n <= 1 || workers_ == 0) {
+            for (int i = 0; i < n; i++) fn(i);
+            return;
+        }
+        auto job = std::make_shared<Job>();
+        job->fn = &fn;
+        job->n = n;
+        job->left.store(n);
+        {
+            std::lock_guard<std::mutex> l(m_);
+            job_ = job;
+            gen_++;
+        }
+        cv_.notify_all();
+        work(*job);
+        std::unique_lock<std::mutex> l(job->m);
+        job->cv.wait(l, [&] { return job->left.load() == 0; });
+    }
+    // memcpy in parts of at least 4 MB, one per pool thread at most.
+    void copy(void *dst, const void *src, size_t n) {
+        const int parts = (int)std::min<size_t>((size_t)width(), std::max<size_t>(1, n >> 22));
+        const size_t per = ((n + parts - 1) / parts + 63) & ~(size_t)63;
+        run(parts, [&](int i) {
+            const size_t o = (size_t)i * per;
+            if (o < n) std::memcpy(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o, std::min(per, n - o));
+        });
+    }
+
+  private:
+    struct Job {
+        const std::function<void(int)> *fn = nullptr;
+        int n = 0;
+        std::atomic<int> next{0}, left{0};
+        std::mutex m;
+        std::condition_variable cv;
+    };
+    HostPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        workers_ = (int)std::min(7u, hw > 2 ? hw / 2 - 1 : 0u);
+        for (int i = 0; i < workers_; i++) std::thread([this] { loop(); }).detach();
+    }
+    // A worker that wakes after its job ended finds the job's parts taken and leaves it.
+    static void work(Job &j) {
+        for (int i; (i = j.next.fetch_add(1)) < j.n;) {
+            (*j.fn)(i);
+            if (j.left.fetch_sub(1) == 1) {
+                std::lock_guard<std::mutex> l(j.m);
+                j.cv.notify_all();
+            }
+        }
+    }
+    void loop() {
+        unsigned long long seen = 0;
+        for (;;) {
+            std::shared_ptr<Job> job;
+            {
+                std::unique_lock<std::mutex> l(m_);
+                cv_.wait(l, [&] { return gen_ != seen; });
+                seen = gen_;
+                job = job_;
+            }
+            work(*job);
+        }
+    }
+    int workers_ = 0;
+    std::mutex job_m_, m_;
+    std::condition_variable cv_;
+    std::shared_ptr<Job> job_;
+    unsigned long long gen_ = 0;
+};
+
+// True for page-locked (registered or cudaHostAlloc'd) host memory and device memory;
+// false for ordinary pageable memory.
+bool dma_ready(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
 struct HostCache {
     std::mutex m;
     int device = -1;
@@ -616,6 +716,74 @@ struct HostCache {
     static constexpr int kSlabs = 4;   // y slabs of the last backprojection chunk
     cudaEvent_t done[kChunks + kSlabs] = {};
     cudaEvent_t ready = nullptr;
+    // pinned staging for pageable caller buffers: kStage buffers of kStageBytes, each with
+    // the event of the last copy that used it (allocated on the first pageable call)
+    static constexpr int kStage = 4;
+    static constexpr size_t kStageBytes = (size_t)32 << 20;
+    void *stage[kStage] = {};
+    cudaEvent_t stage_ev[kStage] = {};
+
+    cudaError_t ensure_stage() {
+        if (stage[0]) return cudaSuccess;
+        cudaError_t e = cudaSuccess;
+        for (int b = 0; b < kStage && e == cudaSuccess; b++)
+            if ((e = cudaHostAlloc(&stage[b], kStageBytes, cudaHostAllocDefault)) == cudaSuccess)
+                e = cudaEventCreateWithFlags(&stage_ev[b], cudaEventDisableTiming);
+        if (e != cudaSuccess) release_stage();
+        return e;
+    }
+    void release_stage() {
+        for (int b = 0; b < kStage; b++) {
+            if (stage_ev[b]) cudaEventSynchronize(stage_ev[b]);
+            if (stage[b]) cudaFreeHost(stage[b]);
+            if (stage_ev[b]) cudaEventDestroy(stage_ev[b]);
+            stage[b] = nullptr;
+            stage_ev[b] = nullptr;
+        }
+    }
+    // Host to device from pageable src through the staging buffers, in order on stream s:
+    // the pool fills one buffer while the copy engine drains the previous one.  Returns
+    // once the last piece is queued (src may then be reused).
+    cudaError_t staged_h2d(void *dst, const void *src, size_t n, cudaStream_t s) {
+        cudaError_t e;
+        for (size_t off = 0, i = 0; off < n; off += kStageBytes, i++) {
+            const int b = (int)(i % kStage);
+            const size_t len = std::min(kStageBytes, n - off);
+            if ((e = cudaEventSynchronize(stage_ev[b])) != cudaSuccess) return e;  // its last copy is done
+            HostPool::get().copy(stage[b], static_cast<const char *>(src) + off, len);
+            if ((e = cudaMemcpyAsync(static_cast<char *>(dst) + off, stage[b], len, cudaMemcpyHostToDevice, s)) !=
+                    cudaSuccess ||
+                (e = cudaEventRecord(stage_ev[b], s)) != cudaSuccess)
+                return e;
+        }
+        return cudaSuccess;
+    }
+    // Device to pageable host after the work queued on stream s: up to kStage pieces in
+    // flight, each copied out by the pool as it lands.  Returns when dst holds the data.
+    cudaError_t staged_d2h(void *dst, const void *src, size_t n, cudaStream_t s) {
+        const size_t np = (n + kStageBytes - 1) / kStageBytes;
+        cudaError_t e;
+        auto issue = [&](size_t i) {
+            const int b = (int)(i % kStage);
+            const size_t off = i * kStageBytes, len = std::min(kStageBytes, n - off);
+            cudaError_t r;
+            if ((r = cudaStreamWaitEvent(s, stage_ev[b], 0)) != cudaSuccess ||
+                (r = cudaMemcpyAsync(stage[b], static_cast<const char *>(src) + off, len, cudaMemcpyDeviceToHost, s)) !=
+                    cudaSuccess)
+                return r;
+            return cudaEventRecord(stage_ev[b], s);
+        };
+        for (size_t i = 0; i < std::min<size_t>(kStage, np); i++)
+            if ((e = issue(i)) != cudaSuccess) return e;
+        for (size_t i = 0; i < np; i++) {
+            const int b = (int)(i % kStage);
+            const size_t off = i * kStageBytes, len = std::min(kStageBytes, n - off);
+            if ((e = cudaEventSynchronize(stage_ev[b])) != cudaSuccess) return e;
+            HostPool::get().copy(static_cast<char *>(dst) + off, stage[b], len);
+            if (i + kStage < np && (e = issue(i + kStage)) != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
 
     void release() {
         int cur = -1;
@@ -631,6 +799,7 @@ struct HostCache {
         }
         if (ready) cudaEventDestroy(ready);
         ready = nullptr;
+        release_stage();
         for (cudaStream_t s : {st, st2, copy})
             if (s) cudaStreamDestroy(s);
         st = st2 = copy = nullptr;
@@ -726,6 +895,16 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
     ctsim_plan *p = h.plan;
     const bool fwd = method == CTSIM_PROJ_DD || method == CTSIM_PROJ_TF;
     const size_t nimg = (size_t)G.nx * G.ny * G.nz, nuv = (size_t)G.nu * G.nv, nsino = nuv * G.noviews;
+    // pageable caller buffers go through the pinned staging buffers (if they can be had;
+    // otherwise the driver stages them)
+    bool stage_in = !dma_ready(in), stage_out = !dma_ready(out);
+    if ((stage_in || stage_out) && h.ensure_stage() != cudaSuccess) {
+        cudaGetLastError();
+        stage_in = stage_out = false;
+    }
+    auto h2d = [&](void *dst, const void *src, size_t n, cudaStream_t st) {
+        return stage_in ? h.staged_h2d(dst, src, n, st) : cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, st);
+    };
     bool ok = false;
     do {
         if (fwd) {
@@ -734,7 +913,7 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
             // copied back on the copy stream while later chunks compute (the views are
             // independent).  All chunks are queued before the first copy: a copy to pageable
             // memory returns only when it has finished.
-            if ((e = cudaMemcpyAsync(h.dimg, in, nimg * sizeof(float), cudaMemcpyHostToDevice, h.st)) != cudaSuccess) {
+            if ((e = h2d(h.dimg, in, nimg * sizeof(float), h.st)) != cudaSuccess) {
                 cuda_fail(e, "host to device copy");
                 break;
             }
@@ -753,10 +932,12 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
             }
             for (int c = 0; c < nch && s == CTSIM_OK; c++) {
                 const int vb = first_view(c), ve = first_view(c + 1);
+                float *hdst = out + (size_t)vb * nuv;
+                const float *dsrc = static_cast<float *>(h.dsino) + (size_t)vb * nuv;
+                const size_t bytes = (size_t)(ve - vb) * nuv * sizeof(float);
                 if ((e = cudaStreamWaitEvent(h.copy, h.done[c], 0)) != cudaSuccess ||
-                    (e = cudaMemcpyAsync(out + (size_t)vb * nuv, static_cast<float *>(h.dsino) + (size_t)vb * nuv,
-                                         (size_t)(ve - vb) * nuv * sizeof(float), cudaMemcpyDeviceToHost, h.copy)) !=
-                        cudaSuccess)
+                    (e = stage_out ? h.staged_d2h(hdst, dsrc, bytes, h.copy)
+                                   : cudaMemcpyAsync(hdst, dsrc, bytes, cudaMemcpyDeviceToHost, h.copy)) != cudaSuccess)
                     s = cuda_fail(e, "device to host copy");
             }
             const cudaError_t e1 = cudaStreamSynchronize(h.st), e2 = cudaStreamSynchronize(h.st2),
@@ -772,7 +953,8 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
             // continuing the image's view sums, while the next one is copied in.  For DD/SF
             // the last chunk runs in y slabs, and each finished slab goes back to the host
             // while the next one computes (voxels are independent).
-            const bool slabs = method == CTSIM_BACK_DD || method == CTSIM_BACK_TF;
+            // (a staged, pageable image goes back in one piece after the last chunk)
+            const bool slabs = (method == CTSIM_BACK_DD || method == CTSIM_BACK_TF) && !stage_out;
             const int nch = std::min(HostCache::kChunks, G.noviews);
             auto first_view = [&](int c) { return (int)((long long)G.noviews * c / nch); };
             auto first_row = [&](int k) { return (int)((long long)G.ny * k / HostCache::kSlabs); };
@@ -780,8 +962,8 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
             for (int c = 0; c < nch && s == CTSIM_OK; c++) {
                 const int vb = first_view(c), ve = first_view(c + 1);
                 float *dproj = static_cast<float *>(h.dsino) + (size_t)vb * nuv;
-                if ((e = cudaMemcpyAsync(dproj, in + (size_t)vb * nuv, (size_t)(ve - vb) * nuv * sizeof(float),
-                                         cudaMemcpyHostToDevice, h.copy)) != cudaSuccess ||
+                if ((e = h2d(dproj, in + (size_t)vb * nuv, (size_t)(ve - vb) * nuv * sizeof(float), h.copy)) !=
+                        cudaSuccess ||
                     (e = cudaEventRecord(h.done[c], h.copy)) != cudaSuccess ||
                     (e = cudaStreamWaitEvent(h.st, h.done[c], 0)) != cudaSuccess) {
                     s = cuda_fail(e, "host to device copy");
@@ -800,7 +982,9 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
             }
             const size_t plane = (size_t)G.nx * G.ny;
             if (!slabs && s == CTSIM_OK &&
-                (e = cudaMemcpyAsync(out, h.dimg, nimg * sizeof(float), cudaMemcpyDeviceToHost, h.st)) != cudaSuccess)
+                (e = stage_out ? h.staged_d2h(out, h.dimg, nimg * sizeof(float), h.st)
+                               : cudaMemcpyAsync(out, h.dimg, nimg * sizeof(float), cudaMemcpyDeviceToHost, h.st)) !=
+                    cudaSuccess)
                 s = cuda_fail(e, "device to host copy");
             for (int k = 0; slabs && k < HostCache::kSlabs && s == CTSIM_OK; k++) {
                 const int y0 = first_row(k), y1 = first_row(k + 1);
