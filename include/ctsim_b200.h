@@ -20,7 +20,9 @@
  *      other methods return CTSIM_ERR_UNSUPPORTED)
  *
  *    Outputs are overwritten (the reference MEX allocates them zero-filled and
- *    accumulates; the result is the same).
+ *    accumulates; the result is the same).  Host buffers may be pageable (they are
+ *    staged through the library's pinned buffers by a few host threads) or
+ *    page-locked (copied directly); the results are identical.
  *
  * 2. Device-resident plans for callers that keep volumes and sinograms in GPU
  *    memory (FDK, OS-PWLS loops, batching).  A plan holds the per-view geometry
