@@ -1114,6 +1114,10 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
     const int iy = blockIdx.x / tiles_x;
     const int ix = (blockIdx.x % tiles_x) * 8 + warp;
     if (ix >= g.nx || iy >= g.ny) return;
+    // per view of the current 32-view chunk, written by the view's own lane:
+    // {wul, omu, w2, w2s}, {couch, 1 if u is on the detector else 0, bits of the detector
+    // column's element offset}
+    __shared__ float4 vtab[8][32][2];
     const size_t nxy = (size_t)g.nx * g.ny;
     const size_t nuv = (size_t)g.nu * g.nv;
     const bool on = map[iy * g.nx + ix] != 0;
@@ -1157,18 +1161,31 @@ __global__ void __launch_bounds__(256) pd_kernel(Geom g, const View *__restrict_
                     }
                     couch = VAR ? v.wz : v.couch_pd;  // back,var: the couch shift is in wz
                 }
+                {
+                    // this lane's view: the detector column and u weights (cbct_back.c:90-99)
+                    float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = make_float4(couch, __int_as_float(0), 0.f, 0.f);
+                    if (kl < view_count && u >= g.u_lo && u <= g.u_hi) {  // cbct_back.c:90
+                        float fiu;
+                        const int iu = floor_pos(u, &fiu);
+                        const float wul = fsub(u, fiu);
+                        a = make_float4(wul, fsub(1.0f, wul), w2, w2s);
+                        const unsigned long long pv = (unsigned long long)kl * nuv + (unsigned long long)iu * g.nv;
+                        b.y = __int_as_float(1);
+                        b.z = __uint_as_float((unsigned)pv);
+                        b.w = __uint_as_float((unsigned)(pv >> 32));
+                    }
+                    __syncwarp();  // the previous chunk's reads are done
+                    vtab[warp][lane][0] = a;
+                    vtab[warp][lane][1] = b;
+                }
+                __syncwarp();
                 const int nk = min(32, view_count - k0);
                 for (int j = 0; j < nk; j++) {
-                    const float uj = __shfl_sync(kFull, u, j);
-                    const float w2j = __shfl_sync(kFull, w2, j);
-                    const float w2sj = __shfl_sync(kFull, w2s, j);
-                    const float cj = __shfl_sync(kFull, couch, j);
-                    if (!(uj >= g.u_lo && uj <= g.u_hi)) continue;  // cbct_back.c:90
-                    float fiu;
-                    const int iu = floor_pos(uj, &fiu);
-                    const float wul = fsub(uj, fiu);
-                    const float omu = fsub(1.0f, wul);
-                    const size_t pv = (size_t)(k0 + j) * nuv + (size_t)iu * g.nv;  // element offset
+                    const float4 b = vtab[warp][j][1];
+                    if (__float_as_int(b.y) == 0) continue;  // u off the detector
+                    const float4 a = vtab[warp][j][0];
+                    const float wul = a.x, omu = a.y, w2j = a.z, w2sj = a.w, cj = b.x;
+                    const size_t pv = ((size_t)__float_as_uint(b.w) << 32) | __float_as_uint(b.z);  // element offset
 #pragma unroll
                     for (int m = 0; m < MZ; m++) {
                         if (lane + 32 * m < izn) {
