@@ -98,8 +98,11 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                                            int block) {
     constexpr int kWS = 17;  // row stride of the per-warp weight table (conflict-free writes)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float *wtab = smem + warp * (32 * kWS + qcap);  // [32 views][17] u weights of the view chunk
-    float *Q = wtab + 32 * kWS;                     // [qcap] q per row (16-byte aligned: 32 * 17 * 4 = 2176)
+    float *wtab = smem + warp * (32 * kWS + 32 * 8 + qcap);  // [32 views][17] u weights of the view chunk
+    // [32 views] per-view scalars of the chunk, written by the view's own lane:
+    // {ampu, zinc, vstart, iumin | nb << 16}, {rbase | r_hi << 16, path + 1 (0: no rows), -, -}
+    float4 *vtab = reinterpret_cast<float4 *>(wtab + 32 * kWS);  // 16-byte aligned: 32 * 17 * 4 = 2176
+    float *Q = wtab + 32 * kWS + 32 * 8;                         // [qcap] q per row
     const int tiles_x = (g.nx + 7) >> 3;
     const int iy = block / tiles_x;
     const int ix = (block % tiles_x) * 8 + warp;
@@ -132,39 +135,58 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                 const int kl = k0 + lane;
                 if (kl < view_count) my = column_footprint<METHOD>(g, views[view_begin + kl * view_stride], ix, iy);
                 // lane-parallel u weights of this lane's view (geom/cbct/cbct_back.c:288-301, :549-578)
-                if (my.hit) {
-                    const int nb = my.iumax - my.iumin + 1;
-                    for (int b = 0; b < nb; b++)
-                        wtab[lane * kWS + b] = u_weight<METHOD>(my.iumin + b, my.iumin, my.iumax, my.p0, my.p1, my.p2, my.p3);
+                // A voxel's vmax - vmin is zinc within 1.5 float ulps of nv (< 2^-10 for nv <=
+                // 8192), so away from zinc = 1 and 2 by a margin every voxel of the view covers
+                // the same number of rows give or take one: n = k_hi - k_lo is 0 or 1 (zinc < 1)
+                // or 1 or 2 (1 < zinc < 2).  Those views run branch-free (paths 1 and 2 below).
+                constexpr float kMargin = 1.0f / 256.0f;
+                __syncwarp();  // the previous chunk's reads of wtab and vtab are done
+                {
+                    int path1 = 0, rows = 0;
+                    if (my.hit) {
+                        const int nb = my.iumax - my.iumin + 1;
+                        for (int b = 0; b < nb; b++)
+                            wtab[lane * kWS + b] =
+                                u_weight<METHOD>(my.iumin + b, my.iumin, my.iumax, my.p0, my.p1, my.p2, my.p3);
+                        // rows reachable by voxels [iz0, iz0+izn) (the reference's clamped
+                        // extents, monotone in iz)
+                        const float zinc = my.zinc, vstart = my.vstart;
+                        const float a0u = fadd(fadd(vstart, fmul(fz_first, zinc)), 0.5f);
+                        const float b1u = fadd(fadd(fadd(vstart, fmul(fz_last, zinc)), zinc), 0.5f);
+                        const float a0 = fmaxf(a0u, 0.0f), b1 = fminf(b1u, fnv);
+                        if (a0 < fnv && b1 >= 0.0f) {
+                            const int r_lo = floor_pos(a0);
+                            int r_hi = min(floor_pos(b1), nvm1);
+                            if (r_lo <= r_hi) {
+                                const int rbase = r_lo & ~3;
+                                // every voxel of the pass exists and lies inside the detector
+                                bool inside = a0u > 0.0f && b1u < fnv && izn == zpass;
+                                if (r_hi - rbase + 1 > qcap) {  // rows rbase..r_hi must fit
+                                    atomicOr(err, 1);
+                                    r_hi = rbase + qcap - 1;
+                                    inside = false;
+                                }
+                                path1 = 1 + (!inside ? 0 : zinc < 1.0f - kMargin ? 1
+                                                     : (zinc > 1.0f + kMargin && zinc < 2.0f - kMargin) ? 2 : 0);
+                                rows = rbase | (r_hi << 16);
+                            }
+                        }
+                        vtab[2 * lane] = make_float4(my.ampu, zinc, vstart, __int_as_float(my.iumin | (nb << 16)));
+                    }
+                    vtab[2 * lane + 1] = make_float4(__int_as_float(rows), __int_as_float(path1), 0.f, 0.f);
                 }
                 __syncwarp();
                 const int nk = min(32, view_count - k0);
                 for (int j = 0; j < nk; j++) {
-                    if (!__shfl_sync(kFull, (int)my.hit, j)) continue;
-                    const int iumin = __shfl_sync(kFull, my.iumin, j);
-                    const int iumax = __shfl_sync(kFull, my.iumax, j);
-                    const float ampu = __shfl_sync(kFull, my.ampu, j);
-                    const float zinc = __shfl_sync(kFull, my.zinc, j);
-                    const float vstart = __shfl_sync(kFull, my.vstart, j);
-                    // rows reachable by voxels [iz0, iz0+izn) (the reference's clamped extents, monotone in iz)
-                    const float a0u = fadd(fadd(vstart, fmul(fz_first, zinc)), 0.5f);
-                    const float b1u = fadd(fadd(fadd(vstart, fmul(fz_last, zinc)), zinc), 0.5f);
-                    const float a0 = fmaxf(a0u, 0.0f), b1 = fminf(b1u, fnv);
-                    if (!(a0 < fnv) || !(b1 >= 0.0f)) continue;
-                    const int r_lo = floor_pos(a0);
-                    int r_hi = min(floor_pos(b1), nvm1);
-                    if (r_lo > r_hi) continue;
-                    const int rbase = r_lo & ~3;
-                    // every voxel of the pass exists and lies inside the detector (no clamps)
-                    bool inside = a0u > 0.0f && b1u < fnv && izn == zpass;
-                    if (r_hi - rbase + 1 > qcap) {  // rows rbase..r_hi must fit
-                        if (lane == 0) atomicOr(err, 1);
-                        r_hi = rbase + qcap - 1;
-                        inside = false;
-                    }
+                    const float4 pb = vtab[2 * j + 1];
+                    const int path1 = __float_as_int(pb.y);
+                    if (path1 == 0) continue;  // no footprint or no rows
+                    const float4 pa = vtab[2 * j];
+                    const float ampu = pa.x, zinc = pa.y, vstart = pa.z;
+                    const int iumin = __float_as_int(pa.w) & 0xffff, nb = __float_as_int(pa.w) >> 16;
+                    const int rbase = __float_as_int(pb.x) & 0xffff, r_hi = __float_as_int(pb.x) >> 16;
                     // q over rows [rbase, r_hi], 128 rows per pass (the voxels read rows
                     // [r_lo, r_hi] only)
-                    const int nb = iumax - iumin + 1;
                     const float *wj = wtab + j * kWS;
                     const size_t pv = (size_t)(k0 + j) * nuv + (size_t)iumin * g.nv;  // element offsets
                     const size_t av = (size_t)iumin * g.nv;
@@ -190,15 +212,10 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                     // shared address of row k is qadj + 4 * bits(k + 2^23) (mod 2^32)
                     const uint32_t qadj = (uint32_t)__cvta_generic_to_shared(Q) - 4u * (uint32_t)rbase -
                                           (0x4B000000u << 2);
-                    // vmax - vmin is zinc within 1.5 float ulps of nv (< 2^-10 for nv <= 8192), so
-                    // away from zinc = 1 and 2 by a margin every voxel of the view covers the same
-                    // number of rows give or take one: n = k_hi - k_lo is 0 or 1 (zinc < 1) or 1 or
-                    // 2 (1 < zinc < 2).  Those views run branch-free: the rows k_lo .. k_lo + 1 (+ 2)
-                    // are always read (the row buffer has 4 spare floats; rows past r_hi may hold
-                    // anything, so their terms are selected, never multiplied by zero).
-                    constexpr float kMargin = 1.0f / 256.0f;
-                    const int path = !inside ? 0 : zinc < 1.0f - kMargin ? 1
-                                                 : (zinc > 1.0f + kMargin && zinc < 2.0f - kMargin) ? 2 : 0;
+                    // Paths 1 and 2 always read the rows k_lo .. k_lo + 1 (+ 2) (the row buffer has 4
+                    // spare floats; rows past r_hi may hold anything, so their terms are selected,
+                    // never multiplied by zero).
+                    const int path = path1 - 1;
                     if (path == 1) {
 #pragma unroll
                         for (int m = 0; m < MZ; m++) {
@@ -1258,7 +1275,7 @@ cudaError_t allow_dynamic_smem(const void *kfn, size_t bytes) {
 
 // per warp: the u weights of 32 views and the row buffer; 4 spare floats past the last
 // warp's buffer for the branch-free row reads
-size_t back_smem_bytes(int qcap) { return ((size_t)8 * (32 * 17 + qcap) + 4) * sizeof(float); }
+size_t back_smem_bytes(int qcap) { return ((size_t)8 * (32 * 17 + 32 * 8 + qcap) + 4) * sizeof(float); }
 
 template <int METHOD, int MZ, bool VEC, int SRC, bool SUM>
 static cudaError_t launch_back_mz(const Geom &g, const View *views, const void *ps, const float *ampv,
