@@ -729,11 +729,6 @@ __device__ __forceinline__ float lds_f32(uint32_t a) {
     asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
     return v;
 }
-__device__ __forceinline__ int lds_s32(uint32_t a) {
-    int v;
-    asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(a));
-    return v;
-}
 __device__ __forceinline__ float4 lds_f32x4(uint32_t a) {
     float4 v;
     asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
@@ -750,14 +745,14 @@ __device__ __forceinline__ void acc_add4(uint32_t a, float w, float r0, float r1
 
 // Dynamic shared-memory layout of the staged forward projector: four mbarriers (first, so
 // that a persistent block keeps them across work items of different shapes), the
-// accumulators, the two stage buffers, the candidate table and its packed index, the
+// accumulators, the two stage buffers, the packed candidate table, the
 // line tables.
 struct StagedSmem {
     int nq, nt, nlines, groups, slots, xstride;
     __host__ __device__ size_t acc_bytes() const { return (size_t)groups * kTU * nq * 16; }
     __host__ __device__ size_t stage_floats() const { return (size_t)slots * xstride; }  // one buffer
     __host__ __device__ size_t bytes() const {
-        return 32 + acc_bytes() + 2 * stage_floats() * 4 + (size_t)nt * (6 + kTU) * 4 +
+        return 32 + acc_bytes() + 2 * stage_floats() * 4 + (size_t)nt * (5 + kTU) * 4 +
                (size_t)(2 * nlines + 1 + 32) * 4;
     }
 };
@@ -877,10 +872,10 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
     StagedSmem L{nq, NT, nlines0, GROUPS, slots, xst};
     float *stage = reinterpret_cast<float *>(acc4 + GROUPS * kTU * nq);  // [2][slots][xst]
     // per candidate slot: {-b0 / zinc, 1 / zinc, rlo | rhi << 16, jlo | jhi << 8} (one 16-byte load)
+    // (all three indexed by the candidate's position among the chunk's valid candidates)
     float4 *c_prm = reinterpret_cast<float4 *>(stage + 2 * L.stage_floats());
     int *c_col = reinterpret_cast<int *>(c_prm + NT);
-    int *c_idx = c_col + NT;                          // slots of the valid candidates, packed
-    float *c_w = reinterpret_cast<float *>(c_idx + NT);  // [NT][kTU]
+    float *c_w = reinterpret_cast<float *>(c_col + NT);  // [NT][kTU]
     int *line_start = reinterpret_cast<int *>(c_w + NT * kTU);
     int *line_off = line_start + nlines0;
     int *s_warp_tot = line_off + nlines0 + 1;  // [32]
@@ -894,7 +889,7 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
     float4 *gacc = acc4 + grp * kTU * nq;
     // 32-bit shared addresses of the row loop's tables
     const uint32_t acc_u32 = smem_addr(gacc), nq16 = 16u * (uint32_t)nq;
-    const uint32_t idx_u32 = smem_addr(c_idx), prm_u32 = smem_addr(c_prm), w_u32 = smem_addr(c_w);
+    const uint32_t prm_u32 = smem_addr(c_prm), w_u32 = smem_addr(c_w);
     const float fnz = (float)g.nz;
     // rows iv0 .. iv0 + 3 (f0 = iv0 as float) of one candidate: X at the five row edges from
     // the staged column (xadj), R = X(iv + 1) - X(iv), added with the weights at wq into the
@@ -932,9 +927,12 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
     int vbase = 0;  // valid candidates of the earlier chunks
 
     for (int c0 = 0; c0 < ncand; c0 += NT) {
-        // 1. exact footprint of candidate c0 + t into slot t; the valid slots are packed
-        // into the index list c_idx
+        // 1. exact footprint of candidate c0 + t; the valid candidates' scalars, weights and
+        // columns are packed in candidate order
         bool valid = false;
+        int my_col = 0;
+        float4 my_prm;
+        float my_w[kTU];
         {
             const int c = c0 + t;
             if (c < ncand) {
@@ -956,7 +954,7 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
                             float w = 0.0f;
                             if (j >= jlo && j <= jhi)
                                 w = u_weight<METHOD>(iu0 + j, fp.iumin, fp.iumax, fp.p0, fp.p1, fp.p2, fp.p3) * scl;
-                            c_w[t * kTU + j] = w;
+                            my_w[j] = w;
                         }
                         const float b0 = fp.vstart + 0.5f;
                         const float btop = fmaf(fnz, fp.zinc, b0);
@@ -965,10 +963,10 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
                         if (rlo <= rhi) {
                             valid = true;
                             const float izc = 1.0f / fp.zinc;
-                            c_col[t] = col;
+                            my_col = col;
                             // s(iv) = iv / zinc - b0 / zinc
-                            c_prm[t] = make_float4(-b0 * izc, izc, __int_as_float(rlo | (rhi << 16)),
-                                                   __int_as_float(jlo | (jhi << 8)));
+                            my_prm = make_float4(-b0 * izc, izc, __int_as_float(rlo | (rhi << 16)),
+                                                 __int_as_float(jlo | (jhi << 8)));
                         }
                     }
                 }
@@ -983,7 +981,13 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
             base += w < warp ? n : 0;
             nval += n;
         }
-        if (valid) c_idx[base + __popc(bal & ((1u << lane) - 1u))] = t;
+        if (valid) {
+            const int q = base + __popc(bal & ((1u << lane) - 1u));
+            c_col[q] = my_col;
+            c_prm[q] = my_prm;
+#pragma unroll
+            for (int j = 0; j < kTU; j++) c_w[q * kTU + j] = my_w[j];
+        }
         __syncthreads();
 
         // 2. the packed candidates, `slots` at a time: warp 0 issues the copies of the next
@@ -1003,7 +1007,7 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
             if (!free) return;
             float *dst = stage + (size_t)buf * L.stage_floats();
             for (int i = lane; i < n; i += 32)
-                bulk_copy_g2s(dst + (size_t)i * xst, xs + (size_t)c_col[c_idx[p0 + i]] * xst, col_bytes, &bar[buf]);
+                bulk_copy_g2s(dst + (size_t)i * xst, xs + (size_t)c_col[p0 + i] * xst, col_bytes, &bar[buf]);
         };
         if (nsub > 0 && warp == 0) issue(0, buf0);
         for (int sub = 0; sub < nsub; sub++) {
@@ -1020,15 +1024,14 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
             if (R == 32) {
                 // one-warp groups walk each candidate's own rows (every row of the group is theirs)
                 for (int p = pstart0; p < p1; p += GROUPS) {
-                    const int q = lds_s32(idx_u32 + 4u * (uint32_t)p);
-                    const float4 prm = lds_f32x4(prm_u32 + 16u * (uint32_t)q);
+                    const float4 prm = lds_f32x4(prm_u32 + 16u * (uint32_t)p);
                     const int rr = __float_as_int(prm.z), jj = __float_as_int(prm.w);
                     const int prlo = rr & 0xffff, prhi = rr >> 16;
                     const int pjlo = jj & 0xff;
                     const uint32_t xadj = sb + (uint32_t)((p - p0) * xst) * 4u;
                     for (int wrow = prlo & ~3; wrow <= prhi; wrow += 128)
                         staged_rows(wrow + 4 * lane, small_int_to_float(wrow + 4 * lane), prm.x, prm.y, xadj,
-                                    w_u32 + 4u * (uint32_t)(q * kTU + pjlo), acc_u32 + nq16 * (uint32_t)pjlo,
+                                    w_u32 + 4u * (uint32_t)(p * kTU + pjlo), acc_u32 + nq16 * (uint32_t)pjlo,
                                     (jj >> 8) - pjlo);
                 }
             } else {
@@ -1038,13 +1041,12 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
                     const int iv0 = wrow + 4 * lane;
                     const float f0 = small_int_to_float(iv0);
                     for (int p = pstart0; p < p1; p += GROUPS) {
-                        const int q = lds_s32(idx_u32 + 4u * (uint32_t)p);
-                        const float4 prm = lds_f32x4(prm_u32 + 16u * (uint32_t)q);
+                        const float4 prm = lds_f32x4(prm_u32 + 16u * (uint32_t)p);
                         const int rr = __float_as_int(prm.z), jj = __float_as_int(prm.w);
                         if (wrow > (rr >> 16) || wrow + 127 < (rr & 0xffff)) continue;  // warp-uniform
                         const int pjlo = jj & 0xff;
                         staged_rows(iv0, f0, prm.x, prm.y, sb + (uint32_t)((p - p0) * xst) * 4u,
-                                    w_u32 + 4u * (uint32_t)(q * kTU + pjlo), acc_u32 + nq16 * (uint32_t)pjlo,
+                                    w_u32 + 4u * (uint32_t)(p * kTU + pjlo), acc_u32 + nq16 * (uint32_t)pjlo,
                                     (jj >> 8) - pjlo);
                     }
                 }
