@@ -226,10 +226,11 @@ __device__ __forceinline__ void back_block(const Geom g, const View *__restrict_
                             const float tlo = __fadd_rd(vmin, kTwo23), thi = __fadd_rd(vmax, kTwo23);
                             const uint32_t qa = qadj + (__float_as_uint(tlo) << 2);
                             const float q0 = lds_ordered(qa), q1 = lds_ordered(qa + 4u);
-                            // one row: (vmax - vmin) q0; two: (k_lo + 1 - vmin) q0 + (vmax - k_hi) q1
+                            // one row: (vmax - vmin) q0; two: (k_lo + 1 - vmin) q0 + (vmax - k_hi) q1,
+                            // where k_hi = k_lo + 1 (kf, exact)
                             const float one = fsub(vmax, vmin) * q0;
-                            const float two = fmaf(fsub(vmax, fsub(thi, kTwo23)), q1,
-                                                   fsub(fsub(tlo, kTwo23 - 1.0f), vmin) * q0);
+                            const float kf = fsub(tlo, kTwo23 - 1.0f);
+                            const float two = fmaf(fsub(vmax, kf), q1, fsub(kf, vmin) * q0);
                             acc[m] = fmaf(ampu, thi == tlo ? one : two, acc[m]);
                         }
                     } else if (path == 2) {
@@ -892,8 +893,9 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
     const uint32_t prm_u32 = smem_addr(c_prm), w_u32 = smem_addr(c_w);
     const float fnz = (float)g.nz;
     // rows iv0 .. iv0 + 3 (f0 = iv0 as float) of one candidate: X at the five row edges from
-    // the staged column (xadj), R = X(iv + 1) - X(iv), added with the weights at wq into the
-    // accumulator columns at aq (pjn + 1 of them).  Boundary iv sits at s = iv / zinc -
+    // the staged column (xadj), R = X(iv + 1) - X(iv), added with the weights at wq (16-byte
+    // aligned, the first for the candidate's first column) into the accumulator columns at aq
+    // (pjn + 1 of them).  Boundary iv sits at s = iv / zinc -
     // b0 / zinc (psa, piz), one rounding from iv alone, so a row's value does not depend on
     // which lane, warp or pass evaluates it; rows outside the column's shadow have both
     // edges clamped to the same end of the column and add exactly 0 (no per-lane test).
@@ -907,13 +909,17 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
         if (iv0 < nv) {
             const float R0 = X1 - X0, R1 = X2 - X1, R2 = X3 - X2, R3 = X4 - X3;
             const uint32_t a = aq + 4u * (uint32_t)iv0;  // float4 of rows iv0 .. iv0 + 3
-            acc_add4(a, lds_f32(wq), R0, R1, R2, R3);
+            const float4 w4 = lds_f32x4(wq);  // the candidate's first four weights
+            acc_add4(a, w4.x, R0, R1, R2, R3);
             if (pjn > 0) {
-                acc_add4(a + nq16, lds_f32(wq + 4u), R0, R1, R2, R3);
+                acc_add4(a + nq16, w4.y, R0, R1, R2, R3);
                 if (pjn > 1) {
-                    acc_add4(a + 2u * nq16, lds_f32(wq + 8u), R0, R1, R2, R3);
-                    for (int j = 3; j <= pjn; j++)
-                        acc_add4(a + (uint32_t)j * nq16, lds_f32(wq + 4u * j), R0, R1, R2, R3);
+                    acc_add4(a + 2u * nq16, w4.z, R0, R1, R2, R3);
+                    if (pjn > 2) {
+                        acc_add4(a + 3u * nq16, w4.w, R0, R1, R2, R3);
+                        for (int j = 4; j <= pjn; j++)
+                            acc_add4(a + (uint32_t)j * nq16, lds_f32(wq + 4u * j), R0, R1, R2, R3);
+                    }
                 }
             }
         }
@@ -949,12 +955,14 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
                     if (fp.hit && fp.iumax >= iu0 && fp.iumin <= iu0 + kTU - 1) {
                         const int jlo = max(fp.iumin, iu0) - iu0, jhi = min(fp.iumax, iu0 + kTU - 1) - iu0;
                         const float scl = fp.ampu * fp.zinc;
+                        // weight i for detector column iu0 + jlo + i (16-byte loads in the row loop)
 #pragma unroll
-                        for (int j = 0; j < kTU; j++) {
+                        for (int i = 0; i < kTU; i++) {
                             float w = 0.0f;
-                            if (j >= jlo && j <= jhi)
-                                w = u_weight<METHOD>(iu0 + j, fp.iumin, fp.iumax, fp.p0, fp.p1, fp.p2, fp.p3) * scl;
-                            my_w[j] = w;
+                            if (jlo + i <= jhi)
+                                w = u_weight<METHOD>(iu0 + jlo + i, fp.iumin, fp.iumax, fp.p0, fp.p1, fp.p2, fp.p3) *
+                                    scl;
+                            my_w[i] = w;
                         }
                         const float b0 = fp.vstart + 0.5f;
                         const float btop = fmaf(fnz, fp.zinc, b0);
@@ -1031,7 +1039,7 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
                     const uint32_t xadj = sb + (uint32_t)((p - p0) * xst) * 4u;
                     for (int wrow = prlo & ~3; wrow <= prhi; wrow += 128)
                         staged_rows(wrow + 4 * lane, small_int_to_float(wrow + 4 * lane), prm.x, prm.y, xadj,
-                                    w_u32 + 4u * (uint32_t)(p * kTU + pjlo), acc_u32 + nq16 * (uint32_t)pjlo,
+                                    w_u32 + 4u * (uint32_t)(p * kTU), acc_u32 + nq16 * (uint32_t)pjlo,
                                     (jj >> 8) - pjlo);
                 }
             } else {
@@ -1046,7 +1054,7 @@ __device__ __forceinline__ bool proj_staged_block(const Geom g, const View *__re
                         if (wrow > (rr >> 16) || wrow + 127 < (rr & 0xffff)) continue;  // warp-uniform
                         const int pjlo = jj & 0xff;
                         staged_rows(iv0, f0, prm.x, prm.y, sb + (uint32_t)((p - p0) * xst) * 4u,
-                                    w_u32 + 4u * (uint32_t)(p * kTU + pjlo), acc_u32 + nq16 * (uint32_t)pjlo,
+                                    w_u32 + 4u * (uint32_t)(p * kTU), acc_u32 + nq16 * (uint32_t)pjlo,
                                     (jj >> 8) - pjlo);
                     }
                 }
