@@ -691,6 +691,17 @@ class HostPool {
     unsigned long long gen_ = 0;
 };
 
+// First view of chunk c (0 .. nch) when n views are split into nch chunks for the host
+// path.  With enough views one chunk, the first (A^T: its copy in cannot overlap compute)
+// or the last (A: its copy out cannot), gets a quarter of the others' views, so the
+// copies outside the overlap are short.  Every chunk keeps at least two views.
+int chunk_first_view(int n, int nch, int c, bool small_last) {
+    if (n < 8 * nch || nch < 2) return (int)((long long)n * c / nch);
+    const long long total = 4LL * (nch - 1) + 1;  // weight 1 for the short chunk, 4 for the others
+    const long long w = small_last ? (c == nch ? total : 4LL * c) : (c == 0 ? 0 : 1 + 4LL * (c - 1));
+    return (int)((long long)n * w / total);
+}
+
 // True for page-locked (registered or cudaHostAlloc'd) host memory and device memory;
 // false for ordinary pageable memory.
 bool dma_ready(const void *p) {
@@ -922,7 +933,7 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
                                   (e = cudaStreamWaitEvent(h.st2, h.ready, 0)) != cudaSuccess))
                 s = cuda_fail(e, "event");
             const int nch = std::min(HostCache::kChunks, G.noviews);
-            auto first_view = [&](int c) { return (int)((long long)G.noviews * c / nch); };
+            auto first_view = [&](int c) { return chunk_first_view(G.noviews, nch, c, true); };
             for (int c = 0; c < nch && s == CTSIM_OK; c++) {
                 const int vb = first_view(c), ve = first_view(c + 1);
                 cudaStream_t sc = (c & 1) ? h.st2 : h.st;
@@ -956,7 +967,7 @@ bool run_host(int method, const ctsim_geom &G, const double *betas, const float 
             // (a staged, pageable image goes back in one piece after the last chunk)
             const bool slabs = (method == CTSIM_BACK_DD || method == CTSIM_BACK_TF) && !stage_out;
             const int nch = std::min(HostCache::kChunks, G.noviews);
-            auto first_view = [&](int c) { return (int)((long long)G.noviews * c / nch); };
+            auto first_view = [&](int c) { return chunk_first_view(G.noviews, nch, c, false); };
             auto first_row = [&](int k) { return (int)((long long)G.ny * k / HostCache::kSlabs); };
             ctsim_status s = CTSIM_OK;
             for (int c = 0; c < nch && s == CTSIM_OK; c++) {

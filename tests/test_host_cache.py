@@ -32,10 +32,10 @@ def _uncached(kind, g, data):
 
 
 @pytest.mark.parametrize("views,size", [(1, (96, 80, 24)), (5, (96, 80, 24)), (37, (96, 80, 24)),
-                                        (11, (7, 3, 40))])
+                                        (11, (7, 3, 40)), (70, (96, 80, 24))])
 def test_cached_calls_equal_uncached_and_plan(views, size):
     """Chunks of one view, fewer views than chunks, uneven chunks; fewer image rows than
-    y slabs."""
+    y slabs; with 64 views or more a short first (A^T) or last (A) chunk."""
     import torch
     g = _geom(views, size=size)
     x, y = case_inputs(g, seed=views)
