@@ -23,7 +23,8 @@ AZ = F32(0.5)
 
 def compute_weights_pwls(sino, r=0.0, v=0.0):
     s = np.asarray(sino, dtype=F32)
-    w = ((s - F32(r)) ** 2 / (s + F32(v))).astype(F32)
+    with np.errstate(divide="ignore", invalid="ignore"):  # s = -v divides by zero, as it does in MATLAB
+        w = ((s - F32(r)) ** 2 / (s + F32(v))).astype(F32)
     w[s <= F32(r)] = 0
     return w
 
