@@ -382,10 +382,16 @@ def run_ours(args):
                 "cpu_baseline": cpu}
         if args.extras:
             line["extras"] = extras(plan, xd, yd, sino, img, vv)
-        if world == 1 and not args.no_serving:
+        if world == 1 and not (args.no_serving and args.no_config1):
             del plan, xd, yd, sino, img
             torch.cuda.empty_cache()
-            line["serving"] = serving_leg(args.seed)
+            if not args.no_config1:
+                try:
+                    line["config1"] = config1_leg(K)
+                except Exception as exc:  # a side figure: the headline line is printed either way
+                    line["config1"] = {"error": f"{type(exc).__name__}: {exc}"}
+            if not args.no_serving:
+                line["serving"] = serving_leg(args.seed)
         print(json.dumps(line), flush=True)
     if dist:
         td.destroy_process_group()
@@ -422,6 +428,54 @@ def extras(plan, xd, yd, sino, img, vv):
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / 3
         out[name] = {"ms": ms, "gvv_s": vv / (ms / 1e3) / 1e9}
+    return out
+
+
+def config1_leg(steps: int):
+    """DD A + A^T on the 128x128x64 / 360-view / 256x96 scan (volume 4 MB, sinogram 35 MB,
+    both L2-resident): y = A x + N(0, 0.01^2), ``steps`` timed steps, each preceded by a
+    512 MB write that flushes L2, so every step starts from HBM.  Events bracket A and
+    A^T only, on the launching stream."""
+    import torch
+    from ctsim_b200.phantom import config1, to_projector_units
+    from ctsim_b200.projector import Plan
+    g, x_mm = config1(seed=1)
+    vv = float(g.nx * g.ny * g.nz * g.noViews)
+    plan = Plan(g)
+    xd = torch.from_numpy(to_projector_units(x_mm)).cuda()
+    gen = torch.Generator(device=xd.device)
+    gen.manual_seed(11)
+    with torch.no_grad():
+        yd = plan.project(xd, "dd")
+        yd = (yd + 0.01 * torch.randn(yd.shape, generator=gen, device=xd.device)).contiguous()
+    sino = torch.empty_like(yd)
+    img = torch.empty_like(xd)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=xd.device)
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        plan.project(xd, "dd", out=sino)
+        plan.backproject(yd, "dd", out=img)
+    torch.cuda.synchronize()
+    plan.check()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    for e in ev:
+        flush.fill_(1)
+        e[0].record(stream)
+        plan.project(xd, "dd", out=sino)
+        e[1].record(stream)
+        plan.backproject(yd, "dd", out=img)
+        e[2].record(stream)
+    torch.cuda.synchronize()
+    t_a = float(np.mean([e[0].elapsed_time(e[1]) for e in ev]))
+    t_b = float(np.mean([e[1].elapsed_time(e[2]) for e in ev]))
+    ms = t_a + t_b
+    out = {"workload": "DD A + A^T, 128x128x64 @1mm, 360 views, flat 256x96 @1.6mm, SAD 1000, SDD 1500 "
+                       "(seeded 12-ellipsoid phantom, y = A x + N(0, 0.01^2))",
+           "value": vv / (ms / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms, "steps": steps,
+           "kernels_ms": {"A (prefix+proj)": t_a, "A^T (back)": t_b},
+           "l2": "512 MB write before each step (volume 4 MB and sinogram 35 MB fit in L2)"}
+    del plan, xd, yd, sino, img, flush
+    torch.cuda.empty_cache()
     return out
 
 
@@ -914,6 +968,8 @@ def main():
     ap.add_argument("--no-e2e", dest="no_e2e", action="store_true", help="skip the end-to-end host-buffer leg")
     ap.add_argument("--no-serving", dest="no_serving", action="store_true",
                     help="skip the bounded served-stream leg of the default run")
+    ap.add_argument("--no-config1", dest="no_config1", action="store_true",
+                    help="skip the 128x128x64 / 360-view DD step of the default run")
     ap.add_argument("--serving", action="store_true", help="served FDK/OS-PWLS request mix instead of A/A^T")
     ap.add_argument("--requests", type=int, default=24, help="requests of the serving run")
     ap.add_argument("--slots", type=int, default=8, help="concurrent requests of the serving run")
