@@ -49,6 +49,30 @@ def test_oracle_matches_reference_library(name):
         assert np.array_equal(oracle_cbct(k, g, src), ref_cbct(k, g, src)), k
 
 
+def _bench_geometry(which: str, nviews: int):
+    """The benchmark scans with ``nviews`` of their views (0, 45, 90, 135 degrees, ...):
+    128x128x64 / 256x96 / 360 views, and 512x512x256 / 1024x384 / 720 views."""
+    from dataclasses import replace
+    from ctsim_b200.phantom import config1, config2, to_projector_units
+    g, x_mm = (config1(seed=1) if which == "config1" else config2(seed=2))
+    s = g.noViews // 8
+    g = replace(g, betas=g.betas[::s][:nviews].copy(), couchZ=g.couchZ[::s][:nviews].copy())
+    return g, to_projector_units(x_mm)
+
+
+@pytest.mark.skipif(not ref_available(), reason="reference library not built")
+@pytest.mark.parametrize("which,nviews", [("config1", 4), ("config2", 2)])
+def test_oracle_matches_reference_library_on_bench_scans(which, nviews):
+    """Bit-identical at the benchmark geometries too (sizes, pitches and magnification of
+    the timed runs), on the seeded phantom and a seeded sinogram, for the DD and SF pairs."""
+    g, x = _bench_geometry(which, nviews)
+    y = np.random.default_rng(3).uniform(0.0, 2.0, g.sino_shape).astype(np.float32)
+    for k in ("proj,dd", "back,dd", "proj,tf", "back,tf"):
+        src = x if k.startswith("proj") else y
+        assert np.array_equal(oracle_cbct(k, g, src), ref_cbct(k, g, src, nthreads=8)
+                              if k.startswith("proj") else ref_cbct(k, g, src)), k
+
+
 def test_planted_mistake_is_detected():
     g = CASES["basic"]
     d = np.load(os.path.join(os.path.dirname(__file__), "golden", "basic.npz"))
