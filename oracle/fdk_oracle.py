@@ -9,8 +9,9 @@ oracle.
     recon_fdk                 fbp/reconFDK.m:1-85
 
 MATLAB itself is not available, and its FFT (FFTW, single precision for single
-input) cannot be run here: parity of the filter step is therefore unpinned
-against MATLAB and checked against this float64 restatement instead.
+input) cannot be run here: parity unpinned. The filter step is checked against
+this float64 restatement (and its FFT against numpy's FP64 FFT), not against MATLAB;
+the backprojection inside it is the pinned C oracle.
 """
 from __future__ import annotations
 

@@ -9,6 +9,11 @@ the reference's MATLAB in single precision, with the projectors of the C oracle.
 
 Arrays follow the package layout [nz, ny, nx]; the MATLAB code indexes x(i,j,k)
 with i along x, so the slicing below is written on the transposed view.
+
+Parity unpinned: MATLAB (and Octave) cannot run here and the reference holds no golden
+output for these functions, so this restatement is checked by reading it against the .m
+sources and by property tests (the penalty gradient is the derivative of its value, the
+first Nesterov step equals the SQS step), not against MATLAB's own results.
 """
 from __future__ import annotations
 

@@ -12,7 +12,8 @@
 
 MATLAB's poissrnd/randn streams cannot be reproduced; the device sampler is checked
 against this restatement of its own published algorithms (bit-exact stream, the same
-integer draws) and against the Poisson moments.
+integer draws) and against the Poisson moments.  Parity unpinned against MATLAB:
+the log transform is restated from the .m source, and no reference output exists here.
 """
 from __future__ import annotations
 
